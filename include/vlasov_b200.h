@@ -1,0 +1,245 @@
+/*
+ * vlasov_b200.h - C ABI of the B200 (sm_100a) Vlasov-Poisson library.
+ *
+ * Plain pointers and sizes only. Every array argument is a DEVICE pointer
+ * unless its comment says "host". Every entry point enqueues work on the
+ * given CUDA stream (a cudaStream_t passed as void*, NULL = legacy default
+ * stream), returns immediately, and reports argument errors synchronously
+ * through its return value. The library never allocates device memory inside
+ * these calls: the caller owns every buffer, including the scratch
+ * "workspace" whose size the *_workspace_bytes() queries return.
+ *
+ * Data layout: the distribution function f is a contiguous row-major array.
+ * 2D2V: f[Nx][Ny][Nvx][Nvy] (vy fastest). 1D1V: f[Nx][Nv].
+ * The sweep entry points view any such array as [n_outer][n_line][n_inner],
+ * where n_line is the advected axis (n_outer = product of the dims before it,
+ * n_inner = product of the dims after it).
+ *
+ * Each entry point cites the function of the reference PyTorch solver
+ * (simulations/vlasov2d_2v/pytorch/src/vlasov2D2V.py and
+ * simulations/vlasov1d_1v/pytorch/src/vlasov1D1V.py of
+ * yasahi-hpc/JAX-PyTorch-Vlasov) whose result it reproduces.
+ */
+#ifndef VLASOV_B200_H
+#define VLASOV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define VP_OK 0
+#define VP_ERR_ARG 1         /* null pointer, non-positive size, aliasing buffers */
+#define VP_ERR_DTYPE 2       /* unknown storage type */
+#define VP_ERR_WORKSPACE 3   /* workspace missing or smaller than required */
+#define VP_ERR_CUDA 4        /* a CUDA call or kernel launch failed (see vp_last_error) */
+#define VP_ERR_UNSUPPORTED 5 /* shape outside what the kernels implement */
+
+/* ---- storage types of f ------------------------------------------------ */
+#define VP_F32 0  /* float storage, float arithmetic */
+#define VP_F64 1  /* double storage, double arithmetic */
+#define VP_BF16 2 /* bfloat16 storage, float arithmetic */
+
+/* The "compute type" of a storage type is double for VP_F64 and float
+ * otherwise; drift weight tables and gather velocities use it. */
+
+/* Library version string and the message of the last failed call on this
+ * host thread. */
+const char* vp_version(void);
+const char* vp_last_error(void);
+
+/* Number of kernels this process has launched through the library so far
+ * (host-side count, all devices). No reference counterpart: it lets a
+ * benchmark state how many of its own kernels ran in a timed region. */
+uint64_t vp_launch_count(void);
+
+/* ---- sweeps ------------------------------------------------------------ */
+
+/* Periodic drift with static per-velocity shifts (the x and y drifts).
+ * Replaces advect_x_static (vlasov2D2V.py:756-819; vlasov1D1V.py:408-448)
+ * with the shift/weight tables of precompute_x_drift (vlasov2D2V.py:670-714):
+ *   out[o,l,c] = sum_k W[k*sel_mod + j] * in[o, (l - shift[j] - (k-2)) mod n_line, c]
+ * for k = 0..5, where j = (c / sel_div) % sel_mod.
+ * shift: int32[sel_mod]; W: compute type [6][sel_mod]. f_out must not
+ * overlap f_in. */
+int vp_drift(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line,
+             int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift,
+             const void* W, void* stream);
+
+/* The same drift fused with the velocity moment of its output (the y drift
+ * before the field solve, vlasov2D2V.py:1064 followed by compute_rho :416-431;
+ * 1D1V: the x drift and n = sum(f,1)*dv, vlasov1D1V.py:685,521):
+ *   rho[o*n_line + l] = (sum_c out[o,l,c]) * scale      (FP64, deterministic)
+ * workspace: vp_drift_rho_workspace_bytes() bytes of scratch. */
+int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line,
+                 int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift,
+                 const void* W, double scale, double* rho, void* workspace,
+                 size_t workspace_bytes, void* stream);
+size_t vp_drift_rho_workspace_bytes(int64_t n_outer, int64_t n_line, int64_t n_inner);
+
+/* Dirichlet kick along n_line with a field constant over each outer row
+ * (the vx or vy kick). Replaces advect_v_static with build_v_tap_weights
+ * (vlasov2D2V.py:822-913; vlasov1D1V.py:450-501): outer row o uses the field
+ * value E[o / e_div] (e_dtype VP_F32 or VP_F64), d = E*dt/dv, s = floor(d),
+ * alpha = d - s, and
+ *   out[o,l,c] = sum_k w_k(alpha) * in[o, l - s - (k-2), c]   (zero outside [0, n_line)).
+ * window >= 0 drops the taps with |s + k - 2| > window + 2, as the
+ * reference's static window S does; window < 0 keeps every tap (exact for
+ * any |d|). */
+int vp_kick(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line,
+            int64_t n_inner, const void* E, int e_dtype, int64_t e_div, double dt, double dv,
+            int32_t window, void* stream);
+
+/* Both kicks of one 2D2V Strang step in one pass over each (x, y) plane:
+ * the vx kick with Ex, then the vy kick with Ey (vlasov2D2V.py:1076-1077).
+ * f is [n_planes][nvx][nvy]; Ex, Ey: double[n_planes].
+ * moments (optional, NULL to skip): double[n_planes][4] per-plane sums
+ *   { sum f_in*(vx^2+vy^2), sum f_out*(vx^2+vy^2), sum f_out^2, sum f_out }
+ * with vx, vy the velocity grids (double[nvx], double[nvy]; required only
+ * with moments). */
+int vp_kick2d(const void* f_in, void* f_out, int dtype, int64_t n_planes, int64_t nvx,
+              int64_t nvy, const double* Ex, const double* Ey, double dt, double dvx,
+              double dvy, int32_t window, const double* vx, const double* vy, double* moments,
+              void* stream);
+
+/* General semi-Lagrangian sweep with a per-element departure point.
+ * Replaces advect_1d / advect_1d_vectorized (vlasov2D2V.py:287-413;
+ * vlasov1D1V.py:212-256): depart = l - (v*dt)/dx, floor/fraction in the
+ * compute type, taps floor+k-2 taken mod n_line (periodic != 0) or masked
+ * to zero outside [0, n_line). The velocity of element (o,l,c) is
+ * vel[o*vs_outer + l*vs_line + c*vs_inner] (compute type). */
+int vp_advect_gather(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line,
+                     int64_t n_inner, const void* vel, int64_t vs_outer, int64_t vs_line,
+                     int64_t vs_inner, double dt, double dx, int periodic, void* stream);
+
+/* ---- moments and field ------------------------------------------------- */
+
+/* Velocity moment. Replaces compute_rho (vlasov2D2V.py:416-431):
+ *   rho[p] = (sum_{c < n_v} f[p*n_v + c]) * dvx * dvy,
+ * summed in FP64 in a fixed order; written as out_dtype (VP_F32/VP_F64). */
+int vp_rho(const void* f, int dtype, int64_t n_points, int64_t n_v, double dvx, double dvy,
+           void* rho, int out_dtype, void* stream);
+
+/* Periodic 2D Poisson solve in FP64. Replaces compute_poisson_real
+ * (vlasov2D2V.py:488-517): delta = rho - 1, phi_k = rfft2(delta)*inv_ksq,
+ * E_k = -i k phi_k, then irfft2 of size (nx, ny) (imaginary parts of the
+ * DC and Nyquist bins of the last axis ignored, as torch.fft does).
+ * kx: double[nx]; ky: double[ny/2+1]; inv_ksq: double[nx][ny/2+1].
+ * Outputs (any may be NULL except ex, ey): ex, ey, drho, phi: double[nx][ny].
+ * energy (optional): double[2] = { 1/2 sum(ex^2+ey^2) dx dy, sum(rho) dx dy }. */
+int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                 const double* inv_ksq, double dx, double dy, double* ex, double* ey,
+                 double* drho, double* phi, double* energy, void* workspace,
+                 size_t workspace_bytes, void* stream);
+size_t vp_poisson2d_workspace_bytes(int64_t nx, int64_t ny);
+
+/* Periodic 1D Poisson solve in FP64 from the density n = sum(f,1)*dv.
+ * Replaces solve_poisson_real (vlasov1D1V.py:538-572) after its sum:
+ * rho = n - 1, E_k = -i rho_k inv_kx, phi_k = rho_k inv_kx_sq, irfft(nx).
+ * inv_kx, inv_kx_sq: double[nx/2+1]. e, rho, phi: double[nx] (rho, phi may
+ * be NULL). energy (optional): double[2] = { 1/2 sum(e^2) dx, sum(n) dx }. */
+int vp_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq,
+                 double dx, double* e, double* rho, double* phi, double* energy,
+                 void* workspace, size_t workspace_bytes, void* stream);
+size_t vp_poisson1d_workspace_bytes(int64_t nx);
+
+/* ---- one Strang step ---------------------------------------------------- */
+
+/* Diagnostics written by the step functions (double[VP_DIAG_COUNT]). */
+#define VP_DIAG_FIELD_ENERGY 0 /* 1/2 sum |E|^2 dx (dy): mid-step field */
+#define VP_DIAG_MASS 1         /* sum n dx (dy), n the mid-step density */
+#define VP_DIAG_L2 2           /* sum f^2 dV after the kick(s) */
+#define VP_DIAG_KINETIC 3      /* 1/2 sum f |v|^2 dV after the kick(s) */
+#define VP_DIAG_KINETIC_PRE 4  /* 1/2 sum f |v|^2 dV before the kick(s) */
+#define VP_DIAG_MAX_SHIFT 5    /* max |E| dt/dv over both kicks, in cells */
+#define VP_DIAG_COUNT 8
+
+/* Phases of a step, for the optional timing events of the step descriptors:
+ * events[2p] is recorded on the stream before phase p, events[2p+1] after
+ * it (cudaEvent_t handles created by the caller; both at the same point
+ * when a phase does not run). */
+#define VP_PHASE_DRIFT_X1 0  /* 1D1V: the first x drift fused with n */
+#define VP_PHASE_DRIFT_Y1 1  /* y drift fused with rho (2D2V only) */
+#define VP_PHASE_FIELD 2     /* Poisson solve */
+#define VP_PHASE_KICK 3      /* vx+vy kick (2D2V), v kick (1D1V) */
+#define VP_PHASE_DRIFT_Y2 4  /* 2D2V only */
+#define VP_PHASE_DRIFT_X2 5
+#define VP_PHASE_DIAG 6
+#define VP_PHASE_COUNT 7
+
+/* One Strang step of the 2D2V system, the schedule of
+ * vlasov_step_gather_free_impl (vlasov2D2V.py:1043-1083):
+ * x(dt/2), y(dt/2) fused with rho, Poisson, vx(dt)+vy(dt) fused,
+ * y(dt/2), x(dt/2). With physics_mode == 0 the field is zero, the kicks are
+ * the identity and are skipped, and drho/phi are zeroed (as the reference
+ * returns zeros). f_in is read only; the result is written to f_out;
+ * f_tmp is a third buffer of the same size. Buffers must not overlap. */
+typedef struct vp_step2d_desc {
+    int32_t dtype;
+    int64_t nx, ny, nvx, nvy;
+    double dt, dx, dy, dvx, dvy;
+    int32_t physics_mode;
+    int32_t window;        /* kick window S (<0: exact kick) */
+    int32_t diagnostics;   /* nonzero: fill diag[] (moments add one FP64 pass in the kick) */
+    const void* f_in;
+    void* f_out;
+    void* f_tmp;
+    const int32_t* shift_x; /* [nvx] */
+    const void* W_x;        /* compute type [6][nvx] */
+    const int32_t* shift_y; /* [nvy] */
+    const void* W_y;        /* compute type [6][nvy] */
+    const double* kx;       /* [nx] */
+    const double* ky;       /* [ny/2+1] */
+    const double* inv_ksq;  /* [nx][ny/2+1] */
+    const double* vx;       /* [nvx] (diagnostics only) */
+    const double* vy;       /* [nvy] (diagnostics only) */
+    double* drho;           /* [nx][ny] mid-step rho - 1 (may be NULL) */
+    double* phi;            /* [nx][ny] mid-step potential (may be NULL) */
+    double* ex;             /* [nx][ny] mid-step field (may be NULL) */
+    double* ey;             /* [nx][ny] (may be NULL) */
+    double* diag;           /* [VP_DIAG_COUNT] (may be NULL) */
+    void* workspace;
+    size_t workspace_bytes;
+    void* const* events;    /* optional [2*VP_PHASE_COUNT] cudaEvent_t, NULL to skip */
+} vp_step2d_desc;
+
+int vp_step2d(const vp_step2d_desc* desc, void* stream);
+size_t vp_step2d_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy);
+
+/* One Strang step of the 1D1V system, the schedule of
+ * vlasov_step_gather_free_impl (vlasov1D1V.py:668-701): x(dt/2) fused with
+ * n, Poisson, v(dt), x(dt/2). rho, phi, e are the mid-step fields. */
+typedef struct vp_step1d_desc {
+    int32_t dtype;
+    int64_t nx, nv;
+    double dt, dx, dv;
+    int32_t physics_mode;
+    int32_t window;
+    int32_t diagnostics;
+    const void* f_in;
+    void* f_out;
+    void* f_tmp;
+    const int32_t* shift; /* [nv] */
+    const void* W;        /* compute type [6][nv] */
+    const double* inv_kx;    /* [nx/2+1] */
+    const double* inv_kx_sq; /* [nx/2+1] */
+    const double* v;         /* [nv] (diagnostics only) */
+    double* rho;
+    double* phi;
+    double* e;
+    double* diag;
+    void* workspace;
+    size_t workspace_bytes;
+    void* const* events; /* optional [2*VP_PHASE_COUNT] cudaEvent_t */
+} vp_step1d_desc;
+
+int vp_step1d(const vp_step1d_desc* desc, void* stream);
+size_t vp_step1d_workspace_bytes(int64_t nx, int64_t nv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VLASOV_B200_H */

@@ -1,0 +1,524 @@
+// FP64 periodic Poisson solves of the Vlasov-Poisson step.
+//
+// 2D (compute_poisson_real, vlasov2D2V.py:488-517): three small kernels,
+//   rows:    delta = rho - 1, real DFT along y      -> R[x][ky]     (ky <= Ny/2)
+//   columns: DFT along x, phi_k = R_k*inv_ksq, E_k = -i k phi_k,
+//            inverse DFT along x of phi_k, Ex_k, Ey_k -> Z*[x][ky]
+//   rows:    complex-to-real inverse along y (imaginary parts of the DC and
+//            Nyquist bins ignored, like torch.fft.irfft2) -> phi, Ex, Ey
+// Each line transform is a direct DFT over a shared-memory twiddle table
+// (sincospi of exact fractions), O(N) per output, any N. At 128x128 the whole
+// solve is ~1 MFLOP per launch and not worth an FFT.
+//
+// 1D (solve_poisson_real, vlasov1D1V.py:538-572): one block. Power-of-two
+// lengths use an in-shared-memory radix-2 FFT (Nx = 4096 would cost ~17
+// MFLOP as a DFT); E and phi come out of ONE inverse transform of
+// E_k + i*phi_k (both are real signals).
+//
+// Reductions (field energy, mass) use per-line partials summed in a fixed
+// order by one block: results are bitwise reproducible run to run.
+#include <algorithm>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace vp {
+
+constexpr int kPBlock = 256;
+
+// twiddle table tw[j] = exp(+2 pi i j / n), j < n
+__device__ __forceinline__ void fill_twiddles(double2* tw, int n) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double s, c;
+        sincospi(2.0 * (double)j / (double)n, &s, &c);
+        tw[j] = make_double2(c, s);
+    }
+}
+
+// fixed-order block sum (blockDim.x a power of two, scratch >= blockDim.x)
+__device__ double block_sum(double v, double* scratch) {
+    scratch[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
+        if (threadIdx.x < off) scratch[threadIdx.x] += scratch[threadIdx.x + off];
+        __syncthreads();
+    }
+    const double r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ double block_max(double v, double* scratch) {
+    scratch[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
+        if (threadIdx.x < off) scratch[threadIdx.x] = fmax(scratch[threadIdx.x], scratch[threadIdx.x + off]);
+        __syncthreads();
+    }
+    const double r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// ---- 2D: rows, forward ------------------------------------------------------
+__global__ void __launch_bounds__(kPBlock) k_p2_rows_fwd(const double* __restrict__ rho, int nx, int ny,
+                                                       double* __restrict__ drho, double2* __restrict__ R,
+                                                       double* __restrict__ mass_part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* tw = reinterpret_cast<double2*>(smem_raw);
+    double* row = reinterpret_cast<double*>(tw + ny);
+    double* scratch = row + ny;
+    const int ix = blockIdx.x;
+    const int nyh = ny / 2 + 1;
+    fill_twiddles(tw, ny);
+    double m = 0.0;
+    for (int iy = threadIdx.x; iy < ny; iy += blockDim.x) {
+        const double v = rho[(int64_t)ix * ny + iy];
+        const double d = v - 1.0;
+        row[iy] = d;
+        if (drho) drho[(int64_t)ix * ny + iy] = d;
+        m += v;
+    }
+    m = block_sum(m, scratch);
+    if (threadIdx.x == 0 && mass_part) mass_part[ix] = m;
+    for (int ky = threadIdx.x; ky < nyh; ky += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        int idx = 0;
+        for (int iy = 0; iy < ny; ++iy) {
+            const double2 t = tw[idx];
+            re = fma(row[iy], t.x, re);
+            im = fma(-row[iy], t.y, im);
+            idx += ky;
+            if (idx >= ny) idx -= ny;
+        }
+        R[(int64_t)ix * nyh + ky] = make_double2(re, im);
+    }
+}
+
+// ---- 2D: columns ------------------------------------------------------------
+__global__ void __launch_bounds__(kPBlock) k_p2_cols(const double2* __restrict__ R, int nx, int ny,
+                                                   const double* __restrict__ kx, const double* __restrict__ ky,
+                                                   const double* __restrict__ inv_ksq, double2* __restrict__ Zp,
+                                                   double2* __restrict__ Zx, double2* __restrict__ Zy) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nyh = ny / 2 + 1;
+    double2* tw = reinterpret_cast<double2*>(smem_raw);
+    double2* col = tw + nx;
+    double2* P = col + nx;
+    double2* X = P + nx;
+    double2* Y = X + nx;
+    const int k = blockIdx.x;  // ky index
+    fill_twiddles(tw, nx);
+    for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) col[ix] = R[(int64_t)ix * nyh + k];
+    __syncthreads();
+    const double kyv = ky[k];
+    for (int q = threadIdx.x; q < nx; q += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        int idx = 0;
+        for (int ix = 0; ix < nx; ++ix) {
+            const double2 t = tw[idx];
+            const double2 c = col[ix];
+            // c * conj(t)
+            re = fma(c.x, t.x, fma(c.y, t.y, re));
+            im = fma(c.y, t.x, fma(-c.x, t.y, im));
+            idx += q;
+            if (idx >= nx) idx -= nx;
+        }
+        const double inv = inv_ksq[(int64_t)q * nyh + k];
+        const double pr = re * inv, pi = im * inv;
+        const double kxv = kx[q];
+        P[q] = make_double2(pr, pi);
+        X[q] = make_double2(pi * kxv, -pr * kxv);
+        Y[q] = make_double2(pi * kyv, -pr * kyv);
+    }
+    __syncthreads();
+    const double sc = 1.0 / (double)nx;
+    for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) {
+        double pr = 0.0, pi = 0.0, xr = 0.0, xi = 0.0, yr = 0.0, yi = 0.0;
+        int idx = 0;
+        for (int q = 0; q < nx; ++q) {
+            const double2 t = tw[idx];
+            const double2 a = P[q], b = X[q], c = Y[q];
+            pr = fma(a.x, t.x, fma(-a.y, t.y, pr));
+            pi = fma(a.y, t.x, fma(a.x, t.y, pi));
+            xr = fma(b.x, t.x, fma(-b.y, t.y, xr));
+            xi = fma(b.y, t.x, fma(b.x, t.y, xi));
+            yr = fma(c.x, t.x, fma(-c.y, t.y, yr));
+            yi = fma(c.y, t.x, fma(c.x, t.y, yi));
+            idx += ix;
+            if (idx >= nx) idx -= nx;
+        }
+        const int64_t o = (int64_t)ix * nyh + k;
+        Zp[o] = make_double2(pr * sc, pi * sc);
+        Zx[o] = make_double2(xr * sc, xi * sc);
+        Zy[o] = make_double2(yr * sc, yi * sc);
+    }
+}
+
+// ---- 2D: rows, complex-to-real inverse ------------------------------------------
+__global__ void __launch_bounds__(kPBlock) k_p2_rows_inv(const double2* __restrict__ Zp,
+                                                       const double2* __restrict__ Zx,
+                                                       const double2* __restrict__ Zy, int nx, int ny,
+                                                       double* __restrict__ phi, double* __restrict__ ex,
+                                                       double* __restrict__ ey, double* __restrict__ we_part,
+                                                       double* __restrict__ emax_part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nyh = ny / 2 + 1;
+    double2* tw = reinterpret_cast<double2*>(smem_raw);
+    double2* zp = tw + ny;
+    double2* zx = zp + nyh;
+    double2* zy = zx + nyh;
+    double* scratch = reinterpret_cast<double*>(zy + nyh);
+    const int ix = blockIdx.x;
+    fill_twiddles(tw, ny);
+    for (int q = threadIdx.x; q < nyh; q += blockDim.x) {
+        const int64_t o = (int64_t)ix * nyh + q;
+        zp[q] = Zp[o];
+        zx[q] = Zx[o];
+        zy[q] = Zy[o];
+    }
+    __syncthreads();
+    const bool even = (ny % 2) == 0;
+    const int last = (ny - 1) / 2;  // last bin that appears twice
+    const double sc = 1.0 / (double)ny;
+    double we = 0.0, exm = 0.0, eym = 0.0;
+    for (int iy = threadIdx.x; iy < ny; iy += blockDim.x) {
+        double sp = 0.0, sx = 0.0, sy = 0.0;
+        int idx = iy;
+        for (int q = 1; q <= last; ++q) {
+            const double2 t = tw[idx];
+            sp = fma(zp[q].x, t.x, fma(-zp[q].y, t.y, sp));
+            sx = fma(zx[q].x, t.x, fma(-zx[q].y, t.y, sx));
+            sy = fma(zy[q].x, t.x, fma(-zy[q].y, t.y, sy));
+            idx += iy;
+            if (idx >= ny) idx -= ny;
+        }
+        double vp = zp[0].x + 2.0 * sp, vx = zx[0].x + 2.0 * sx, vy = zy[0].x + 2.0 * sy;
+        if (even) {
+            const double sgn = (iy & 1) ? -1.0 : 1.0;
+            vp += sgn * zp[ny / 2].x;
+            vx += sgn * zx[ny / 2].x;
+            vy += sgn * zy[ny / 2].x;
+        }
+        vp *= sc;
+        vx *= sc;
+        vy *= sc;
+        const int64_t o = (int64_t)ix * ny + iy;
+        if (phi) phi[o] = vp;
+        if (ex) ex[o] = vx;
+        if (ey) ey[o] = vy;
+        we = fma(vx, vx, fma(vy, vy, we));
+        exm = fmax(exm, fabs(vx));
+        eym = fmax(eym, fabs(vy));
+    }
+    we = block_sum(we, scratch);
+    exm = block_max(exm, scratch);
+    eym = block_max(eym, scratch);
+    if (threadIdx.x == 0) {
+        if (we_part) we_part[ix] = we;
+        if (emax_part) {
+            emax_part[2 * ix] = exm;
+            emax_part[2 * ix + 1] = eym;
+        }
+    }
+}
+
+// ---- diagnostics finalize (one block, fixed order) -------------------------------
+struct DiagArgs {
+    const double* mass_part;  // [n_mass]
+    int n_mass;
+    const double* we_part;  // [n_we]
+    int n_we;
+    const double* emax_part;  // [n_emax][2]
+    int n_emax;
+    const double* moments;  // [n_mom][4]
+    int64_t n_mom;
+    double mass_scale, we_scale, dv_scale;  // dx*dy, 0.5*dx*dy, dV
+    double shift_x, shift_y;                // dt/dvx, dt/dvy
+    double* energy;                         // optional [2]: {W_E, mass}
+    double* diag;                           // optional [VP_DIAG_COUNT]
+};
+
+__global__ void __launch_bounds__(kPBlock) k_diag_finalize(DiagArgs a) {
+    __shared__ double scratch[kPBlock];
+    double m = 0.0, w = 0.0, ex = 0.0, ey = 0.0, pre = 0.0, post = 0.0, l2 = 0.0;
+    for (int i = threadIdx.x; i < a.n_mass; i += blockDim.x) m += a.mass_part[i];
+    for (int i = threadIdx.x; i < a.n_we; i += blockDim.x) w += a.we_part[i];
+    for (int i = threadIdx.x; i < a.n_emax; i += blockDim.x) {
+        ex = fmax(ex, a.emax_part[2 * i]);
+        ey = fmax(ey, a.emax_part[2 * i + 1]);
+    }
+    for (int64_t i = threadIdx.x; i < a.n_mom; i += blockDim.x) {
+        pre += a.moments[4 * i + 0];
+        post += a.moments[4 * i + 1];
+        l2 += a.moments[4 * i + 2];
+    }
+    m = block_sum(m, scratch);
+    w = block_sum(w, scratch);
+    ex = block_max(ex, scratch);
+    ey = block_max(ey, scratch);
+    pre = block_sum(pre, scratch);
+    post = block_sum(post, scratch);
+    l2 = block_sum(l2, scratch);
+    if (threadIdx.x == 0) {
+        const double we = w * a.we_scale, mass = m * a.mass_scale;
+        if (a.energy) {
+            a.energy[0] = we;
+            a.energy[1] = mass;
+        }
+        if (a.diag) {
+            const double nan = __longlong_as_double(0x7ff8000000000000ULL);
+            a.diag[VP_DIAG_FIELD_ENERGY] = a.n_we ? we : 0.0;
+            a.diag[VP_DIAG_MASS] = a.n_mass ? mass : nan;
+            a.diag[VP_DIAG_L2] = a.n_mom ? l2 * a.dv_scale : nan;
+            a.diag[VP_DIAG_KINETIC] = a.n_mom ? 0.5 * post * a.dv_scale : nan;
+            a.diag[VP_DIAG_KINETIC_PRE] = a.n_mom ? 0.5 * pre * a.dv_scale : nan;
+            a.diag[VP_DIAG_MAX_SHIFT] = a.n_emax ? fmax(ex * a.shift_x, ey * a.shift_y) : 0.0;
+            a.diag[6] = 0.0;
+            a.diag[7] = 0.0;
+        }
+    }
+}
+
+// ---- 2D host ------------------------------------------------------------------
+struct Pois2dWs {
+    double2 *R, *Zp, *Zx, *Zy;
+    double *mass_part, *we_part, *emax_part;
+};
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+static size_t pois2d_layout(int64_t nx, int64_t ny, char* base, Pois2dWs* w) {
+    const int64_t nyh = ny / 2 + 1;
+    const size_t cplx = align256((size_t)nx * nyh * sizeof(double2));
+    const size_t line = align256((size_t)nx * sizeof(double));
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* p = base ? base + off : nullptr;
+        off += b;
+        return p;
+    };
+    Pois2dWs t;
+    t.R = reinterpret_cast<double2*>(take(cplx));
+    t.Zp = reinterpret_cast<double2*>(take(cplx));
+    t.Zx = reinterpret_cast<double2*>(take(cplx));
+    t.Zy = reinterpret_cast<double2*>(take(cplx));
+    t.mass_part = reinterpret_cast<double*>(take(line));
+    t.we_part = reinterpret_cast<double*>(take(line));
+    t.emax_part = reinterpret_cast<double*>(take(2 * line));
+    if (w) *w = t;
+    return off;
+}
+
+size_t poisson2d_ws_bytes(int64_t nx, int64_t ny) { return pois2d_layout(nx, ny, nullptr, nullptr); }
+
+static int set_smem(const void* kern, size_t smem) {
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return set_cuda_error("cudaFuncSetAttribute(poisson)");
+    return VP_OK;
+}
+
+// Launches the three transform kernels; partials stay in the workspace.
+int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                  const double* inv_ksq, double* ex, double* ey, double* drho, double* phi, void* ws,
+                  Pois2dWsView* view, cudaStream_t st) {
+    Pois2dWs w;
+    pois2d_layout(nx, ny, static_cast<char*>(ws), &w);
+    const int64_t nyh = ny / 2 + 1;
+    int rc;
+    const size_t s1 = ny * sizeof(double2) + ny * sizeof(double) + kPBlock * sizeof(double);
+    if ((rc = set_smem((const void*)k_p2_rows_fwd, s1))) return rc;
+    k_p2_rows_fwd<<<(unsigned)nx, kPBlock, s1, st>>>(rho, (int)nx, (int)ny, drho, w.R, w.mass_part);
+    if ((rc = check_launch("k_p2_rows_fwd"))) return rc;
+    const size_t s2 = 5 * nx * sizeof(double2);
+    if ((rc = set_smem((const void*)k_p2_cols, s2))) return rc;
+    k_p2_cols<<<(unsigned)nyh, kPBlock, s2, st>>>(w.R, (int)nx, (int)ny, kx, ky, inv_ksq, w.Zp, w.Zx, w.Zy);
+    if ((rc = check_launch("k_p2_cols"))) return rc;
+    const size_t s3 = ny * sizeof(double2) + 3 * nyh * sizeof(double2) + kPBlock * sizeof(double);
+    if ((rc = set_smem((const void*)k_p2_rows_inv, s3))) return rc;
+    k_p2_rows_inv<<<(unsigned)nx, kPBlock, s3, st>>>(w.Zp, w.Zx, w.Zy, (int)nx, (int)ny, phi, ex, ey, w.we_part,
+                                                     w.emax_part);
+    if ((rc = check_launch("k_p2_rows_inv"))) return rc;
+    if (view) {
+        view->mass_part = w.mass_part;
+        view->we_part = w.we_part;
+        view->emax_part = w.emax_part;
+        view->n_lines = (int)nx;
+    }
+    return VP_OK;
+}
+
+int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_mom, double mass_scale,
+                      double we_scale, double dv_scale, double shift_x, double shift_y, double* energy,
+                      double* diag, cudaStream_t st) {
+    DiagArgs a{};
+    a.mass_part = pv.mass_part;
+    a.n_mass = pv.mass_part ? pv.n_lines : 0;
+    a.we_part = pv.we_part;
+    a.n_we = pv.we_part ? pv.n_lines : 0;
+    a.emax_part = pv.emax_part;
+    a.n_emax = pv.emax_part ? pv.n_lines : 0;
+    a.moments = moments;
+    a.n_mom = moments ? n_mom : 0;
+    a.mass_scale = mass_scale;
+    a.we_scale = we_scale;
+    a.dv_scale = dv_scale;
+    a.shift_x = shift_x;
+    a.shift_y = shift_y;
+    a.energy = energy;
+    a.diag = diag;
+    k_diag_finalize<<<1, kPBlock, 0, st>>>(a);
+    return check_launch("k_diag_finalize");
+}
+
+// ---- 1D ----------------------------------------------------------------------
+// In-place radix-2 complex FFT of x[0..n) in shared memory, sign = -1 forward
+// (exp(-2 pi i jk/n)), +1 inverse (unscaled). tw[j] = exp(+2 pi i j/n), j < n/2.
+__device__ void fft_radix2(double2* x, const double2* tw, int n, int logn, int sign) {
+    if (logn == 0) return;  // length 1: identity
+    // bit-reversal permutation
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int j = (int)(__brev((unsigned)i) >> (32 - logn));
+        if (j > i) {
+            const double2 t = x[i];
+            x[i] = x[j];
+            x[j] = t;
+        }
+    }
+    __syncthreads();
+    for (int s = 1; s <= logn; ++s) {
+        const int m = 1 << s, half = m >> 1;
+        const int tstride = n / m;
+        for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
+            const int grp = b / half, pos = b % half;
+            const int i0 = grp * m + pos, i1 = i0 + half;
+            double2 t = tw[pos * tstride];
+            t.y *= sign;
+            const double2 u = x[i0], v = x[i1];
+            const double2 tv = make_double2(v.x * t.x - v.y * t.y, v.x * t.y + v.y * t.x);
+            x[i0] = make_double2(u.x + tv.x, u.y + tv.y);
+            x[i1] = make_double2(u.x - tv.x, u.y - tv.y);
+        }
+        __syncthreads();
+    }
+}
+
+// Direct DFT variant for lengths that are not powers of two: y = sum x w^(sign jk)
+__device__ void dft_direct(const double2* x, double2* y, const double2* tw, int n, int sign) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        int idx = 0;
+        for (int j = 0; j < n; ++j) {
+            double2 t = tw[idx];
+            t.y *= sign;
+            re = fma(x[j].x, t.x, fma(-x[j].y, t.y, re));
+            im = fma(x[j].y, t.x, fma(x[j].x, t.y, im));
+            idx += k;
+            if (idx >= n) idx -= n;
+        }
+        y[k] = make_double2(re, im);
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_p1(const double* __restrict__ nrho, int nx,
+                                            const double* __restrict__ inv_kx,
+                                            const double* __restrict__ inv_kx_sq, double* __restrict__ e,
+                                            double* __restrict__ rho_out, double* __restrict__ phi,
+                                            double* __restrict__ parts /* [3]: mass, we, emax */) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* tw = reinterpret_cast<double2*>(smem_raw);  // n entries
+    double2* a = tw + nx;
+    double2* b = a + nx;
+    double* scratch = reinterpret_cast<double*>(b + nx);
+    const int n = nx;
+    int logn = 0;
+    while ((1 << logn) < n) ++logn;
+    const bool pow2 = (1 << logn) == n;
+    fill_twiddles(tw, n);
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = nrho[i];
+        m += v;
+        const double r = v - 1.0;
+        if (rho_out) rho_out[i] = r;
+        a[i] = make_double2(r, 0.0);
+    }
+    m = block_sum(m, scratch);
+    __syncthreads();
+    double2* spec;
+    if (pow2) {
+        fft_radix2(a, tw, n, logn, -1);
+        spec = a;
+    } else {
+        dft_direct(a, b, tw, n, -1);
+        __syncthreads();
+        spec = b;
+    }
+    // Build the hermitian spectrum of E_k + i*phi_k (bins 0..n/2 from the
+    // half spectrum, imaginary parts of DC and Nyquist dropped as c2r does).
+    double2* z = (spec == a) ? b : a;
+    const int nh = n / 2 + 1;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int kk = k < nh ? k : n - k;  // mirror
+        const double2 r = spec[kk];
+        // E_k = (im*ik, -re*ik); phi_k = (re*ik2, im*ik2)
+        double er = r.y * inv_kx[kk], ei = -r.x * inv_kx[kk];
+        double pr = r.x * inv_kx_sq[kk], pi = r.y * inv_kx_sq[kk];
+        if (kk == 0 || (n % 2 == 0 && kk == n / 2)) {
+            ei = 0.0;
+            pi = 0.0;
+        }
+        if (k >= nh) {  // conjugate of the mirrored bin
+            ei = -ei;
+            pi = -pi;
+        }
+        // Z = E + i*phi
+        z[k] = make_double2(er - pi, ei + pr);
+    }
+    __syncthreads();
+    double2* res;
+    if (pow2) {
+        fft_radix2(z, tw, n, logn, +1);
+        res = z;
+    } else {
+        double2* y = (z == a) ? b : a;
+        dft_direct(z, y, tw, n, +1);
+        __syncthreads();
+        res = y;
+    }
+    const double sc = 1.0 / (double)n;
+    double we = 0.0, em = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double ev = res[i].x * sc, pv = res[i].y * sc;
+        e[i] = ev;
+        if (phi) phi[i] = pv;
+        we = fma(ev, ev, we);
+        em = fmax(em, fabs(ev));
+    }
+    we = block_sum(we, scratch);
+    em = block_max(em, scratch);
+    if (threadIdx.x == 0 && parts) {
+        parts[0] = m;
+        parts[1] = we;
+        parts[2] = em;
+        parts[3] = 0.0;
+    }
+}
+
+size_t poisson1d_ws_bytes(int64_t nx) {
+    (void)nx;
+    return 256;
+}
+
+int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double* e,
+                  double* rho, double* phi, double* parts, cudaStream_t st) {
+    const size_t smem = 3 * (size_t)nx * sizeof(double2) + 1024 * sizeof(double);
+    if (smem > 220 * 1024) return set_error(VP_ERR_UNSUPPORTED, "1D Poisson: nx too large for one block");
+    int rc;
+    if ((rc = set_smem((const void*)k_p1, smem))) return rc;
+    k_p1<<<1, 1024, smem, st>>>(n, (int)nx, inv_kx, inv_kx_sq, e, rho, phi, parts);
+    return check_launch("k_p1");
+}
+
+}  // namespace vp

@@ -8,6 +8,7 @@
  * routines and the reference lines each one follows.
  */
 #include <math.h>
+#include <stdlib.h>
 #include <stdint.h>
 
 #define REAL double

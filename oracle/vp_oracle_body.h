@@ -52,22 +52,57 @@ void CAT(or_lagrange5_weights_, SFX)(const REAL* alpha, int64_t n, REAL* w /* [6
 void CAT(or_drift_static_, SFX)(const REAL* in, REAL* out, int64_t n_outer, int64_t n_line,
                                 int64_t n_inner, int64_t sel_div, int64_t sel_mod,
                                 const int64_t* shift, const REAL* W /* [6][sel_mod] */) {
-#pragma omp parallel for collapse(2) schedule(static)
-    for (int64_t o = 0; o < n_outer; ++o) {
-        for (int64_t l = 0; l < n_line; ++l) {
-            const REAL* src = in + o * n_line * n_inner;
-            REAL* dst = out + (o * n_line + l) * n_inner;
-            for (int64_t c = 0; c < n_inner; ++c) {
-                int64_t j = (c / sel_div) % sel_mod;
-                REAL acc = (REAL)0;
-                for (int k = 0; k < 6; ++k) {
-                    int64_t r = (l - shift[j] - (k - 2)) % n_line;
-                    if (r < 0) r += n_line;
-                    acc = acc + src[r * n_inner + c] * W[k * sel_mod + j];
+    /* Columns with the same table entry j form runs of sel_div contiguous
+     * elements; per output row the 6 source rows of each j are resolved
+     * once, and the arithmetic of every element is the reference's. */
+    const int64_t period = sel_div * sel_mod;
+    const int blocked = (n_inner % period) == 0;
+#pragma omp parallel
+    {
+        int64_t* rows = (int64_t*)malloc(sizeof(int64_t) * 6 * (size_t)sel_mod);
+#pragma omp for collapse(2) schedule(static)
+        for (int64_t o = 0; o < n_outer; ++o) {
+            for (int64_t l = 0; l < n_line; ++l) {
+                const REAL* src = in + o * n_line * n_inner;
+                REAL* dst = out + (o * n_line + l) * n_inner;
+                for (int64_t j = 0; j < sel_mod; ++j) {
+                    for (int k = 0; k < 6; ++k) {
+                        int64_t r = (l - shift[j] - (k - 2)) % n_line;
+                        rows[j * 6 + k] = (r < 0 ? r + n_line : r) * n_inner;
+                    }
                 }
-                dst[c] = acc;
+                if (blocked) {
+                    for (int64_t q = 0; q < n_inner; q += period) {
+                        for (int64_t j = 0; j < sel_mod; ++j) {
+                            const int64_t* rj = rows + j * 6;
+                            const REAL w0 = W[0 * sel_mod + j], w1 = W[1 * sel_mod + j], w2 = W[2 * sel_mod + j];
+                            const REAL w3 = W[3 * sel_mod + j], w4 = W[4 * sel_mod + j], w5 = W[5 * sel_mod + j];
+                            const int64_t c0 = q + j * sel_div;
+                            const REAL *s0 = src + rj[0], *s1 = src + rj[1], *s2 = src + rj[2];
+                            const REAL *s3 = src + rj[3], *s4 = src + rj[4], *s5 = src + rj[5];
+                            for (int64_t c = c0; c < c0 + sel_div; ++c) {
+                                REAL acc = (REAL)0;
+                                acc = acc + s0[c] * w0;
+                                acc = acc + s1[c] * w1;
+                                acc = acc + s2[c] * w2;
+                                acc = acc + s3[c] * w3;
+                                acc = acc + s4[c] * w4;
+                                acc = acc + s5[c] * w5;
+                                dst[c] = acc;
+                            }
+                        }
+                    }
+                } else {
+                    for (int64_t c = 0; c < n_inner; ++c) {
+                        const int64_t j = (c / sel_div) % sel_mod;
+                        REAL acc = (REAL)0;
+                        for (int k = 0; k < 6; ++k) acc = acc + src[rows[j * 6 + k] + c] * W[k * sel_mod + j];
+                        dst[c] = acc;
+                    }
+                }
             }
         }
+        free(rows);
     }
 }
 
@@ -92,16 +127,18 @@ void CAT(or_kick_static_, SFX)(const REAL* in, REAL* out, int64_t n_outer, int64
         const REAL* src = in + o * n_line * n_inner;
         REAL* dst = out + o * n_line * n_inner;
         for (int64_t l = 0; l < n_line; ++l) {
-            for (int64_t c = 0; c < n_inner; ++c) {
-                REAL acc = (REAL)0;
-                for (int k = 0; k < 6; ++k) {
-                    int64_t m = s + (k - 2);
-                    if (window >= 0 && (m < -window - 2 || m > window + 2)) continue;
-                    int64_t r = l - m;
-                    REAL v = (r >= 0 && r < n_line) ? src[r * n_inner + c] : (REAL)0;
-                    acc = acc + w[k] * v;
-                }
-                dst[l * n_inner + c] = acc;
+            REAL* drow = dst + l * n_inner;
+            for (int64_t c = 0; c < n_inner; ++c) drow[c] = (REAL)0;
+            /* taps in ascending order; a tap outside the line reads the zero
+             * padding and leaves every element unchanged */
+            for (int k = 0; k < 6; ++k) {
+                const int64_t m = s + (k - 2);
+                if (window >= 0 && (m < -window - 2 || m > window + 2)) continue;
+                const int64_t r = l - m;
+                if (r < 0 || r >= n_line) continue;
+                const REAL* srow = src + r * n_inner;
+                const REAL wk = w[k];
+                for (int64_t c = 0; c < n_inner; ++c) drow[c] = drow[c] + wk * srow[c];
             }
         }
     }

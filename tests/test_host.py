@@ -1,0 +1,121 @@
+"""Host-side logic that needs no GPU: static drift tables, argument checks of
+the tensor API, velocity-layout classification, snapshot files, and the
+multi-process plumbing on gloo (world size 2)."""
+import importlib
+import math
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+from conftest import PACKAGE, ROOT
+
+
+@pytest.mark.parametrize("tag", ["c1", "c2", "c3", "ref128", "oned4096"])
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_drift_tables_match_reference(vp, golden, tag, dt):
+    """The library's drift tables equal precompute_x_drift's bit for bit."""
+    t = golden("tables")
+    n, vmax, dx, half_dt = t[f"{tag}_{dt}_meta"]
+    tdt = torch.float64 if dt == "f64" else torch.float32
+    s, W = vp.ops.drift_table_np(torch.from_numpy(t[f"{tag}_{dt}_v"]), half_dt, dx, tdt)
+    np.testing.assert_array_equal(s, t[f"{tag}_{dt}_shift"])
+    np.testing.assert_array_equal(W, t[f"{tag}_{dt}_W"])
+    v2 = importlib.import_module(PACKAGE + ".vlasov2d2v")
+    blocks, Wt = v2.precompute_x_drift(torch.from_numpy(t[f"{tag}_{dt}_v"]), half_dt, dx, tdt)
+    np.testing.assert_array_equal(v2._blocks_to_shift(blocks, int(n)), t[f"{tag}_{dt}_shift"])
+    np.testing.assert_array_equal(Wt.numpy(), t[f"{tag}_{dt}_W"])
+
+
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_lagrange_weights_host(vp, golden, dt):
+    t = golden("tables")
+    a = t["alpha"].astype(np.float64 if dt == "f64" else np.float32)
+    np.testing.assert_array_equal(vp.ops.lagrange5_weights_np(a), t[f"lag5_{dt}"])
+
+
+def test_tensor_api_rejects_cpu_tensors(vp):
+    f = torch.zeros(4, 4, 4, 4)
+    table = type("T", (), {"n": 4, "shift": torch.zeros(4, dtype=torch.int32), "W": torch.zeros(6, 4)})()
+    with pytest.raises(ValueError, match="CUDA"):
+        vp.ops.drift(f, table, 0, 2)
+    with pytest.raises(ValueError, match="CUDA"):
+        vp.ops.kick(f, torch.zeros(4, 4), 0.1, 0.1, 2)
+    with pytest.raises(ValueError, match="CUDA"):
+        vp.ops.velocity_moment(f, 1.0, 1.0, 2)
+    with pytest.raises(TypeError):
+        vp._lib.dtype_code(torch.int32)
+
+
+def test_stepper_requires_cuda(vp):
+    with pytest.raises(ValueError):
+        vp.Stepper2D(4, 4, 4, 4, 1.0, 1.0, 1.0, 1.0, 0.1, device="cpu")
+
+
+def test_velocity_layout_classification(vp):
+    v2 = importlib.import_module(PACKAGE + ".vlasov2d2v")
+    f = torch.zeros(3, 4, 5, 6)
+    k = v2._line_velocity_structure(f, torch.arange(5.0)[None, :, None], 0)
+    assert k[0] == "drift" and k[1] == 2 and k[2].numel() == 5
+    k = v2._line_velocity_structure(f, torch.arange(6.0)[None, None, :], 1)
+    assert k[0] == "drift" and k[1] == 3
+    k = v2._line_velocity_structure(f, torch.zeros(3, 4)[:, :, None], 2)
+    assert k[0] == "kick" and tuple(k[1].shape) == (3, 4)
+    k = v2._line_velocity_structure(f, torch.zeros(3, 4)[:, :, None], 3)
+    assert k[0] == "kick" and tuple(k[1].shape) == (3, 4, 5)
+    assert v2._line_velocity_structure(f, torch.zeros(4, 5, 6), 0) is None
+
+
+def test_stencil_offsets_checked(vp):
+    v2 = importlib.import_module(PACKAGE + ".vlasov2d2v")
+    v2._check_offsets(torch.arange(-2, 4))
+    with pytest.raises(NotImplementedError):
+        v2._check_offsets(torch.arange(-3, 3))
+
+
+def test_snapshot_raw_round_trip(vp, tmp_path):
+    snap = importlib.import_module(PACKAGE + ".snapshot")
+    a = np.random.default_rng(0).random((3, 4, 5)).astype(np.float32)
+    snap.write_raw(tmp_path, 7, fn=a, rho=a[0])
+    b = snap.read_raw(tmp_path / "fn_000007.bin", a.shape, np.float32)
+    np.testing.assert_array_equal(a, b)
+    assert (tmp_path / "rho_000007.bin").stat().st_size == a[0].nbytes
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    import sys
+
+    sys.path.insert(0, ROOT)
+    dist = importlib.import_module(PACKAGE + ".dist")
+    r, _, w = dist.init(backend="gloo", timeout_s=60)
+    dist.barrier()
+    mx = dist.max_over_ranks(10.0 + r)
+    sm = dist.sum_over_ranks(1.0)
+    out[r] = (w, mx, sm)
+    dist.finalize()
+
+
+def test_dist_gloo_world2():
+    """bench.py's multi-rank timing: max over ranks, sum, barrier (gloo, CPU)."""
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    assert out[0] == (2, 11.0, 2.0) and out[1] == (2, 11.0, 2.0)
