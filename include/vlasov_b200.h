@@ -64,10 +64,15 @@ uint64_t vp_launch_count(void);
  *   out[o,l,c] = sum_k W[k*sel_mod + j] * in[o, (l - shift[j] - (k-2)) mod n_line, c]
  * for k = 0..5, where j = (c / sel_div) % sel_mod.
  * shift: int32[sel_mod]; W: compute type [6][sel_mod]. f_out must not
- * overlap f_in. */
+ * overlap f_in.
+ * shift_spread: an upper bound, supplied by the caller from the host copy of
+ * the table, of max(shift) - min(shift) over every aligned group of 4 table
+ * entries (4q .. 4q+3), or -1 if unknown. With sel_div == 1 (the y drift,
+ * whose shift follows the contiguous vy index) a bound of 0 or 1 lets each
+ * thread move 4 columns at once; otherwise the sweep uses scalar columns. */
 int vp_drift(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line,
              int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift,
-             const void* W, void* stream);
+             int32_t shift_spread, const void* W, void* stream);
 
 /* The same drift fused with the velocity moment of its output (the y drift
  * before the field solve, vlasov2D2V.py:1064 followed by compute_rho :416-431;
@@ -76,7 +81,7 @@ int vp_drift(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t 
  * workspace: vp_drift_rho_workspace_bytes() bytes of scratch. */
 int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line,
                  int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift,
-                 const void* W, double scale, double* rho, void* workspace,
+                 int32_t shift_spread, const void* W, double scale, double* rho, void* workspace,
                  size_t workspace_bytes, void* stream);
 size_t vp_drift_rho_workspace_bytes(int64_t n_outer, int64_t n_line, int64_t n_inner);
 
@@ -183,7 +188,10 @@ typedef struct vp_step2d_desc {
     double dt, dx, dy, dvx, dvy;
     int32_t physics_mode;
     int32_t window;        /* kick window S (<0: exact kick) */
-    int32_t diagnostics;   /* nonzero: fill diag[] (moments add one FP64 pass in the kick) */
+    int32_t diagnostics;   /* 0: none; 1: field energy, mass, max shift; 2: also the
+                              L2 / kinetic moments (an FP64 epilogue in the kick) */
+    int32_t shift_spread_x; /* see vp_drift (tables of the x and y drifts) */
+    int32_t shift_spread_y;
     const void* f_in;
     void* f_out;
     void* f_tmp;
@@ -219,6 +227,7 @@ typedef struct vp_step1d_desc {
     int32_t physics_mode;
     int32_t window;
     int32_t diagnostics;
+    int32_t shift_spread; /* see vp_drift */
     const void* f_in;
     void* f_out;
     void* f_tmp;

@@ -48,6 +48,7 @@ class Step2dDesc(ctypes.Structure):
         ("dtype", I32), ("nx", I64), ("ny", I64), ("nvx", I64), ("nvy", I64),
         ("dt", D), ("dx", D), ("dy", D), ("dvx", D), ("dvy", D),
         ("physics_mode", I32), ("window", I32), ("diagnostics", I32),
+        ("shift_spread_x", I32), ("shift_spread_y", I32),
         ("f_in", P), ("f_out", P), ("f_tmp", P),
         ("shift_x", P), ("W_x", P), ("shift_y", P), ("W_y", P),
         ("kx", P), ("ky", P), ("inv_ksq", P), ("vx", P), ("vy", P),
@@ -60,7 +61,7 @@ class Step1dDesc(ctypes.Structure):
     _fields_ = [
         ("dtype", I32), ("nx", I64), ("nv", I64),
         ("dt", D), ("dx", D), ("dv", D),
-        ("physics_mode", I32), ("window", I32), ("diagnostics", I32),
+        ("physics_mode", I32), ("window", I32), ("diagnostics", I32), ("shift_spread", I32),
         ("f_in", P), ("f_out", P), ("f_tmp", P),
         ("shift", P), ("W", P), ("inv_kx", P), ("inv_kx_sq", P), ("v", P),
         ("rho", P), ("phi", P), ("e", P), ("diag", P),
@@ -73,8 +74,8 @@ SIGNATURES = {
     "vp_version": (ctypes.c_char_p, []),
     "vp_last_error": (ctypes.c_char_p, []),
     "vp_launch_count": (ctypes.c_uint64, []),
-    "vp_drift": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I64, P, P, P]),
-    "vp_drift_rho": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I64, P, P, D, P, P, SZ, P]),
+    "vp_drift": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I64, P, I32, P, P]),
+    "vp_drift_rho": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I64, P, I32, P, D, P, P, SZ, P]),
     "vp_drift_rho_workspace_bytes": (SZ, [I64, I64, I64]),
     "vp_kick": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, P, ctypes.c_int, I64, D, D, I32, P]),
     "vp_kick2d": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, P, P, D, D, D, I32, P, P, P, P]),

@@ -155,13 +155,14 @@ const char* vp_last_error(void) { return g_last_error.c_str(); }
 uint64_t vp_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int vp_drift(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line, int64_t n_inner,
-             int64_t sel_div, int64_t sel_mod, const int32_t* shift, const void* W, void* stream) {
+             int64_t sel_div, int64_t sel_mod, const int32_t* shift, int32_t shift_spread, const void* W,
+             void* stream) {
     if (!dtype_ok(dtype)) return set_error(VP_ERR_DTYPE, "vp_drift: unknown dtype");
     VP_CHECK(f_in && f_out && shift && W, "vp_drift: null pointer");
     VP_CHECK(f_in != f_out, "vp_drift: f_out must not alias f_in");
     VP_CHECK(n_outer > 0 && n_line > 0 && n_inner > 0 && sel_div > 0 && sel_mod > 0, "vp_drift: bad size");
     VP_CHECK(n_line < (1 << 30), "vp_drift: line too long");
-    return run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, false, sel_div, sel_mod, shift, W, nullptr, 0,
+    return run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, false, sel_div, sel_mod, shift_spread, shift, W, nullptr, 0,
                        1, 0.0, 1.0, -1, nullptr, nullptr, S(stream));
 }
 
@@ -170,7 +171,8 @@ size_t vp_drift_rho_workspace_bytes(int64_t n_outer, int64_t n_line, int64_t n_i
 }
 
 int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line, int64_t n_inner,
-                 int64_t sel_div, int64_t sel_mod, const int32_t* shift, const void* W, double scale, double* rho,
+                 int64_t sel_div, int64_t sel_mod, const int32_t* shift, int32_t shift_spread, const void* W,
+                 double scale, double* rho,
                  void* workspace, size_t workspace_bytes, void* stream) {
     if (!dtype_ok(dtype)) return set_error(VP_ERR_DTYPE, "vp_drift_rho: unknown dtype");
     VP_CHECK(f_in && f_out && shift && W && rho, "vp_drift_rho: null pointer");
@@ -181,7 +183,7 @@ int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int6
         return set_error(VP_ERR_WORKSPACE, "vp_drift_rho: workspace too small");
     int tiles = 0;
     double* part = static_cast<double*>(workspace);
-    int rc = run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, false, sel_div, sel_mod, shift, W, nullptr,
+    int rc = run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, false, sel_div, sel_mod, shift_spread, shift, W, nullptr,
                          0, 1, 0.0, 1.0, -1, part, &tiles, S(stream));
     if (rc) return rc;
     return run_rho_finalize(part, n_outer, n_line, tiles, scale, rho, S(stream));
@@ -199,7 +201,7 @@ int vp_kick(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n
     const int e_f64 = e_dtype == VP_F64;
     if (n_inner == 1)
         return run_kick_contig(dtype, f_in, f_out, n_outer, n_line, E, e_f64, e_div, dt, dv, window, S(stream));
-    return run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, true, 1, 1, nullptr, nullptr, E, e_f64, e_div,
+    return run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, true, 1, 1, -1, nullptr, nullptr, E, e_f64, e_div,
                        dt, dv, window, nullptr, nullptr, S(stream));
 }
 
@@ -307,7 +309,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     // x drift (dt/2)
     if ((rc = mk.begin(VP_PHASE_DRIFT_X1))) return rc;
     void* dst = dst_of(i++);
-    rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_x, d->W_x, nullptr, 0, 1,
+    rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_spread_x, d->shift_x, d->W_x, nullptr, 0, 1,
                      0.0, 1.0, -1, nullptr, nullptr, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
     src = dst;
@@ -316,12 +318,12 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     dst = dst_of(i++);
     if (want_rho) {
         int tiles = 0;
-        rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
+        rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_spread_y, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
                          1.0, -1, w.part, &tiles, st);
         if (rc) return rc;
         rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, w.rho, st);
     } else {
-        rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
+        rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_spread_y, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
                          1.0, -1, nullptr, nullptr, st);
     }
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
@@ -335,7 +337,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         rc = run_poisson2d(w.rho, nx, ny, d->kx, d->ky, d->inv_ksq, ex, ey, d->drho, d->phi, w.pois, &pv, st);
         if (rc || (rc = mk.end(VP_PHASE_FIELD)) || (rc = mk.begin(VP_PHASE_KICK))) return rc;
         if (fused) {
-            moments = want_diag ? w.moments : nullptr;
+            moments = (want_diag && d->diagnostics >= 2) ? w.moments : nullptr;
             dst = dst_of(i++);
             rc = run_kick2d(d->dtype, src, dst, nx * ny, nvx, nvy, ex, ey, d->dt, d->dvx, d->dvy, d->window, d->vx,
                             d->vy, moments, st);
@@ -343,7 +345,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
             src = dst;
         } else {
             dst = dst_of(i++);
-            rc = run_strided(d->dtype, src, dst, nx * ny, nvx, nvy, true, 1, 1, nullptr, nullptr, ex, 1, 1, d->dt,
+            rc = run_strided(d->dtype, src, dst, nx * ny, nvx, nvy, true, 1, 1, -1, nullptr, nullptr, ex, 1, 1, d->dt,
                              d->dvx, d->window, nullptr, nullptr, st);
             if (rc) return rc;
             src = dst;
@@ -368,14 +370,14 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     // y drift (dt/2)
     if ((rc = mk.begin(VP_PHASE_DRIFT_Y2))) return rc;
     dst = dst_of(i++);
-    rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
+    rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_spread_y, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
                      1.0, -1, nullptr, nullptr, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_Y2))) return rc;
     src = dst;
     // x drift (dt/2)
     if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
     dst = dst_of(i++);
-    rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_x, d->W_x, nullptr, 0, 1,
+    rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_spread_x, d->shift_x, d->W_x, nullptr, 0, 1,
                      0.0, 1.0, -1, nullptr, nullptr, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     if (want_diag) {
@@ -424,12 +426,12 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     void* dst = dst_of(i++);
     if (phys || want_diag) {
         int tiles = 0;
-        rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
+        rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
                          w.part, &tiles, st);
         if (rc) return rc;
         rc = run_rho_finalize(w.part, 1, nx, tiles, d->dv, w.n, st);
     } else {
-        rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
+        rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
                          nullptr, nullptr, st);
     }
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
@@ -457,7 +459,7 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     if ((rc = mk.begin(VP_PHASE_DRIFT_Y2)) || (rc = mk.end(VP_PHASE_DRIFT_Y2))) return rc;
     if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
     dst = dst_of(i++);
-    rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1, nullptr,
+    rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1, nullptr,
                      nullptr, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     if (want_diag) {

@@ -28,7 +28,7 @@ struct Pois2dWsView {
 
 // sweeps.cu
 int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner, bool kick,
-                int64_t sel_div, int64_t sel_mod, const int32_t* shift, const void* W, const void* E, int e_f64,
+                int64_t sel_div, int64_t sel_mod, int spread, const int32_t* shift, const void* W, const void* E, int e_f64,
                 int64_t e_div, double dt, double dv, int window, double* part, int* tiles_out, cudaStream_t st);
 int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double* rho,
                      cudaStream_t st);

@@ -55,17 +55,24 @@ struct StridedArgs {
     double* part;
 };
 
-template <typename TS, int VEC, bool KICK, bool RHO, bool WRAPREUSE>
-__global__ void __launch_bounds__(kBlock) k_strided(StridedArgs a) {
+// NT = rows of the interpolation window of one output: 6 when the VEC
+// columns of a thread share one shift, 7 when their shifts differ by at most
+// one (the y drift, whose shift follows vy, the contiguous index): each
+// element then gets its own 7-tap weight vector with one zero tap.
+template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE>
+__global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
-    using TT = typename std::conditional<sizeof(C) == 8, double, float>::type;  // tile type
+    constexpr int NW = NT - 1;  // window rows carried from chunk to chunk
+    constexpr int WV = NT == 6 ? 1 : VEC;  // distinct weight vectors per thread
+    static_assert(NT == 6 || (NT == 7 && !KICK), "7-row windows are for drifts");
+    using TT = typename std::conditional<(sizeof(C) == 8 || VEC > 1), double, float>::type;  // tile type
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
-    double* wpart = reinterpret_cast<double*>(smem_raw);                  // [nwarps][seg]
+    double* wpart = reinterpret_cast<double*>(smem_raw);                       // [nwarps][seg]
     TT* tile_all = reinterpret_cast<TT*>(wpart + (RHO ? nwarps * a.seg : 0));  // [nwarps][8][33]
     TT* tile = tile_all + warp * (kU * 33);
     const int n = a.n_line;
@@ -83,21 +90,47 @@ __global__ void __launch_bounds__(kBlock) k_strided(StridedArgs a) {
         const int l_end = min(l0 + a.seg, n);
         const int64_t col = active ? cg * VEC : 0;
 
-        C w[6];
-        int s;
+        // wt[e][j]: weight of window row j (base row l - s_hi - 3) for element e
+        C wt[WV][NT];
+        int s_hi;
         if constexpr (KICK) {
+            C w[6];
             const int64_t ei = o / a.e_div;
             if (a.e_f64)
-                s = kick_weights<double, C>(static_cast<const double*>(a.E)[ei], a.dt, a.dv, a.window, w);
+                s_hi = kick_weights<double, C>(static_cast<const double*>(a.E)[ei], a.dt, a.dv, a.window, w);
             else
-                s = kick_weights<float, C>(static_cast<const float*>(a.E)[ei], a.dt, a.dv, a.window, w);
-            s = max(-(1 << 28), min(1 << 28, s));
-        } else {
-            const int j = (int)((col / a.sel_div) % a.sel_mod);
-            s = a.shift[j];
+                s_hi = kick_weights<float, C>(static_cast<const float*>(a.E)[ei], a.dt, a.dv, a.window, w);
+            s_hi = max(-(1 << 28), min(1 << 28, s_hi));
+#pragma unroll
+            for (int j = 0; j < 6; ++j) wt[0][j] = w[5 - j];
+        } else if constexpr (NT == 6) {
+            const int jt = (int)((col / a.sel_div) % a.sel_mod);
+            s_hi = a.shift[jt];
             const C* Wt = static_cast<const C*>(a.W);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) w[k] = Wt[k * a.sel_mod + j];
+            for (int j = 0; j < 6; ++j) wt[0][j] = Wt[(5 - j) * a.sel_mod + jt];
+        } else {
+            int se[VEC];
+            s_hi = -(1 << 30);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+                const int jt = (int)(((col + e) / a.sel_div) % a.sel_mod);
+                se[e] = a.shift[jt];
+                s_hi = max(s_hi, se[e]);
+            }
+            const C* Wt = static_cast<const C*>(a.W);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+                const int jt = (int)(((col + e) / a.sel_div) % a.sel_mod);
+                const bool lo = se[e] != s_hi;  // shift one below the group maximum
+#pragma unroll
+                for (int j = 0; j < NT; ++j) {
+                    // tap k sits at row j = (s_hi - s_e) + 5 - k
+                    const C w_same = j <= 5 ? Wt[(5 - j) * a.sel_mod + jt] : C(0);
+                    const C w_lo = j >= 1 ? Wt[(6 - j) * a.sel_mod + jt] : C(0);
+                    wt[e][j] = lo ? w_lo : w_same;
+                }
+            }
         }
         const TS* src = in + (o * n) * ni + col;
         TS* dst = out + (o * n) * ni + col;
@@ -106,31 +139,30 @@ __global__ void __launch_bounds__(kBlock) k_strided(StridedArgs a) {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) zero.v[e] = C(0);
 
-        // window base row for output l0: l0 - s - 3
-        V win[5];
+        V win[NW];
         int rnext;
         if constexpr (!KICK) {
-            int64_t r64 = ((int64_t)l0 - s - 3) % n;
+            int64_t r64 = ((int64_t)l0 - s_hi - 3) % n;
             int r = (int)(r64 < 0 ? r64 + n : r64);
 #pragma unroll
-            for (int j = 0; j < 5; ++j) {
+            for (int j = 0; j < NW; ++j) {
                 win[j] = active ? ldv<TS, VEC>(src + (int64_t)r * ni) : zero;
                 r = wrap_up(r + 1, n);
             }
             rnext = r;
         } else {
-            const int r = l0 - s - 3;
+            const int r = l0 - s_hi - 3;
 #pragma unroll
-            for (int j = 0; j < 5; ++j) {
+            for (int j = 0; j < NW; ++j) {
                 const int rr = r + j;
                 win[j] = (active && rr >= 0 && rr < n) ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
             }
-            rnext = r + 5;
+            rnext = r + NW;
         }
-        V first[5];
+        V first[WRAPREUSE ? NW : 1];
         if constexpr (WRAPREUSE) {
 #pragma unroll
-            for (int j = 0; j < 5; ++j) first[j] = win[j];
+            for (int j = 0; j < NW; ++j) first[j] = win[j];
         }
 
         for (int l = l0; l < l_end; l += kU) {
@@ -140,8 +172,8 @@ __global__ void __launch_bounds__(kBlock) k_strided(StridedArgs a) {
             for (int u = 0; u < kU; ++u) {
                 if constexpr (!KICK) {
                     const int rr = wrap_up(rnext + u, n);
-                    if (WRAPREUSE && last && u >= kU - 5)
-                        nx[u] = first[u - (kU - 5)];
+                    if (WRAPREUSE && last && u >= kU - NW)
+                        nx[u] = first[WRAPREUSE ? u - (kU - NW) : 0];
                     else
                         nx[u] = active ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
                 } else {
@@ -156,14 +188,12 @@ __global__ void __launch_bounds__(kBlock) k_strided(StridedArgs a) {
             for (int u = 0; u < kU; ++u) {
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
-                    // tap k reads window row u + 5 - k
-                    auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : nx[j - 5].v[e]; };
-                    C acc = w[0] * g(u + 5);
-                    acc = fma(w[1], g(u + 4), acc);
-                    acc = fma(w[2], g(u + 3), acc);
-                    acc = fma(w[3], g(u + 2), acc);
-                    acc = fma(w[4], g(u + 1), acc);
-                    acc = fma(w[5], g(u + 0), acc);
+                    auto g = [&](int j) -> C { return j < NW ? win[j].v[e] : nx[j - NW].v[e]; };
+                    const int we = NT == 6 ? 0 : e;
+                    // ascending stencil tap k = descending window row j
+                    C acc = wt[we][NT - 1] * g(u + NT - 1);
+#pragma unroll
+                    for (int j = NT - 2; j >= 0; --j) acc = fma(wt[we][j], g(u + j), acc);
                     res[u].v[e] = acc;
                 }
             }
@@ -192,7 +222,7 @@ __global__ void __launch_bounds__(kBlock) k_strided(StridedArgs a) {
                 __syncwarp();
             }
 #pragma unroll
-            for (int j = 0; j < 5; ++j) win[j] = nx[kU - 5 + j];
+            for (int j = 0; j < NW; ++j) win[j] = nx[kU - NW + j];
         }
 
         if constexpr (RHO) {
@@ -223,34 +253,44 @@ __global__ void k_rho_finalize(const double* __restrict__ part, int64_t n_outer,
 // host side of the strided sweeps
 // ---------------------------------------------------------------------------
 struct StridedPlan {
-    int vec;
+    int vec, nt;
     int tiles, seg, nseg;
     int64_t ncg, items;
 };
 
-static int pick_vec(int dtype, int64_t n_inner, int64_t sel_div, bool kick, const void* in, const void* out) {
-    // VEC elements of one thread must share the shift: consecutive columns do
-    // when the table index changes only every sel_div columns (kick: always).
+// Elements per thread (VEC) and window rows (NT). The VEC consecutive columns
+// of a thread share one shift when the table index changes only every sel_div
+// columns (and always in a kick); when it changes with every column
+// (sel_div == 1), a 7-row window covers groups whose shifts differ by at most
+// one, which the caller certifies through `spread` (max over aligned groups of
+// 4 table entries of max shift - min shift; negative = unknown).
+static void pick_vec(int dtype, int64_t n_inner, int64_t sel_div, int64_t sel_mod, bool kick, int spread,
+                     const void* in, const void* out, int* vec, int* nt) {
     const int64_t esz = dtype == VP_F64 ? 8 : (dtype == VP_F32 ? 4 : 2);
-    const int cands[2] = {dtype == VP_F64 ? 2 : 4, 1};
-    for (int v : cands) {
-        if (v == 1) return 1;
-        if (n_inner % v) continue;
-        if (!kick && sel_div % v) continue;
-        if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % (v * esz)) continue;
-        return v;
+    const int v = dtype == VP_F64 ? 2 : 4;
+    *vec = 1;
+    *nt = 6;
+    if (n_inner % v) return;
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % (v * esz)) return;
+    if (kick || sel_div % v == 0) {
+        *vec = v;
+        return;
     }
-    return 1;
+    if (sel_div == 1 && sel_mod % 4 == 0 && spread >= 0 && spread <= 1) {
+        *vec = v;
+        *nt = spread == 0 ? 6 : 7;
+    }
 }
 
-static StridedPlan plan_strided(int64_t n_outer, int64_t n_line, int64_t n_inner, int vec, int occ_blocks,
-                                int sms, bool rho) {
+static StridedPlan plan_strided(int64_t n_outer, int64_t n_line, int64_t n_inner, int vec, int nt,
+                                int occ_blocks, int sms, bool rho) {
     StridedPlan p;
     p.vec = vec;
+    p.nt = nt;
     p.ncg = n_inner / vec;
     p.tiles = (int)((p.ncg + kBlock - 1) / kBlock);
     // whole lines when there are enough of them to fill the GPU; otherwise
-    // split lines into segments (each costs 5 extra halo rows)
+    // split lines into segments (each costs NT-1 extra halo rows)
     const int64_t want = (int64_t)sms * std::max(occ_blocks, 1) * 2;
     int seg = (int)n_line;
     const int64_t base = n_outer * p.tiles;
@@ -262,13 +302,14 @@ static StridedPlan plan_strided(int64_t n_outer, int64_t n_line, int64_t n_inner
     return p;
 }
 
-template <typename TS, int VEC, bool KICK, bool RHO>
+template <typename TS, int VEC, int NT, bool KICK, bool RHO>
 static int launch_strided_t(StridedArgs a, int sms, cudaStream_t st) {
+    using C = compute_t<TS>;
+    using TT = typename std::conditional<(sizeof(C) == 8 || VEC > 1), double, float>::type;
     const bool full = (a.nseg == 1) && (a.n_line % kU == 0) && (a.n_line >= kU);
-    const size_t smem = RHO ? (size_t)(kBlock / 32) * a.seg * sizeof(double) +
-                                  (size_t)(kBlock / 32) * kU * 33 * sizeof(compute_t<TS>)
-                            : 0;
-    auto kern = (!KICK && full) ? k_strided<TS, VEC, KICK, RHO, true> : k_strided<TS, VEC, KICK, RHO, false>;
+    const size_t smem =
+        RHO ? (size_t)(kBlock / 32) * a.seg * sizeof(double) + (size_t)(kBlock / 32) * kU * 33 * sizeof(TT) : 0;
+    auto kern = (!KICK && full) ? k_strided<TS, VEC, NT, KICK, RHO, true> : k_strided<TS, VEC, NT, KICK, RHO, false>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return set_cuda_error("cudaFuncSetAttribute(k_strided)");
@@ -280,42 +321,37 @@ static int launch_strided_t(StridedArgs a, int sms, cudaStream_t st) {
 }
 
 template <typename TS, bool KICK, bool RHO>
-static int launch_strided_vec(StridedArgs a, int vec, int sms, cudaStream_t st) {
-    if constexpr (sizeof(TS) == 8) {
-        if (vec == 2) return launch_strided_t<TS, 2, KICK, RHO>(a, sms, st);
-    } else {
-        if (vec == 4) return launch_strided_t<TS, 4, KICK, RHO>(a, sms, st);
+static int launch_strided_vec(StridedArgs a, int vec, int nt, int sms, cudaStream_t st) {
+    constexpr int V = sizeof(TS) == 8 ? 2 : 4;
+    if (vec == V) {
+        if constexpr (!KICK) {
+            if (nt == 7) return launch_strided_t<TS, V, 7, KICK, RHO>(a, sms, st);
+        }
+        return launch_strided_t<TS, V, 6, KICK, RHO>(a, sms, st);
     }
-    return launch_strided_t<TS, 1, KICK, RHO>(a, sms, st);
+    return launch_strided_t<TS, 1, 6, KICK, RHO>(a, sms, st);
 }
 
 template <bool KICK, bool RHO>
-static int launch_strided(int dtype, StridedArgs a, int vec, int sms, cudaStream_t st) {
+static int launch_strided(int dtype, StridedArgs a, int vec, int nt, int sms, cudaStream_t st) {
     switch (dtype) {
-        case VP_F32: return launch_strided_vec<float, KICK, RHO>(a, vec, sms, st);
-        case VP_F64: return launch_strided_vec<double, KICK, RHO>(a, vec, sms, st);
-        case VP_BF16: return launch_strided_vec<__nv_bfloat16, KICK, RHO>(a, vec, sms, st);
+        case VP_F32: return launch_strided_vec<float, KICK, RHO>(a, vec, nt, sms, st);
+        case VP_F64: return launch_strided_vec<double, KICK, RHO>(a, vec, nt, sms, st);
+        case VP_BF16: return launch_strided_vec<__nv_bfloat16, KICK, RHO>(a, vec, nt, sms, st);
     }
     return set_error(VP_ERR_DTYPE, "unknown dtype");
 }
 
-template <typename TS>
-static int occ_of_strided(int vec, bool kick, bool rho) {
-    (void)vec;
-    (void)kick;
-    (void)rho;
-    return 2;  // planning estimate; the launch queries the exact occupancy
-}
-
 int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner,
-                bool kick, int64_t sel_div, int64_t sel_mod, const int32_t* shift, const void* W,
+                bool kick, int64_t sel_div, int64_t sel_mod, int spread, const int32_t* shift, const void* W,
                 const void* E, int e_f64, int64_t e_div, double dt, double dv, int window, double* part,
                 int* tiles_out, cudaStream_t st) {
     const int sms = sm_count();
     const bool rho = part != nullptr || tiles_out != nullptr;
-    const int vec = rho ? 1 : pick_vec(dtype, n_inner, sel_div, kick, in, out);
-    const int occ_est = rho ? 8 : (vec > 1 ? 2 : 8);
-    StridedPlan p = plan_strided(n_outer, n_line, n_inner, vec, occ_est, sms, rho);
+    int vec, nt;
+    pick_vec(dtype, n_inner, sel_div, sel_mod, kick, spread, in, out, &vec, &nt);
+    const int occ_est = vec > 1 ? 2 : 4;
+    StridedPlan p = plan_strided(n_outer, n_line, n_inner, vec, nt, occ_est, sms, rho);
     if (tiles_out) *tiles_out = p.tiles;
     if (tiles_out && !part) return VP_OK;  // plan query only
     StridedArgs a{};
@@ -340,9 +376,9 @@ int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n
     a.dv = dv;
     a.window = window;
     a.part = part;
-    if (kick) return launch_strided<true, false>(dtype, a, vec, sms, st);
-    if (rho) return launch_strided<false, true>(dtype, a, vec, sms, st);
-    return launch_strided<false, false>(dtype, a, vec, sms, st);
+    if (kick) return launch_strided<true, false>(dtype, a, vec, nt, sms, st);
+    if (rho) return launch_strided<false, true>(dtype, a, vec, nt, sms, st);
+    return launch_strided<false, false>(dtype, a, vec, nt, sms, st);
 }
 
 int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double* rho,
@@ -371,8 +407,47 @@ struct Kick2dArgs {
     double* moments;
 };
 
+// 4 consecutive compute-type values from shared memory (16-byte aligned)
+template <typename C>
+__device__ __forceinline__ void lds4(const C* p, C (&v)[4]) {
+    if constexpr (sizeof(C) == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else {
+        const double2 t = reinterpret_cast<const double2*>(p)[0];
+        const double2 u = reinterpret_cast<const double2*>(p)[1];
+        v[0] = t.x; v[1] = t.y; v[2] = u.x; v[3] = u.y;
+    }
+}
+
+template <typename C>
+__device__ __forceinline__ void sts4(C* p, const C (&v)[4]) {
+    if constexpr (sizeof(C) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+}
+
+// vy kick of 4 elements from the 12 row values t[0..11] that start at the
+// element offset R (static) before the window of the first element
+template <int R, typename C>
+__device__ __forceinline__ void vy_taps(const C (&t)[12], const C (&wy)[6], C (&o)[4]) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        C acc = wy[0] * t[R + e + 5];
+        acc = fma(wy[1], t[R + e + 4], acc);
+        acc = fma(wy[2], t[R + e + 3], acc);
+        acc = fma(wy[3], t[R + e + 2], acc);
+        acc = fma(wy[4], t[R + e + 1], acc);
+        acc = fma(wy[5], t[R + e + 0], acc);
+        o[e] = acc;
+    }
+}
+
 template <typename TS, int VEC, bool DIAG>
-__global__ void __launch_bounds__(kBlock) k_kick2d(Kick2dArgs a) {
+__global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
@@ -383,7 +458,7 @@ __global__ void __launch_bounds__(kBlock) k_kick2d(Kick2dArgs a) {
     const int tid_team = threadIdx.x / team;
     const int li = threadIdx.x % team;
     const bool lane_ok = li < a.groups;
-    const int nvx = a.nvx, nvy = a.nvy;
+    const int nvx = a.nvx, nvy = a.nvy, groups = a.groups;
     C* rowbuf = reinterpret_cast<C*>(smem_raw) + (size_t)tid_team * kU * nvy;
 
     double vy2[VEC];
@@ -415,15 +490,20 @@ __global__ void __launch_bounds__(kBlock) k_kick2d(Kick2dArgs a) {
         }
         sx = max(-(1 << 28), min(1 << 28, sx));
         sy = max(-(1 << 28), min(1 << 28, sy));
+        // vy window of the lane's first element starts gshift elements away:
+        // group offset gd (floor division) and element remainder r in [0, 4)
+        const int gshift = -sy - 3;
+        const int gd = gshift >= 0 ? gshift / 4 : -((-gshift + 3) / 4);
+        const int r = gshift - 4 * gd;
         const TS* src = in + p * (int64_t)nvx * nvy + li * VEC;
         TS* dst = out + p * (int64_t)nvx * nvy + li * VEC;
         double m_pre = 0.0, m_post = 0.0, m_l2 = 0.0, m_sum = 0.0;
 
-        auto load_row = [&](int r) -> V {
-            V v = (active && r >= 0 && r < nvx) ? ldv<TS, VEC>(src + (int64_t)r * nvy) : zero;
+        auto load_row = [&](int rr) -> V {
+            V v = (active && rr >= 0 && rr < nvx) ? ldv<TS, VEC>(src + (int64_t)rr * nvy) : zero;
             if constexpr (DIAG) {
-                if (active && r >= 0 && r < nvx) {
-                    const double vx2 = a.vx[r] * a.vx[r];
+                if (active && rr >= 0 && rr < nvx) {
+                    const double vx2 = a.vx[rr] * a.vx[rr];
 #pragma unroll
                     for (int e = 0; e < VEC; ++e) m_pre += (double)v.v[e] * (vx2 + vy2[e]);
                 }
@@ -442,9 +522,11 @@ __global__ void __launch_bounds__(kBlock) k_kick2d(Kick2dArgs a) {
 #pragma unroll
             for (int u = 0; u < kU; ++u) nx[u] = load_row(rnext + u);
             rnext += kU;
-            // vx kick of rows l..l+kU-1 into the team's row buffer
+            // vx kick of rows l..l+kU-1 into the team's row buffer (rounded to
+            // the storage type, as the reference stores f between the kicks)
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
+                C rv[VEC];
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
                     auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : nx[j - 5].v[e]; };
@@ -454,38 +536,65 @@ __global__ void __launch_bounds__(kBlock) k_kick2d(Kick2dArgs a) {
                     acc = fma(wx[3], g(u + 2), acc);
                     acc = fma(wx[4], g(u + 1), acc);
                     acc = fma(wx[5], g(u + 0), acc);
-                    // the intermediate f between the two kicks is rounded to the
-                    // storage type, as the reference stores it between sweeps
-                    if (lane_ok) rowbuf[u * nvy + li * VEC + e] = as_stored<TS>(acc);
+                    rv[e] = as_stored<TS>(acc);
+                }
+                if (lane_ok) {
+                    if constexpr (VEC == 4) {
+                        sts4<C>(rowbuf + u * nvy + li * 4, rv);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) rowbuf[u * nvy + li * VEC + e] = rv[e];
+                    }
                 }
             }
             __syncwarp();
             // vy kick of the buffered rows
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                V r;
+                V rres;
+                if constexpr (VEC == 4) {
+                    C t[12];
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) {
-                    const int iv = li * VEC + e;
-                    auto g = [&](int k) -> C {
-                        const int j = iv - sy + 2 - k;
-                        return (j >= 0 && j < nvy) ? rowbuf[u * nvy + j] : C(0);
-                    };
-                    C acc = wy[0] * g(0);
-                    acc = fma(wy[1], g(1), acc);
-                    acc = fma(wy[2], g(2), acc);
-                    acc = fma(wy[3], g(3), acc);
-                    acc = fma(wy[4], g(4), acc);
-                    acc = fma(wy[5], g(5), acc);
-                    r.v[e] = acc;
+                    for (int j = 0; j < 3; ++j) {
+                        const int gi = li + gd + j;
+                        C q[4] = {C(0), C(0), C(0), C(0)};
+                        if (gi >= 0 && gi < groups) lds4<C>(rowbuf + u * nvy + gi * 4, q);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) t[4 * j + e] = q[e];
+                    }
+                    C o4[4];
+                    switch (r) {
+                        case 0: vy_taps<0, C>(t, wy, o4); break;
+                        case 1: vy_taps<1, C>(t, wy, o4); break;
+                        case 2: vy_taps<2, C>(t, wy, o4); break;
+                        default: vy_taps<3, C>(t, wy, o4); break;
+                    }
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) rres.v[e] = o4[e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) {
+                        const int iv = li * VEC + e;
+                        auto g = [&](int k) -> C {
+                            const int j = iv - sy + 2 - k;
+                            return (j >= 0 && j < nvy) ? rowbuf[u * nvy + j] : C(0);
+                        };
+                        C acc = wy[0] * g(0);
+                        acc = fma(wy[1], g(1), acc);
+                        acc = fma(wy[2], g(2), acc);
+                        acc = fma(wy[3], g(3), acc);
+                        acc = fma(wy[4], g(4), acc);
+                        acc = fma(wy[5], g(5), acc);
+                        rres.v[e] = acc;
+                    }
                 }
                 if (active && l + u < nvx) {
-                    stv<TS, VEC>(dst + (int64_t)(l + u) * nvy, r);
+                    stv<TS, VEC>(dst + (int64_t)(l + u) * nvy, rres);
                     if constexpr (DIAG) {
                         const double vx2 = a.vx[l + u] * a.vx[l + u];
 #pragma unroll
                         for (int e = 0; e < VEC; ++e) {
-                            const double fv = (double)as_stored<TS>(r.v[e]);
+                            const double fv = (double)as_stored<TS>(rres.v[e]);
                             m_post += fv * (vx2 + vy2[e]);
                             m_l2 += fv * fv;
                             m_sum += fv;
@@ -543,8 +652,12 @@ static int launch_kick2d_vec(Kick2dArgs a, int vec, cudaStream_t st) {
 // 128-element row per warp), else 2 (FP64), else 1.
 static int kick2d_vec(int dtype, int64_t nvy, uintptr_t addr_or) {
     const int64_t esz = dtype == VP_F64 ? 8 : (dtype == VP_F32 ? 4 : 2);
+    // FP64 prefers 2 per lane (4 doubles per lane spill registers) while a
+    // plane row still fits one warp
+    const bool f64_narrow = dtype == VP_F64 && nvy <= 64;
     for (int vec : {4, 2}) {
         if (vec == 2 && dtype != VP_F64) continue;
+        if (vec == 4 && f64_narrow) continue;
         if (nvy % vec == 0 && addr_or % (vec * esz) == 0) return vec;
     }
     return 1;

@@ -45,7 +45,7 @@ class Stepper2D:
         self.dtype = dtype
         self.physics_mode = bool(physics_mode)
         self.window = int(window)
-        self.diagnostics = bool(diagnostics)
+        self.diagnostics = int(diagnostics)  # 0 none, 1 field energy + mass, 2 + L2 / kinetic moments
         self.set_spacings(2 * Vx_max / (Nvx - 1), 2 * Vy_max / (Nvy - 1))
         self.tx = ops.DriftTable.from_velocity(vx_t, self.dt / 2.0, self.dx, dtype, self.device)
         self.ty = ops.DriftTable.from_velocity(vy_t, self.dt / 2.0, self.dy, dtype, self.device)
@@ -74,7 +74,8 @@ class Stepper2D:
         d.dt, d.dx, d.dy, d.dvx, d.dvy = self.dt, self.dx, self.dy, self.dvx, self.dvy
         d.physics_mode = 1 if self.physics_mode else 0
         d.window = self.window
-        d.diagnostics = 1 if (self.diagnostics and diag is not None) else 0
+        d.diagnostics = self.diagnostics if diag is not None else 0
+        d.shift_spread_x, d.shift_spread_y = self.tx.spread, self.ty.spread
         d.f_in, d.f_out, d.f_tmp = f_in.data_ptr(), f_out.data_ptr(), self.f_tmp.data_ptr()
         d.shift_x, d.W_x = self.tx.shift.data_ptr(), self.tx.W.data_ptr()
         d.shift_y, d.W_y = self.ty.shift.data_ptr(), self.ty.W.data_ptr()
@@ -167,7 +168,7 @@ class Stepper1D:
         self.dtype = dtype
         self.physics_mode = bool(physics_mode)
         self.window = int(window)
-        self.diagnostics = bool(diagnostics)
+        self.diagnostics = int(diagnostics)
         self.table = ops.DriftTable.from_velocity(v_t, self.dt / 2.0, self.dx, dtype, self.device)
         self.inv_kx, self.inv_kx_sq = ops.spectral_1d(Nx, self.L, self.device)
         self.v64 = v_t.to(torch.float64).to(self.device)
@@ -197,7 +198,8 @@ class Stepper1D:
         d.dt, d.dx, d.dv = self.dt, self.dx, self.dv
         d.physics_mode = 1 if self.physics_mode else 0
         d.window = self.window
-        d.diagnostics = 1 if (self.diagnostics and diag is not None) else 0
+        d.diagnostics = self.diagnostics if diag is not None else 0
+        d.shift_spread = self.table.spread
         d.f_in, d.f_out, d.f_tmp = f_in.data_ptr(), f_out.data_ptr(), self.f_tmp.data_ptr()
         d.shift, d.W = self.table.shift.data_ptr(), self.table.W.data_ptr()
         d.inv_kx, d.inv_kx_sq, d.v = self.inv_kx.data_ptr(), self.inv_kx_sq.data_ptr(), self.v64.data_ptr()

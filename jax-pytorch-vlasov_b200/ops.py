@@ -71,6 +71,16 @@ def drift_table_np(v, dt: float, dx: float, dtype: torch.dtype):
     return s.astype(np.int64), lagrange5_weights_np(alpha.astype(np_t))
 
 
+def group_spread(shift: np.ndarray, group: int = 4) -> int:
+    """max(shift) - min(shift) over aligned groups of `group` entries, or -1
+    when the table does not split into such groups (vp_drift's shift_spread)."""
+    s = np.asarray(shift, dtype=np.int64)
+    if s.size == 0 or s.size % group:
+        return -1
+    g = s.reshape(-1, group)
+    return int((g.max(axis=1) - g.min(axis=1)).max())
+
+
 class DriftTable:
     """Device copy of one drift table: shift int32[Nv], W compute-type [6][Nv]."""
 
@@ -78,6 +88,7 @@ class DriftTable:
         if np.abs(shift).max(initial=0) >= 2 ** 30:
             raise ValueError("drift shift out of range")
         self.n = int(shift.shape[0])
+        self.spread = group_spread(shift)
         self.shift = torch.as_tensor(shift.astype(np.int32), device=device)
         self.W = torch.as_tensor(np.ascontiguousarray(W), device=device).to(L.compute_dtype(dtype)).contiguous()
 
@@ -100,7 +111,7 @@ def drift(f: torch.Tensor, table: DriftTable, axis: int, vel_axis: int, out: tor
     if table.n != sel_mod:
         raise ValueError(f"drift table has {table.n} entries, axis {vel_axis} has {sel_mod}")
     L.call("vp_drift", L.ptr(f), L.ptr(out), L.dtype_code(f.dtype), n_outer, n_line, n_inner, sel_div, sel_mod,
-           L.ptr(table.shift), L.ptr(table.W), L.stream_of(f))
+           L.ptr(table.shift), table.spread, L.ptr(table.W), L.stream_of(f))
     return out
 
 
@@ -117,7 +128,8 @@ def drift_rho(f: torch.Tensor, table: DriftTable, axis: int, vel_axis: int, scal
     nb = L.query("vp_drift_rho_workspace_bytes", n_outer, n_line, n_inner)
     ws = workspace(f.device, nb)
     L.call("vp_drift_rho", L.ptr(f), L.ptr(out), L.dtype_code(f.dtype), n_outer, n_line, n_inner, sel_div, sel_mod,
-           L.ptr(table.shift), L.ptr(table.W), float(scale), L.ptr(rho), L.ptr(ws), ws.numel(), L.stream_of(f))
+           L.ptr(table.shift), table.spread, L.ptr(table.W), float(scale), L.ptr(rho), L.ptr(ws), ws.numel(),
+           L.stream_of(f))
     return out, rho
 
 

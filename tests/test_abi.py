@@ -67,12 +67,12 @@ def test_descriptor_layout_matches_c(vp, tmp_path):
 def test_argument_errors_without_gpu(lib, vp):
     L = vp._lib
     # null pointers and aliasing are rejected before any CUDA call
-    rc = lib.vp_drift(None, None, L.VP_F32, 1, 8, 8, 1, 8, None, None, None)
+    rc = lib.vp_drift(None, None, L.VP_F32, 1, 8, 8, 1, 8, None, -1, None, None)
     assert rc == 1 and b"null" in lib.vp_last_error()
     p = ctypes.c_void_p(0x1000)
-    rc = lib.vp_drift(p, p, L.VP_F32, 1, 8, 8, 1, 8, p, p, None)
+    rc = lib.vp_drift(p, p, L.VP_F32, 1, 8, 8, 1, 8, p, -1, p, None)
     assert rc == 1 and b"alias" in lib.vp_last_error()
-    rc = lib.vp_drift(p, ctypes.c_void_p(0x2000), 7, 1, 8, 8, 1, 8, p, p, None)
+    rc = lib.vp_drift(p, ctypes.c_void_p(0x2000), 7, 1, 8, 8, 1, 8, p, -1, p, None)
     assert rc == 2
     rc = lib.vp_kick(p, ctypes.c_void_p(0x2000), L.VP_F32, 4, 8, 1, p, L.VP_F64, 1, 0.1, 0.0, -1, None)
     assert rc == 1 and b"dv" in lib.vp_last_error()

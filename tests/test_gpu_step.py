@@ -110,7 +110,7 @@ def test_step2d_diag_moments(vp):
     g = O.make_grid2d(*shape, 4 * math.pi, 4 * math.pi, 6.0, 5.0, dtype=np.float64)
     f = O.landau_2d(g, 0.1, 0.5)
     st_o = O.Stepper2D(g, 0.2, window=-1)
-    st = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 5.0, 0.2, dtype=torch.float64)
+    st = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 5.0, 0.2, dtype=torch.float64, diagnostics=2)
     # oracle: state right after the kicks of the first step
     a = st_o.drift_y(st_o.drift_x(f))
     Ex, Ey, _, _ = O.solve_poisson_real(a, g)
