@@ -276,9 +276,11 @@ static void pick_vec(int dtype, int64_t n_inner, int64_t sel_div, int64_t sel_mo
         *vec = v;
         return;
     }
+    // every column has its own weights here, so the per-element (7-row) form
+    // is used even when the integer shifts of a group coincide
     if (sel_div == 1 && sel_mod % 4 == 0 && spread >= 0 && spread <= 1) {
         *vec = v;
-        *nt = spread == 0 ? 6 : 7;
+        *nt = 7;
     }
 }
 

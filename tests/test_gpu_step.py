@@ -196,8 +196,8 @@ def test_graph_replay_matches_eager(vp):
     shape = (8, 8, 16, 16)
     g = O.make_grid2d(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, dtype=np.float64)
     f0 = dev(O.landau_2d(g, 0.05, 0.5)).float()
-    a = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1)
-    b = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1)
+    a = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1, diagnostics=2)
+    b = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1, diagnostics=2)
     ha = torch.zeros((23, 8), dtype=torch.float64, device="cuda")
     hb = torch.zeros_like(ha)
     fa = a.run(f0.clone(), 23, history=ha, graph=False)
