@@ -66,15 +66,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
     constexpr int NW = NT - 1;  // window rows carried from chunk to chunk
     constexpr int WV = NT == 6 ? 1 : VEC;  // distinct weight vectors per thread
     static_assert(NT == 6 || (NT == 7 && !KICK), "7-row windows are for drifts");
-    using TT = typename std::conditional<(sizeof(C) == 8 || VEC > 1), double, float>::type;  // tile type
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
-    double* wpart = reinterpret_cast<double*>(smem_raw);                       // [nwarps][seg]
-    TT* tile_all = reinterpret_cast<TT*>(wpart + (RHO ? nwarps * a.seg : 0));  // [nwarps][8][33]
-    TT* tile = tile_all + warp * (kU * 33);
+    double* wpart = reinterpret_cast<double*>(smem_raw);  // [nwarps][seg] per-warp row sums
     const int n = a.n_line;
     const int64_t ni = a.n_inner;
 
@@ -165,9 +162,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
             for (int j = 0; j < NW; ++j) first[j] = win[j];
         }
 
-        for (int l = l0; l < l_end; l += kU) {
-            V nx[kU];
-            const bool last = WRAPREUSE && (l + kU >= l_end);
+        // rows of the chunk whose first output row is lc (U loads in flight)
+        V nx[kU];
+        auto load_chunk = [&](int lc) {
+            const bool last = WRAPREUSE && (lc + kU >= l_end);
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 if constexpr (!KICK) {
@@ -182,7 +180,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
                 }
             }
             rnext = KICK ? rnext + kU : wrap_up(rnext + kU, n);
+        };
+        load_chunk(l0);
 
+        for (int l = l0; l < l_end; l += kU) {
             V res[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
@@ -201,28 +202,51 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
             for (int u = 0; u < kU; ++u)
                 if (active && l + u < l_end) stv<TS, VEC>(dst + (int64_t)(l + u) * ni, res[u]);
 
+            double rs[RHO ? kU : 1];
             if constexpr (RHO) {
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    TT acc = TT(0);
+                    double acc = 0.0;
                     if (active && l + u < l_end) {
 #pragma unroll
-                        for (int e = 0; e < VEC; ++e) acc += TT(as_stored<TS>(res[u].v[e]));
+                        for (int e = 0; e < VEC; ++e) acc += (double)as_stored<TS>(res[u].v[e]);
                     }
-                    tile[u * 33 + lane] = acc;
+                    rs[u] = acc;
                 }
-                __syncwarp();
-                const int row = lane >> 2, q = lane & 3;
-                double acc = 0.0;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc += (double)tile[row * 33 + q * 8 + j];
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                if (q == 0 && l + row < l_end) wpart[warp * a.seg + (l - l0) + row] = acc;
-                __syncwarp();
             }
 #pragma unroll
             for (int j = 0; j < NW; ++j) win[j] = nx[kU - NW + j];
+            // next chunk's loads go out before the moment epilogue
+            if (l + kU < l_end) load_chunk(l + kU);
+
+            if constexpr (RHO) {
+                // reduce-scatter of the 8 row sums over the 32 lanes (fixed
+                // order): lane ends with row ((lane>>4)&1)*4 + ((lane>>3)&1)*2 + ((lane>>2)&1)
+                const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+                double t4[4], t2[2];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const double send = h16 ? rs[i] : rs[i + 4];
+                    const double keep = h16 ? rs[i + 4] : rs[i];
+                    t4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const double send = h8 ? t4[i] : t4[i + 2];
+                    const double keep = h8 ? t4[i + 2] : t4[i];
+                    t2[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+                }
+                double t1;
+                {
+                    const double send = h4 ? t2[0] : t2[1];
+                    const double keep = h4 ? t2[1] : t2[0];
+                    t1 = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+                }
+                t1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+                t1 += __shfl_xor_sync(0xffffffffu, t1, 1);
+                const int row = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
+                if ((lane & 3) == 0 && l + row < l_end) wpart[warp * a.seg + (l - l0) + row] = t1;
+            }
         }
 
         if constexpr (RHO) {
@@ -306,11 +330,10 @@ static StridedPlan plan_strided(int64_t n_outer, int64_t n_line, int64_t n_inner
 
 template <typename TS, int VEC, int NT, bool KICK, bool RHO>
 static int launch_strided_t(StridedArgs a, int sms, cudaStream_t st) {
-    using C = compute_t<TS>;
-    using TT = typename std::conditional<(sizeof(C) == 8 || VEC > 1), double, float>::type;
-    const bool full = (a.nseg == 1) && (a.n_line % kU == 0) && (a.n_line >= kU);
-    const size_t smem =
-        RHO ? (size_t)(kBlock / 32) * a.seg * sizeof(double) + (size_t)(kBlock / 32) * kU * 33 * sizeof(TT) : 0;
+    // whole periodic lines reuse their first rows for the wrap (not with the
+    // moment epilogue, whose prefetched chunk needs the registers)
+    const bool full = (a.nseg == 1) && (a.n_line % kU == 0) && (a.n_line >= kU) && !RHO;
+    const size_t smem = RHO ? (size_t)(kBlock / 32) * a.seg * sizeof(double) : 0;
     auto kern = (!KICK && full) ? k_strided<TS, VEC, NT, KICK, RHO, true> : k_strided<TS, VEC, NT, KICK, RHO, false>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
