@@ -141,6 +141,26 @@ int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, co
                  size_t workspace_bytes, void* stream);
 size_t vp_poisson2d_workspace_bytes(int64_t nx, int64_t ny);
 
+/* vp_poisson2d for callers that cannot allocate device memory. No
+ * counterpart in the reference (whose field solve allocates through
+ * torch.fft): this entry point serves hosts that must not call cudaMalloc or
+ * any allocating routine at the point of the call, such as code recording a
+ * CUDA stream capture, a foreign runtime that hands over only pre-registered
+ * input and output buffers, or a solver with a fixed device-memory budget.
+ * The caller passes inputs and outputs exactly as for vp_poisson2d; the
+ * scratch comes from a file-scope device array of the library, sized for
+ * nx, ny <= VP_POISSON2D_STATIC_MAX_N (about 2 MiB, held on every GPU that
+ * loads the library until the process exits). Larger grids are rejected with
+ * VP_ERR_UNSUPPORTED. The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. All calls share the one array and it keeps the last call's
+ * contents (nothing in it has to start at zero): calls that overlap on the
+ * GPU, e.g. on two streams at once, race with each other. */
+#define VP_POISSON2D_STATIC_MAX_N 256
+int vp_poisson2d_static(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                        const double* inv_ksq, double dx, double dy, double* ex, double* ey,
+                        double* drho, double* phi, double* energy, void* stream);
+
 /* Periodic 1D Poisson solve in FP64 from the density n = sum(f,1)*dv.
  * Replaces solve_poisson_real (vlasov1D1V.py:538-572) after its sum:
  * rho = n - 1, E_k = -i rho_k inv_kx, phi_k = rho_k inv_kx_sq, irfft(nx).

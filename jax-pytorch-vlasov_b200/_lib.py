@@ -83,6 +83,7 @@ SIGNATURES = {
     "vp_rho": (ctypes.c_int, [P, ctypes.c_int, I64, I64, D, D, P, ctypes.c_int, P]),
     "vp_poisson2d": (ctypes.c_int, [P, I64, I64, P, P, P, D, D, P, P, P, P, P, P, SZ, P]),
     "vp_poisson2d_workspace_bytes": (SZ, [I64, I64]),
+    "vp_poisson2d_static": (ctypes.c_int, [P, I64, I64, P, P, P, D, D, P, P, P, P, P, P]),
     "vp_poisson1d": (ctypes.c_int, [P, I64, P, P, D, P, P, P, P, P, SZ, P]),
     "vp_poisson1d_workspace_bytes": (SZ, [I64]),
     "vp_step2d": (ctypes.c_int, [ctypes.POINTER(Step2dDesc), P]),

@@ -257,6 +257,16 @@ int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, co
     return run_diag_finalize(v, nullptr, 0, dx * dy, 0.5 * dx * dy, 0.0, 0.0, 0.0, energy, nullptr, S(stream));
 }
 
+int vp_poisson2d_static(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                        const double* inv_ksq, double dx, double dy, double* ex, double* ey, double* drho,
+                        double* phi, double* energy, void* stream) {
+    VP_CHECK(rho && kx && ky && inv_ksq && ex && ey, "vp_poisson2d_static: null pointer");
+    VP_CHECK(nx > 0 && ny > 0, "vp_poisson2d_static: sizes must be positive");
+    if (nx > VP_POISSON2D_STATIC_MAX_N || ny > VP_POISSON2D_STATIC_MAX_N)
+        return set_error(VP_ERR_UNSUPPORTED, "vp_poisson2d_static: nx and ny must be <= VP_POISSON2D_STATIC_MAX_N");
+    return run_poisson2d_static(rho, nx, ny, kx, ky, inv_ksq, dx, dy, ex, ey, drho, phi, energy, S(stream));
+}
+
 size_t vp_poisson1d_workspace_bytes(int64_t nx) { return poisson1d_ws_bytes(nx); }
 
 int vp_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double dx, double* e,

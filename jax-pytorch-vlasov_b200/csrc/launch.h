@@ -51,6 +51,9 @@ int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, c
 int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_mom, double mass_scale,
                       double we_scale, double dv_scale, double shift_x, double shift_y, double* energy,
                       double* diag, cudaStream_t st);
+int run_poisson2d_static(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                         const double* inv_ksq, double dx, double dy, double* ex, double* ey, double* drho,
+                         double* phi, double* energy, cudaStream_t st);
 size_t poisson1d_ws_bytes(int64_t nx);
 int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double* e,
                   double* rho, double* phi, double* parts, cudaStream_t st);

@@ -18,6 +18,7 @@
 // Reductions (field energy, mass) use per-line partials summed in a fixed
 // order by one block: results are bitwise reproducible run to run.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "launch.h"
@@ -519,6 +520,63 @@ int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const doubl
     if ((rc = set_smem((const void*)k_p1, smem))) return rc;
     k_p1<<<1, 1024, smem, st>>>(n, (int)nx, inv_kx, inv_kx_sq, e, rho, phi, parts);
     return check_launch("k_p1");
+}
+
+}  // namespace vp
+
+// ---- 2D, allocation-free variant ---------------------------------------------
+// Scratch of vp_poisson2d_static: a file-scope device array sized for the
+// largest grid that entry point accepts (VP_POISSON2D_STATIC_MAX_N in each
+// direction). Every GPU that loads the library holds it until the process
+// exits. Host code cannot use the symbol as an address: the device address is
+// looked up once per device with cudaGetSymbolAddress and cached.
+namespace vp {
+
+constexpr size_t kStaticAlign(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kPoisStaticBytes =
+    4 * kStaticAlign((size_t)VP_POISSON2D_STATIC_MAX_N * (VP_POISSON2D_STATIC_MAX_N / 2 + 1) * sizeof(double2)) +
+    4 * kStaticAlign((size_t)VP_POISSON2D_STATIC_MAX_N * sizeof(double));
+
+static __device__ __align__(256) unsigned char g_poisson2d_scratch[kPoisStaticBytes];
+
+static std::mutex g_poisson2d_scratch_mu;
+static void* g_poisson2d_scratch_ptr[64] = {nullptr};
+
+// Device address of the scratch on the current device (looked up on the
+// first call per device, which therefore should not happen inside a stream
+// capture).
+static int poisson2d_static_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_cuda_error("cudaGetDevice");
+    if (dev < 0 || dev >= 64) return set_error(VP_ERR_UNSUPPORTED, "vp_poisson2d_static: device index >= 64");
+    std::lock_guard<std::mutex> lock(g_poisson2d_scratch_mu);
+    if (!g_poisson2d_scratch_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_poisson2d_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return set_error(VP_ERR_CUDA, "vp_poisson2d_static: cudaGetSymbolAddress of the scratch array failed");
+        }
+        g_poisson2d_scratch_ptr[dev] = p;
+    }
+    *out = g_poisson2d_scratch_ptr[dev];
+    return VP_OK;
+}
+
+int run_poisson2d_static(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                         const double* inv_ksq, double dx, double dy, double* ex, double* ey, double* drho,
+                         double* phi, double* energy, cudaStream_t st) {
+    if (poisson2d_ws_bytes(nx, ny) > kPoisStaticBytes)
+        return set_error(VP_ERR_UNSUPPORTED, "vp_poisson2d_static: grid larger than the static scratch");
+    void* ws = nullptr;
+    int rc = poisson2d_static_scratch(&ws);
+    if (rc) return rc;
+    // every kernel below writes its part of the scratch before reading it,
+    // so nothing has to be cleared between calls
+    Pois2dWsView v{};
+    rc = run_poisson2d(rho, nx, ny, kx, ky, inv_ksq, ex, ey, drho, phi, ws, &v, st);
+    if (rc || !energy) return rc;
+    return run_diag_finalize(v, nullptr, 0, dx * dy, 0.5 * dx * dy, 0.0, 0.0, 0.0, energy, nullptr, st);
 }
 
 }  // namespace vp
