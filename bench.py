@@ -1,20 +1,23 @@
-"""Benchmark of the 2D2V Vlasov-Poisson Strang step on B200.
+"""Benchmark of the Vlasov-Poisson Strang step on B200.
 
-Workload (default): the bandwidth-roofline configuration, 2D2V linear Landau
-damping on a 128^4 grid (268,435,456 cells), FP32 storage of f, amplitude
-0.05, k = 0.5 (Lx = Ly = 4 pi), v in [-6, 6], dt = 0.1. A "step" is one full
-Strang step (x, y + rho, FP64 Poisson, vx + vy kick, y, x, diagnostics).
-Metric: cell-updates/s = Nx*Ny*Nvx*Nvy * steps / seconds. Inputs are
-synthetic (the initial condition is generated, nothing is downloaded);
-f is 1 GiB, far above the 126 MB L2, so no flush is needed between steps.
+Default workload (the headline line): the bandwidth-roofline configuration,
+2D2V linear Landau damping on a 128^4 grid (268,435,456 cells), FP32 storage
+of f, amplitude 0.05, k = 0.5 (Lx = Ly = 4 pi), v in [-6, 6], dt = 0.1. A
+"step" is one full Strang step (x, y + rho, FP64 Poisson, vx + vy kick, y, x,
+field-energy and mass diagnostics). Metric: cell-updates/s = cells * steps /
+seconds. The input is synthetic (the initial condition is generated on the
+device); f is 1 GiB per buffer, 8x the 126 MB L2, so no flush is needed.
+
+Other workloads (--workload): c1 (Landau 32^4 FP64), c2 (two-stream 64^4
+FP32), oned (1D1V Landau 4096 x 4096 FP32, the reference's 1D benchmark
+grid). These are small enough to be launch-bound and run as CUDA graphs.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--dtype float32|bfloat16|float64] [--size 128]
+                  [--workload c3|c1|c2|oned] [--dtype float32|bfloat16|float64]
 
---impl reference times the CPU restatement of the reference's algorithm
-(the oracle: C + OpenMP over all host threads) on a bounded sample of the
-same workload; the reference itself is Python that is not present on the
-GPU host.
+--impl reference times the CPU restatement of the reference's algorithm (the
+oracle: C + OpenMP over all host threads) on a bounded sample of the same
+workload: the reference itself is Python that is not present on the GPU host.
 """
 from __future__ import annotations
 
@@ -34,49 +37,63 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAK_FALLBACK_GBS = 6650.0
-LX = 4.0 * math.pi
-VMAX = 6.0
-DT = 0.1
-EPS = 0.05
-KMODE = 0.5
-
 PHASES = ("drift_x1", "drift_y1_rho", "field", "kick_vx_vy", "drift_y2", "drift_x2", "diag")
+
+WORKLOADS = {
+    # name: (kind, grid, L, vmax, dt, ic, ic parameters, default dtype, description)
+    "c3": ("2d", (128, 128, 128, 128), 4 * math.pi, 6.0, 0.1, "landau", (0.05, 0.5), "float32",
+           "2D2V Landau 128^4, eps=0.05, k=0.5, v in [-6,6], dt=0.1"),
+    "c1": ("2d", (32, 32, 32, 32), 4 * math.pi, 6.0, 0.1, "landau", (0.01, 0.5), "float64",
+           "2D2V Landau 32^4, eps=0.01, k=0.5, v in [-6,6], dt=0.1"),
+    "c2": ("2d", (64, 64, 64, 64), 10 * math.pi, 8.0, 0.05, "two_stream", (0.001, 0.2, 2.4), "float32",
+           "2D2V two-stream 64^4, eps=0.001, k=0.2, v0=2.4, v in [-8,8], dt=0.05"),
+    "oned": ("1d", (4096, 4096), 4 * math.pi, 5.0, 0.05, "landau", (0.001, 0.5), "float32",
+             "1D1V Landau 4096x4096, eps=0.001, k=0.5, v in [-5,5], dt=0.05"),
+}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--dtype", choices=["float32", "bfloat16", "float64"], default="float32")
-    ap.add_argument("--size", type=int, default=128)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
+    ap.add_argument("--dtype", choices=["float32", "bfloat16", "float64"], default=None)
+    ap.add_argument("--size", type=int, default=None, help="override N of a 2D2V workload (N^4 grid)")
+    ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
-    return ap.parse_args()
+    a = ap.parse_args()
+    wl = WORKLOADS[a.workload]
+    a.kind, a.grid, a.L, a.vmax, a.dt, a.ic, a.icp, dflt, a.desc = wl
+    a.dtype = a.dtype or dflt
+    if a.size:
+        if a.kind != "2d":
+            raise SystemExit("--size applies to 2D2V workloads")
+        a.grid = (a.size,) * 4
+        a.desc = a.desc.replace("128^4", f"{a.size}^4")
+    return a
 
 
-def workload_name(n, dtype):
-    return f"2D2V Landau {n}x{n}x{n}x{n} {dtype} storage, eps={EPS}, k={KMODE}, v in [-6,6], dt={DT}"
+def short_dtype(name):
+    return {"float32": "f32", "bfloat16": "bf16", "float64": "f64"}[name]
 
 
 def measured_peak():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        with open(p) as fh:
-            d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
     except Exception:
         return PEAK_FALLBACK_GBS, "fallback"
 
 
-def ncu_traffic(kernel_tag):
-    """dram bytes per launch from a committed ncu summary (profiles/*.txt with a
-    'dram_bytes_per_launch: <n>' line), or None."""
-    p = os.path.join(ROOT, "profiles", f"traffic_{kernel_tag}.txt")
+def ncu_traffic(tag):
+    """DRAM bytes per launch from a committed ncu summary (a line
+    'dram_bytes_per_launch: <n>' in profiles/traffic_<tag>.txt), or None."""
     try:
-        with open(p) as fh:
+        with open(os.path.join(ROOT, "profiles", f"traffic_{tag}.txt")) as fh:
             for line in fh:
                 if line.startswith("dram_bytes_per_launch:"):
                     return float(line.split(":", 1)[1])
@@ -86,7 +103,8 @@ def ncu_traffic(kernel_tag):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons every 50 ms, stamped with the
+    host clock so that the summary covers the timed window."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -95,25 +113,29 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.samples = []
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except (OSError, FileNotFoundError):
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.samples.append((time.monotonic(), line.strip()))
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
 
     def __exit__(self, *a):
         if self.proc is not None:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -121,95 +143,105 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
+
+        def parse(lines):
+            sm, mx, reasons = [], None, set()
+            for _, ln in lines:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+            return sm, mx, reasons
+
+        window = "timed"
+        lines = self.samples
+        if self.window:
+            t0, t1 = self.window
+            inwin = [s for s in self.samples if t0 - 0.05 <= s[0] <= t1 + 0.05]
+            if len(inwin) >= 3:
+                lines = inwin
+            else:
+                window = "run (the timed region is shorter than three samples)"
+        sm, mx, reasons = parse(lines)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "window": window}
 
 
 # ---------------------------------------------------------------------------
 # CPU side (the oracle): cpu_baseline and --impl reference
 # ---------------------------------------------------------------------------
-def cpu_sample(n, dtype_name, budget_s, min_steps=1):
-    """Time the oracle's Strang step on (n, n, m, m) with m <= n chosen so the
-    timed steps take about budget_s. Returns (cells_per_step, steps, seconds, m)."""
+def _oracle_setup(a, grid):
     import numpy as np
 
     from oracle import core as O
 
-    npdt = np.float64 if dtype_name == "float64" else np.float32
-    # calibrate on a small grid
-    g = O.make_grid2d(n, n, 16, 16, LX, LX, VMAX, VMAX, dtype=npdt)
-    st = O.Stepper2D(g, DT, window=1)
-    f = O.landau_2d(g, EPS, KMODE)
+    npdt = np.float64 if a.dtype == "float64" else np.float32
+    if a.kind == "1d":
+        g = O.make_grid1d(grid[0], grid[1], a.L, a.vmax, dtype=npdt)
+        return O.Stepper1D(g, a.dt, window=1), O.landau_1d(g, a.icp[0], a.icp[1])
+    g = O.make_grid2d(*grid, a.L, a.L, a.vmax, a.vmax, dtype=npdt)
+    f = O.landau_2d(g, *a.icp) if a.ic == "landau" else O.two_stream_2d(g, *a.icp)
+    return O.Stepper2D(g, a.dt, window=1), f
+
+
+def cpu_sample_grid(a, budget_s):
+    """The largest sample of the workload (velocity dims reduced for 2D2V)
+    whose one step fits in budget_s on the host, from a small calibration."""
+    if a.kind == "1d":
+        return a.grid
+    n = a.grid[0]
+    st, f = _oracle_setup(a, (n, n, 16, 16))
     st.step(f)
     t0 = time.perf_counter()
     st.step(f)
     rate = (n * n * 256) / (time.perf_counter() - t0)
-    m = 16
-    for cand in (n, 96, 64, 48, 32, 24, 16):
-        if cand <= n and (n * n * cand * cand) / rate * min_steps <= budget_s:
-            m = cand
-            break
-    g = O.make_grid2d(n, n, m, m, LX, LX, VMAX, VMAX, dtype=npdt)
-    st = O.Stepper2D(g, DT, window=1)
-    f = O.landau_2d(g, EPS, KMODE)
-    f = st.step(f).f  # warm-up
-    steps = max(min_steps, int(budget_s / ((n * n * m * m) / rate)))
+    for m in (a.grid[2], 96, 64, 48, 32, 24, 16):
+        if m <= a.grid[2] and (n * n * m * m) / rate <= budget_s:
+            return (n, n, m, m)
+    return (n, n, 16, 16)
+
+
+def time_oracle(a, grid, steps, warmup):
+    st, f = _oracle_setup(a, grid)
+    for _ in range(warmup):
+        f = st.step(f).f
     t0 = time.perf_counter()
     for _ in range(steps):
         f = st.step(f).f
-    sec = time.perf_counter() - t0
-    return n * n * m * m, steps, sec, m
+    return time.perf_counter() - t0
 
 
-def run_reference(args):
-    rank = int(os.environ.get("RANK", 0))
-    if rank != 0:
+def run_reference(a):
+    if int(os.environ.get("RANK", 0)) != 0:
         return 0
     from oracle import core as O
 
-    n = args.size
-    cores = O.num_threads()
-    # each step is one Strang step of a bounded sample of the workload: the
-    # whole --warmup + --steps run is kept to about three minutes
-    per_step_budget = max(1.0, 150.0 / max(1, args.steps + args.warmup))
-    cells, _, sec, m = cpu_sample(n, args.dtype, per_step_budget)
-    import numpy as np
-
-    npdt = np.float64 if args.dtype == "float64" else np.float32
-    g = O.make_grid2d(n, n, m, m, LX, LX, VMAX, VMAX, dtype=npdt)
-    st = O.Stepper2D(g, DT, window=1)
-    f = O.landau_2d(g, EPS, KMODE)
-    for _ in range(args.warmup):
-        f = st.step(f).f
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        f = st.step(f).f
-    sec = time.perf_counter() - t0
-    value = cells * args.steps / sec
-    sample = (f"oracle Strang step (C+OpenMP restatement of vlasov_step_gather_free) on a "
-              f"{n}x{n}x{m}x{m} sample of the workload, {args.steps} steps after {args.warmup} warm-up")
+    # a bounded sample of the workload per step, so that --warmup + --steps
+    # stays within about three minutes
+    per_step = max(0.5, 150.0 / max(1, a.steps + a.warmup))
+    grid = cpu_sample_grid(a, per_step)
+    cells = math.prod(grid)
+    sec = time_oracle(a, grid, a.steps, a.warmup)
+    value = cells * a.steps / sec
+    sample = (f"oracle Strang step (C + OpenMP restatement of the reference's vlasov_step_gather_free) on a "
+              f"{'x'.join(map(str, grid))} sample of the workload, {a.steps} steps after {a.warmup} warm-up")
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.dtype != "float64"
-        else "f64", "data": "synthetic",
-        "config": {"workload": workload_name(n, args.dtype), "sample_grid": [n, n, m, m]},
-        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "port", "sample": sample},
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": short_dtype(a.dtype),
+        "data": "synthetic", "config": {"workload": a.desc + f", {a.dtype} storage", "sample_grid": list(grid)},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -219,167 +251,176 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU side
 # ---------------------------------------------------------------------------
-def run_ours(args):
+def _initial_f(a, dev, dtype, rank, torch):
+    """Initial condition built on the device (not timed)."""
+    gdt = torch.float64
+    eps = a.icp[0] * (1.0 + 0.01 * rank)  # each rank runs its own replica
+    if a.kind == "1d":
+        nx, nv = a.grid
+        x = torch.linspace(0, a.L, nx + 1, dtype=gdt, device=dev)[:-1]
+        v = torch.linspace(-a.vmax, a.vmax, nv, dtype=gdt, device=dev)
+        f = (1.0 + eps * torch.cos(a.icp[1] * x))[:, None] * torch.exp(-0.5 * v * v)[None, :] / math.sqrt(2 * math.pi)
+        return f.to(dtype).contiguous()
+    n, _, nv, _ = a.grid
+    x = torch.linspace(0, a.L, n + 1, dtype=gdt, device=dev)[:-1]
+    v = torch.linspace(-a.vmax, a.vmax, nv, dtype=gdt, device=dev)
+    k = a.icp[1]
+    sp = 1.0 + eps * (torch.cos(k * x)[:, None] + torch.cos(k * x)[None, :])
+    M = lambda u: torch.exp(-0.5 * u * u) / math.sqrt(2 * math.pi)  # noqa: E731
+    if a.ic == "landau":
+        fv = M(v)[:, None] * M(v)[None, :]
+    else:
+        fv = (0.5 * (M(v - a.icp[2]) + M(v + a.icp[2])))[:, None] * M(v)[None, :]
+    return (sp.float()[:, :, None, None] * fv.float()[None, None]).to(dtype).contiguous()
+
+
+def run_ours(a):
     import torch
 
     vp = importlib.import_module("jax-pytorch-vlasov_b200")
-    from importlib import import_module
-
-    dist = import_module("jax-pytorch-vlasov_b200.dist")
-    v2 = import_module("jax-pytorch-vlasov_b200.vlasov2d2v")
+    dist = importlib.import_module("jax-pytorch-vlasov_b200.dist")
     L = vp._lib
 
     rank, local, world = dist.init()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    n = args.size
-    dtype = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float64": torch.float64}[args.dtype]
+    dtype = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float64": torch.float64}[a.dtype]
     esz = {torch.float32: 4, torch.bfloat16: 2, torch.float64: 8}[dtype]
-    cells = n ** 4
-
-    st = vp.Stepper2D(n, n, n, n, LX, LX, VMAX, VMAX, DT, dtype=dtype, device=dev, physics_mode=True, window=1,
-                      diagnostics=True)
-    # Landau initial condition, built on the device (not timed); each rank runs
-    # an independent replica with its own amplitude
-    gdt = torch.float64
-    x = torch.linspace(0, LX, n + 1, dtype=gdt, device=dev)[:-1]
-    v = torch.linspace(-VMAX, VMAX, n, dtype=gdt, device=dev)
-    eps = EPS * (1.0 + 0.01 * rank)
-    sp = 1.0 + eps * (torch.cos(KMODE * x)[:, None] + torch.cos(KMODE * x)[None, :])
-    fv = torch.exp(-0.5 * (v[:, None] ** 2 + v[None, :] ** 2)) / (2.0 * math.pi)
-    f = (sp.float()[:, :, None, None] * fv.float()[None, None]).to(dtype).contiguous()
-    del sp, fv
+    cells = math.prod(a.grid)
+    big = cells * esz > 256 * 2 ** 20
+    if a.kind == "1d":
+        st = vp.Stepper1D(*a.grid, a.L, a.vmax, a.dt, dtype=dtype, device=dev, window=1, diagnostics=a.diagnostics)
+        n_sweeps = 3
+    else:
+        st = vp.Stepper2D(*a.grid, a.L, a.L, a.vmax, a.vmax, a.dt, dtype=dtype, device=dev, window=1,
+                          diagnostics=a.diagnostics)
+        n_sweeps = 5
+    f = _initial_f(a, dev, dtype, rank, torch)
     b = st.empty_f()
-    diag = torch.zeros((max(args.steps, 1), L.DIAG_COUNT), dtype=torch.float64, device=dev)
+    K = max(a.steps, 1)
+    hist = torch.zeros((K, L.DIAG_COUNT), dtype=torch.float64, device=dev)
+    use_events = a.kind == "2d" and big  # per-phase events on the big grid; graphs for the small ones
 
-    # per-phase timing events recorded by the library inside each step
     nph = len(PHASES)
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * nph)] for _ in range(args.steps)]
-    for row in evs:  # materialise the CUDA events
-        for e in row:
-            e.record()
-    torch.cuda.synchronize(dev)
-    ev_arrays = [(ctypes.c_void_p * (2 * nph))(*[e.cuda_event for e in row]) for row in evs]
+    if use_events:
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * nph)] for _ in range(K)]
+        for row in evs:  # materialise the CUDA events before handing them to the library
+            for e in row:
+                e.record()
+        torch.cuda.synchronize(dev)
+        ev_arrays = [(ctypes.c_void_p * (2 * nph))(*[e.cuda_event for e in row]) for row in evs]
 
-    def step(a, bb, i, timed):
-        d = st._desc(a, bb, diag[i] if timed else diag[0])
-        if timed:
+    def step(x, y, i, timed):
+        d = st._desc(x, y, hist[i] if timed else hist[0])
+        if timed and use_events:
             d.events = ctypes.cast(ev_arrays[i], ctypes.c_void_p)
-        L.call("vp_step2d", ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        name = "vp_step1d" if a.kind == "1d" else "vp_step2d"
+        L.call(name, ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
 
-    a = f
-    for i in range(args.warmup):
-        step(a, b, 0, False)
-        a, b = b, a
-    torch.cuda.synchronize(dev)
-    dist.barrier()
-    torch.cuda.synchronize(dev)
-    launches0 = L.load().vp_launch_count()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        x, y = f, b
+        if use_events or a.kind == "1d":
+            for i in range(a.warmup):
+                step(x, y, 0, False)
+                x, y = y, x
+        else:
+            x = st.run(x, max(a.warmup, 4), graph=True, graph_chunk=10)  # also captures the graph
+        torch.cuda.synchronize(dev)
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        launches0 = L.load().vp_launch_count()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        h0 = time.monotonic()
         t_start.record()
-        for i in range(args.steps):
-            step(a, b, i, True)
-            a, b = b, a
+        if use_events or a.kind == "1d":
+            for i in range(K):
+                step(x, y, i, True)
+                x, y = y, x
+        else:
+            x = st.run(x, K, history=hist, graph=True, graph_chunk=10)
         t_end.record()
         torch.cuda.synchronize(dev)
-    launches = L.load().vp_launch_count() - launches0
+        clk.mark(h0, time.monotonic())
+        launches = L.load().vp_launch_count() - launches0
     dist.barrier()
     torch.cuda.synchronize(dev)
     ms = t_start.elapsed_time(t_end)
     ms_max = dist.max_over_ranks(ms)
-    value = world * cells * args.steps / (ms_max / 1e3)
-
-    # phase durations (ms), averaged over the timed steps
-    ph = {p: 0.0 for p in PHASES}
-    for row in evs:
-        for j, p in enumerate(PHASES):
-            ph[p] += row[2 * j].elapsed_time(row[2 * j + 1]) / args.steps
+    value = world * cells * K / (ms_max / 1e3)
     sweep_bytes = 2.0 * esz * cells  # read f once + write f once per sweep
-    phase_gbs = {p: (sweep_bytes / (ph[p] * 1e-3) / 1e9 if ph[p] > 0 and p not in ("field", "diag") else None)
-                 for p in PHASES}
-    # dominant kernel: the x drift (two launches per step) or the largest phase
-    groups = {"drift_x": ph["drift_x1"] + ph["drift_x2"], "drift_y_rho": ph["drift_y1_rho"],
-              "kick_vx_vy": ph["kick_vx_vy"], "drift_y": ph["drift_y2"]}
-    dom = max(groups, key=groups.get)
-    dom_launch_ms = groups[dom] / (2 if dom == "drift_x" else 1)
     peak, peak_kind = measured_peak()
-    achieved = sweep_bytes / (dom_launch_ms * 1e-3) / 1e9
-    traffic = ncu_traffic(f"{dom}_{n}x{n}x{n}x{n}_{args.dtype}")
+    ms_step = ms_max / K
 
-    hist = diag[: args.steps].cpu()
-    we = hist[:, 0]
-    finite = bool(torch.isfinite(hist[:, :2]).all())  # field energy and mass (level-1 diagnostics)
+    ph = None
+    phase_gbs = None
+    if use_events:
+        ph = {p: 0.0 for p in PHASES}
+        for row in evs:
+            for j, p in enumerate(PHASES):
+                ph[p] += row[2 * j].elapsed_time(row[2 * j + 1]) / K
+        phase_gbs = {p: (sweep_bytes / (ph[p] * 1e-3) / 1e9 if ph[p] > 0 and p not in ("field", "diag") else None)
+                     for p in PHASES}
+        groups = {"drift_x": ph["drift_x1"] + ph["drift_x2"], "drift_y_rho": ph["drift_y1_rho"],
+                  "kick_vx_vy": ph["kick_vx_vy"], "drift_y": ph["drift_y2"]}
+        dom = max(groups, key=groups.get)
+        dom_ms = groups[dom] / (2 if dom == "drift_x" else 1)
+        achieved = sweep_bytes / (dom_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": ncu_traffic(f"{dom}_{'x'.join(map(str, a.grid))}_{a.dtype}"),
+                "algorithmic_bytes_per_launch": sweep_bytes}
+    else:
+        # graph-replayed small grids: whole-step bandwidth (the f-sized sweeps
+        # dominate; the grid fits the L2, so this may exceed the HBM figure)
+        achieved = n_sweeps * sweep_bytes / (ms_step * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "whole step (graph replay)", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": n_sweeps * sweep_bytes,
+                "note": "f fits the 126 MB L2" if cells * esz * 3 < 126e6 else ""}
+
+    h = hist[:K].cpu()
+    finite = bool(torch.isfinite(h[:, :2]).all())
 
     # end to end through the public API with pinned host buffers: every step
-    # copies its input f host->device, runs the drop-in step function and
-    # copies the resulting f and diagnostics back
+    # copies its input f host->device, runs the drop-in step function, and
+    # copies the resulting f and mid-step density back
     e2e = None
-    if args.e2e_steps > 0:
-        g = v2.Grid.create(n, n, n, n, LX, LX, VMAX, VMAX, device=dev,
-                           dtype=torch.float64 if dtype == torch.float64 else torch.float32)
-        h_in = a.cpu().pin_memory()
-        h_out = torch.empty_like(h_in).pin_memory()
-        h_rho = torch.empty((n, n), dtype=torch.float64 if dtype == torch.float64 else torch.float32).pin_memory()
-        d_in = torch.empty_like(a)
-        f0 = torch.zeros((n, n), device=dev)
-
-        def e2e_step():
-            d_in.copy_(h_in, non_blocking=True)
-            fo, rho, phi = v2.vlasov_step_gather_free(
-                d_in, f0, DT, g.x, g.y, g.vx, g.vy, g.kx, g.ky, g.inv_ksq, g.x_indices, g.y_indices, g.vx_indices,
-                g.vy_indices, g.stencil_offsets, g.dx, g.dy, g.dvx, g.dvy, g.Nx, g.Ny, True, 1)
-            h_out.copy_(fo, non_blocking=True)
-            h_rho.copy_(rho, non_blocking=True)
-
-        e2e_step()
-        torch.cuda.synchronize(dev)
-        dist.barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.e2e_steps):
-            e2e_step()
-        e1.record()
-        torch.cuda.synchronize(dev)
-        ems = dist.max_over_ranks(e0.elapsed_time(e1))
-        e2e = {"value": world * cells * args.e2e_steps / (ems / 1e3), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": h_in.numel() * h_in.element_size(),
-               "d2h_bytes_per_step": h_out.numel() * h_out.element_size() + h_rho.numel() * h_rho.element_size(),
-               "steps": args.e2e_steps, "path": "vlasov2d2v.vlasov_step_gather_free with pinned host f in/out"}
+    if a.e2e_steps > 0:
+        e2e = run_e2e(a, x, dev, dtype, world, dist, torch, vp)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
         from oracle import core as O
 
-        c_cells, c_steps, c_sec, m = cpu_sample(n, args.dtype, args.cpu_budget)
-        cpu = {"value": c_cells * c_steps / c_sec, "unit": "cell-updates/s", "cores": O.num_threads(),
+        grid = cpu_sample_grid(a, a.cpu_budget / 2)
+        c_steps = 2
+        sec = time_oracle(a, grid, c_steps, 1)
+        cpu = {"value": math.prod(grid) * c_steps / sec, "unit": "cell-updates/s", "cores": O.num_threads(),
                "kind": "port",
-               "sample": f"oracle Strang step on a {n}x{n}x{m}x{m} sample, {c_steps} step(s), {c_sec:.1f} s"}
+               "sample": f"oracle Strang step on a {'x'.join(map(str, grid))} sample, {c_steps} steps, {sec:.1f} s"}
 
     if rank == 0:
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"float32": "f32", "bfloat16": "bf16", "float64": "f64"}[args.dtype], "data": "synthetic",
-            "config": {"workload": workload_name(n, args.dtype), "grid": [n, n, n, n], "global_batch": world,
+            "steps": K, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": short_dtype(a.dtype), "data": "synthetic",
+            "config": {"workload": a.desc + f", {a.dtype} storage", "grid": list(a.grid), "global_batch": world,
                        "parallelism": f"{world} independent replicas" if world > 1 else "single run",
-                       "l2_flush": "not needed: f is 1 GiB per buffer, 8x the L2"
-                       if n >= 128 else "inputs smaller than L2"},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": sweep_bytes},
-            "phases_ms": ph, "phases_gbs": phase_gbs,
-            "step_gbs_5pass": 5 * sweep_bytes / (ms_max / args.steps * 1e-3) / 1e9,
+                       "l2_flush": "not needed: f exceeds the L2 several times" if big
+                       else "none: the whole state is L2-resident (launch/latency-bound size)",
+                       "diagnostics_level": a.diagnostics},
+            "roofline": roof,
+            "step_gbs": n_sweeps * sweep_bytes / (ms_step * 1e-3) / 1e9,
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "diagnostics": {"field_energy_first": float(we[0]), "field_energy_last": float(we[-1]),
-                            "mass_drift_rel": float((hist[-1, 1] - hist[0, 1]) / hist[0, 1]),
-                            "finite": finite},
+            "diagnostics": {"field_energy_first": float(h[0, 0]), "field_energy_last": float(h[-1, 0]),
+                            "mass_drift_rel": float((h[-1, 1] - h[0, 1]) / h[0, 1]), "finite": finite},
         }
+        if ph is not None:
+            line["phases_ms"] = ph
+            line["phases_gbs"] = phase_gbs
         clk_s = clk.summary()
         if clk_s:
             line["clocks"] = clk_s
@@ -388,11 +429,62 @@ def run_ours(args):
     return 0
 
 
+def run_e2e(a, f_dev, dev, dtype, world, dist, torch, vp):
+    cells = math.prod(a.grid)
+    gdt = torch.float64 if dtype == torch.float64 else torch.float32
+    h_in = f_dev.cpu().pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    d_in = torch.empty_like(f_dev)
+    if a.kind == "1d":
+        m = importlib.import_module("jax-pytorch-vlasov_b200.vlasov1d1v")
+        g = m.Grid.create(*a.grid, a.L, a.vmax, device=dev, dtype=gdt)
+        h_rho = torch.empty(a.grid[0], dtype=gdt).pin_memory()
+
+        def call():
+            return m.vlasov_step_gather_free(d_in, a.dt, g.v, g.inv_kx, g.inv_kx_sq, g.x_indices, g.v_indices,
+                                             g.x_batch_offsets, g.v_batch_offsets, g.stencil_offsets, g.dx, g.dv,
+                                             g.V_max, True, 1)
+        path = "vlasov1d1v.vlasov_step_gather_free with pinned host f in/out"
+    else:
+        m = importlib.import_module("jax-pytorch-vlasov_b200.vlasov2d2v")
+        g = m.Grid.create(*a.grid, a.L, a.L, a.vmax, a.vmax, device=dev, dtype=gdt)
+        h_rho = torch.empty(a.grid[:2], dtype=gdt).pin_memory()
+        f0 = torch.zeros(a.grid[2:], dtype=gdt, device=dev)
+
+        def call():
+            return m.vlasov_step_gather_free(d_in, f0, a.dt, g.x, g.y, g.vx, g.vy, g.kx, g.ky, g.inv_ksq,
+                                             g.x_indices, g.y_indices, g.vx_indices, g.vy_indices,
+                                             g.stencil_offsets, g.dx, g.dy, g.dvx, g.dvy, g.Nx, g.Ny, True, 1)
+        path = "vlasov2d2v.vlasov_step_gather_free with pinned host f in/out"
+
+    def e2e_step():
+        d_in.copy_(h_in, non_blocking=True)
+        fo, rho, _ = call()
+        h_out.copy_(fo, non_blocking=True)
+        h_rho.copy_(rho, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.e2e_steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ems = dist.max_over_ranks(e0.elapsed_time(e1))
+    return {"value": world * cells * a.e2e_steps / (ems / 1e3), "unit": "cell-updates/s",
+            "h2d_bytes_per_step": h_in.numel() * h_in.element_size(),
+            "d2h_bytes_per_step": h_out.numel() * h_out.element_size() + h_rho.numel() * h_rho.element_size(),
+            "steps": a.e2e_steps, "path": path}
+
+
 def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
-    return run_ours(args)
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
 
 
 if __name__ == "__main__":

@@ -15,7 +15,104 @@ from . import _lib as L
 from . import ops
 
 
-class Stepper2D:
+class _Stepper:
+    """Shared run loop: eager steps, or chunks of `graph_chunk` steps captured
+    once per (input buffer, output buffer) pair and replayed."""
+
+    _lib_fn = ""
+
+    def _init_common(self, dtype, device, physics_mode, window, diagnostics):
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError(f"{type(self).__name__} runs on a CUDA device only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.dtype = dtype
+        self.physics_mode = bool(physics_mode)
+        self.window = int(window)
+        self.diagnostics = int(diagnostics)  # 0 none, 1 field energy + mass, 2 + L2 / kinetic moments
+        self.diag = torch.zeros(L.DIAG_COUNT, dtype=torch.float64, device=self.device)
+        self._graphs = {}
+        self._bufs = [None, None]
+
+    def empty_f(self) -> torch.Tensor:
+        return torch.empty(self.shape, dtype=self.dtype, device=self.device)
+
+    def _check(self, f):
+        if (tuple(f.shape) != self.shape or f.dtype != self.dtype or f.device != self.device
+                or not f.is_contiguous()):
+            raise ValueError(f"f must be a contiguous {self.dtype} tensor of shape {self.shape} on {self.device}")
+
+    def _desc(self, f_in, f_out, diag):
+        raise NotImplementedError
+
+    def step(self, f_in: torch.Tensor, f_out: torch.Tensor | None = None, diag: torch.Tensor | None = None):
+        """One Strang step f_in -> f_out (a new tensor if None). Mid-step
+        fields land in the stepper's field buffers; diagnostics in `diag`
+        (default self.diag) when enabled."""
+        self._check(f_in)
+        f_out = self.empty_f() if f_out is None else f_out
+        self._check(f_out)
+        if diag is None and self.diagnostics:
+            diag = self.diag
+        desc = self._desc(f_in, f_out, diag)
+        L.call(self._lib_fn, ctypes.byref(desc), ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+        return f_out
+
+    def _partner(self, f):
+        """A persistent second buffer distinct from f (and from f_tmp)."""
+        if self._bufs[0] is None:
+            self._bufs[0] = self.empty_f()
+        if f.data_ptr() == self._bufs[0].data_ptr():
+            if self._bufs[1] is None:
+                self._bufs[1] = self.empty_f()
+            return self._bufs[1]
+        return self._bufs[0]
+
+    def run(self, f: torch.Tensor, nsteps: int, history: torch.Tensor | None = None, graph: bool = False,
+            graph_chunk: int = 10) -> torch.Tensor:
+        """Advance f by nsteps and return the buffer holding the result (f
+        itself after an even number of steps). history: optional float64
+        [nsteps, VP_DIAG_COUNT] per-step diagnostics."""
+        self._check(f)
+        a, b = f, self._partner(f)
+        done = 0
+        if graph:
+            k = max(2, graph_chunk + (graph_chunk & 1))  # even: every replay returns to `a`
+            while nsteps - done >= k:
+                key = (a.data_ptr(), b.data_ptr(), k)
+                entry = self._graphs.get(key)
+                if entry is None:
+                    stage = torch.zeros((k, L.DIAG_COUNT), dtype=torch.float64, device=self.device)
+                    s = torch.cuda.Stream(self.device)
+                    s.wait_stream(torch.cuda.current_stream(self.device))
+                    with torch.cuda.stream(s):  # first launches outside the capture
+                        self.step(a, b, stage[0])
+                        self.step(b, a, stage[1])
+                    torch.cuda.current_stream(self.device).wait_stream(s)
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g):
+                        x, y = a, b
+                        for i in range(k):
+                            self.step(x, y, stage[i])
+                            x, y = y, x
+                    self._graphs[key] = (g, stage)
+                    if history is not None:
+                        history[done: done + 2].copy_(stage[:2])
+                    done += 2  # the two launches before the capture advanced the state
+                    continue
+                g, stage = entry
+                g.replay()
+                if history is not None:
+                    history[done: done + k].copy_(stage)
+                done += k
+        for i in range(done, nsteps):
+            self.step(a, b, history[i] if history is not None else None)
+            a, b = b, a
+        return a
+
+
+class Stepper2D(_Stepper):
     """One 2D2V configuration: grid sizes, extents, dt and storage dtype.
 
     The velocity grids are built as Grid.create builds them
@@ -24,15 +121,15 @@ class Stepper2D:
     storage dtype's precision exactly as precompute_x_drift does.
     window: kick window S (-1: exact kick for any |E dt/dv|; the reference
     solver 2 uses S = 1, which equals the exact kick while |E dt/dv| < 1).
+    diagnostics: 0 none, 1 field energy / mass / max shift, 2 also the L2 and
+    kinetic moments after the kicks.
     """
 
+    _lib_fn = "vp_step2d"
+
     def __init__(self, Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt, dtype=torch.float32, device="cuda",
-                 physics_mode=True, window=-1, diagnostics=True, vx=None, vy=None):
-        self.device = torch.device(device)
-        if self.device.type != "cuda":
-            raise ValueError("Stepper2D runs on a CUDA device only")
-        if self.device.index is None:
-            self.device = torch.device("cuda", torch.cuda.current_device())
+                 physics_mode=True, window=-1, diagnostics=1, vx=None, vy=None):
+        self._init_common(dtype, device, physics_mode, window, diagnostics)
         self.shape = (int(Nx), int(Ny), int(Nvx), int(Nvy))
         self.Lx, self.Ly = float(Lx), float(Ly)
         self.dx, self.dy = self.Lx / Nx, self.Ly / Ny
@@ -42,11 +139,7 @@ class Stepper2D:
         vy_t = (torch.linspace(-Vy_max, Vy_max, Nvy, dtype=grid_dt) if vy is None
                 else torch.as_tensor(vy).detach().cpu())
         self.dt = float(dt)
-        self.dtype = dtype
-        self.physics_mode = bool(physics_mode)
-        self.window = int(window)
-        self.diagnostics = int(diagnostics)  # 0 none, 1 field energy + mass, 2 + L2 / kinetic moments
-        self.set_spacings(2 * Vx_max / (Nvx - 1), 2 * Vy_max / (Nvy - 1))
+        self.dvx, self.dvy = 2 * Vx_max / (Nvx - 1), 2 * Vy_max / (Nvy - 1)
         self.tx = ops.DriftTable.from_velocity(vx_t, self.dt / 2.0, self.dx, dtype, self.device)
         self.ty = ops.DriftTable.from_velocity(vy_t, self.dt / 2.0, self.dy, dtype, self.device)
         self.kx, self.ky, self.inv_ksq = ops.spectral_2d(Nx, Ny, self.Lx, self.Ly, self.device)
@@ -54,18 +147,9 @@ class Stepper2D:
         self.vy64 = vy_t.to(torch.float64).to(self.device)
         nb = L.query("vp_step2d_workspace_bytes", *self.shape)
         self.ws = torch.empty(nb, dtype=torch.uint8, device=self.device)
-        self.f_tmp = torch.empty(self.shape, dtype=dtype, device=self.device)
+        self.f_tmp = self.empty_f()
         z = lambda: torch.zeros((Nx, Ny), dtype=torch.float64, device=self.device)  # noqa: E731
         self.drho, self.phi, self.ex, self.ey = z(), z(), z(), z()
-        self.diag = torch.zeros(L.DIAG_COUNT, dtype=torch.float64, device=self.device)
-        self._graph = None
-
-    def set_spacings(self, dvx: float, dvy: float) -> None:
-        """Velocity spacings used by the kicks (defaults: from the grids)."""
-        self.dvx, self.dvy = float(dvx), float(dvy)
-
-    def empty_f(self) -> torch.Tensor:
-        return torch.empty(self.shape, dtype=self.dtype, device=self.device)
 
     def _desc(self, f_in, f_out, diag) -> L.Step2dDesc:
         d = L.Step2dDesc()
@@ -87,77 +171,16 @@ class Stepper2D:
         d.workspace, d.workspace_bytes = self.ws.data_ptr(), self.ws.numel()
         return d
 
-    def _check(self, f):
-        if f.shape != self.shape or f.dtype != self.dtype or f.device != self.device or not f.is_contiguous():
-            raise ValueError(f"f must be a contiguous {self.dtype} tensor of shape {self.shape} on {self.device}")
 
-    def step(self, f_in: torch.Tensor, f_out: torch.Tensor | None = None, diag: torch.Tensor | None = None):
-        """One Strang step f_in -> f_out (new tensor if None). Mid-step fields
-        land in self.drho / self.phi / self.ex / self.ey; diagnostics in diag
-        (default self.diag) when enabled."""
-        self._check(f_in)
-        f_out = self.empty_f() if f_out is None else f_out
-        self._check(f_out)
-        if diag is None and self.diagnostics:
-            diag = self.diag
-        desc = self._desc(f_in, f_out, diag)
-        L.call("vp_step2d", ctypes.byref(desc), ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
-        return f_out
+class Stepper1D(_Stepper):
+    """One 1D1V configuration (f is (Nx, Nv), v contiguous); grids as
+    Grid.create builds them (vlasov1D1V.py:95-122)."""
 
-    def run(self, f: torch.Tensor, nsteps: int, history: torch.Tensor | None = None, graph: bool = False,
-            graph_chunk: int = 10) -> torch.Tensor:
-        """Advance f by nsteps; returns the buffer holding the result (f or a
-        second buffer). history: optional float64 [nsteps, 8] diagnostics."""
-        self._check(f)
-        a, b = f, self.empty_f()
-        if not graph:
-            for i in range(nsteps):
-                self.step(a, b, history[i] if history is not None else None)
-                a, b = b, a
-            return a
-        # capture graph_chunk steps (even, so buffers return to a)
-        k = max(2, graph_chunk + (graph_chunk & 1))
-        stage = torch.zeros((k, L.DIAG_COUNT), dtype=torch.float64, device=self.device)
-        done = 0
-        while nsteps - done >= k:
-            if self._graph is None or self._graph[1] != (a.data_ptr(), b.data_ptr(), k):
-                g = torch.cuda.CUDAGraph()
-                s = torch.cuda.Stream(self.device)
-                s.wait_stream(torch.cuda.current_stream(self.device))
-                with torch.cuda.stream(s):
-                    # warm (outside capture) once so lazy driver setup happens first
-                    self.step(a, b, stage[0])
-                    self.step(b, a, stage[1])
-                torch.cuda.current_stream(self.device).wait_stream(s)
-                with torch.cuda.graph(g):
-                    x, y = a, b
-                    for i in range(k):
-                        self.step(x, y, stage[i])
-                        x, y = y, x
-                self._graph = (g, (a.data_ptr(), b.data_ptr(), k), stage)
-                done += 2  # the warm-up steps advanced the state
-                if history is not None:
-                    history[done - 2: done].copy_(stage[:2])
-                continue
-            g, _, stage = self._graph
-            g.replay()
-            if history is not None:
-                history[done: done + k].copy_(stage)
-            done += k
-        for i in range(done, nsteps):
-            self.step(a, b, history[i] if history is not None else None)
-            a, b = b, a
-        return a
-
-
-class Stepper1D:
-    """One 1D1V configuration (f is (Nx, Nv), v contiguous)."""
+    _lib_fn = "vp_step1d"
 
     def __init__(self, Nx, Nv, L_, V_max, dt, dtype=torch.float32, device="cuda", physics_mode=True, window=-1,
-                 diagnostics=True, v=None):
-        self.device = torch.device(device)
-        if self.device.index is None:
-            self.device = torch.device("cuda", torch.cuda.current_device())
+                 diagnostics=1, v=None):
+        self._init_common(dtype, device, physics_mode, window, diagnostics)
         self.shape = (int(Nx), int(Nv))
         self.L = float(L_)
         self.dx = self.L / Nx
@@ -165,33 +188,17 @@ class Stepper1D:
         v_t = torch.linspace(-V_max, V_max, Nv, dtype=grid_dt) if v is None else torch.as_tensor(v).detach().cpu()
         self.dv = 2 * V_max / (Nv - 1)
         self.dt = float(dt)
-        self.dtype = dtype
-        self.physics_mode = bool(physics_mode)
-        self.window = int(window)
-        self.diagnostics = int(diagnostics)
         self.table = ops.DriftTable.from_velocity(v_t, self.dt / 2.0, self.dx, dtype, self.device)
         self.inv_kx, self.inv_kx_sq = ops.spectral_1d(Nx, self.L, self.device)
         self.v64 = v_t.to(torch.float64).to(self.device)
         nb = L.query("vp_step1d_workspace_bytes", *self.shape)
         self.ws = torch.empty(nb, dtype=torch.uint8, device=self.device)
-        self.f_tmp = torch.empty(self.shape, dtype=dtype, device=self.device)
+        self.f_tmp = self.empty_f()
         self.rho = torch.zeros(Nx, dtype=torch.float64, device=self.device)
         self.phi = torch.zeros_like(self.rho)
         self.e = torch.zeros_like(self.rho)
-        self.diag = torch.zeros(L.DIAG_COUNT, dtype=torch.float64, device=self.device)
 
-    def set_dv(self, dv: float) -> None:
-        self.dv = float(dv)
-
-    def empty_f(self):
-        return torch.empty(self.shape, dtype=self.dtype, device=self.device)
-
-    def step(self, f_in, f_out=None, diag=None):
-        if f_in.shape != self.shape or f_in.dtype != self.dtype or not f_in.is_cuda or not f_in.is_contiguous():
-            raise ValueError(f"f must be a contiguous {self.dtype} CUDA tensor of shape {self.shape}")
-        f_out = self.empty_f() if f_out is None else f_out
-        if diag is None and self.diagnostics:
-            diag = self.diag
+    def _desc(self, f_in, f_out, diag) -> L.Step1dDesc:
         d = L.Step1dDesc()
         d.dtype = L.dtype_code(self.dtype)
         d.nx, d.nv = self.shape
@@ -206,12 +213,4 @@ class Stepper1D:
         d.rho, d.phi, d.e = self.rho.data_ptr(), self.phi.data_ptr(), self.e.data_ptr()
         d.diag = diag.data_ptr() if diag is not None else None
         d.workspace, d.workspace_bytes = self.ws.data_ptr(), self.ws.numel()
-        L.call("vp_step1d", ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
-        return f_out
-
-    def run(self, f, nsteps, history=None):
-        a, b = f, self.empty_f()
-        for i in range(nsteps):
-            self.step(a, b, history[i] if history is not None else None)
-            a, b = b, a
-        return a
+        return d

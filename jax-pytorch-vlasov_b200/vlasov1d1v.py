@@ -210,6 +210,8 @@ def _fused(f, dt, table, grid_inv_kx, grid_inv_kx_sq, grid_dx, grid_dv, physics_
         st.phi = torch.zeros_like(st.rho)
         st.e = torch.zeros_like(st.rho)
         st.diag = None
+        st._graphs = {}
+        st._bufs = [None, None]
         if len(_PLANS) > 16:
             _PLANS.clear()
         _PLANS[key] = st

@@ -323,7 +323,8 @@ def _fused_step(f, dt, tables, spectral, grid_dx, grid_dy, grid_dvx, grid_dvy, p
         z = lambda: torch.zeros((Nx, Ny), dtype=torch.float64, device=f.device)  # noqa: E731
         st.drho, st.phi, st.ex, st.ey = z(), z(), z(), z()
         st.diag = None
-        st._graph = None
+        st._graphs = {}
+        st._bufs = [None, None]
         if len(_PLANS) > 16:
             _PLANS.clear()
         _PLANS[key] = plan = st
