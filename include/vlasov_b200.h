@@ -232,6 +232,19 @@ typedef struct vp_step2d_desc {
     void* workspace;
     size_t workspace_bytes;
     void* const* events;    /* optional [2*VP_PHASE_COUNT] cudaEvent_t, NULL to skip */
+    /* Equilibrium split (optional, both NULL to disable): f = feq + g with a
+     * separable equilibrium feq(vx, vy) = eq_vx[ivx] * eq_vy[ivy] (double).
+     * f_in / f_out / f_tmp then hold g, and every sweep advances g so that
+     * feq + g follows the unsplit step exactly in exact arithmetic (the
+     * drifts add feq*(sum of weights - 1), the kicks add the kicked
+     * equilibrium minus feq). The stored precision then applies to the
+     * perturbation instead of f. eq_moment = sum(eq_vx)*dvx * sum(eq_vy)*dvy
+     * (the equilibrium's density, added to rho). Needs the fused kick (a
+     * plane row of at most 128 elements per warp). No reference counterpart:
+     * the reference stores the full f. */
+    const double* eq_vx;
+    const double* eq_vy;
+    double eq_moment;
 } vp_step2d_desc;
 
 int vp_step2d(const vp_step2d_desc* desc, void* stream);
@@ -263,6 +276,10 @@ typedef struct vp_step1d_desc {
     void* workspace;
     size_t workspace_bytes;
     void* const* events; /* optional [2*VP_PHASE_COUNT] cudaEvent_t */
+    /* Equilibrium split (optional): f = eq_v[iv] + g, as in vp_step2d_desc;
+     * eq_moment = sum(eq_v) * dv. */
+    const double* eq_v;
+    double eq_moment;
 } vp_step1d_desc;
 
 int vp_step1d(const vp_step1d_desc* desc, void* stream);

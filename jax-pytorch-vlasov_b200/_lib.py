@@ -54,6 +54,7 @@ class Step2dDesc(ctypes.Structure):
         ("kx", P), ("ky", P), ("inv_ksq", P), ("vx", P), ("vy", P),
         ("drho", P), ("phi", P), ("ex", P), ("ey", P), ("diag", P),
         ("workspace", P), ("workspace_bytes", SZ), ("events", P),
+        ("eq_vx", P), ("eq_vy", P), ("eq_moment", D),
     ]
 
 
@@ -66,6 +67,7 @@ class Step1dDesc(ctypes.Structure):
         ("shift", P), ("W", P), ("inv_kx", P), ("inv_kx_sq", P), ("v", P),
         ("rho", P), ("phi", P), ("e", P), ("diag", P),
         ("workspace", P), ("workspace_bytes", SZ), ("events", P),
+        ("eq_v", P), ("eq_moment", D),
     ]
 
 

@@ -163,7 +163,7 @@ int vp_drift(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t 
     VP_CHECK(n_outer > 0 && n_line > 0 && n_inner > 0 && sel_div > 0 && sel_mod > 0, "vp_drift: bad size");
     VP_CHECK(n_line < (1 << 30), "vp_drift: line too long");
     return run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, false, sel_div, sel_mod, shift_spread, shift, W, nullptr, 0,
-                       1, 0.0, 1.0, -1, nullptr, nullptr, S(stream));
+                       1, 0.0, 1.0, -1, nullptr, nullptr, EQ_NONE, S(stream));
 }
 
 size_t vp_drift_rho_workspace_bytes(int64_t n_outer, int64_t n_line, int64_t n_inner) {
@@ -184,9 +184,9 @@ int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int6
     int tiles = 0;
     double* part = static_cast<double*>(workspace);
     int rc = run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, false, sel_div, sel_mod, shift_spread, shift, W, nullptr,
-                         0, 1, 0.0, 1.0, -1, part, &tiles, S(stream));
+                         0, 1, 0.0, 1.0, -1, part, &tiles, EQ_NONE, S(stream));
     if (rc) return rc;
-    return run_rho_finalize(part, n_outer, n_line, tiles, scale, rho, S(stream));
+    return run_rho_finalize(part, n_outer, n_line, tiles, scale, 0.0, rho, S(stream));
 }
 
 int vp_kick(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line, int64_t n_inner,
@@ -200,9 +200,10 @@ int vp_kick(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n
     VP_CHECK(n_line < (1 << 30), "vp_kick: line too long");
     const int e_f64 = e_dtype == VP_F64;
     if (n_inner == 1)
-        return run_kick_contig(dtype, f_in, f_out, n_outer, n_line, E, e_f64, e_div, dt, dv, window, S(stream));
+        return run_kick_contig(dtype, f_in, f_out, n_outer, n_line, E, e_f64, e_div, dt, dv, window, EQ_NONE,
+                               S(stream));
     return run_strided(dtype, f_in, f_out, n_outer, n_line, n_inner, true, 1, 1, -1, nullptr, nullptr, E, e_f64, e_div,
-                       dt, dv, window, nullptr, nullptr, S(stream));
+                       dt, dv, window, nullptr, nullptr, EQ_NONE, S(stream));
 }
 
 int vp_kick2d(const void* f_in, void* f_out, int dtype, int64_t n_planes, int64_t nvx, int64_t nvy,
@@ -215,7 +216,7 @@ int vp_kick2d(const void* f_in, void* f_out, int dtype, int64_t n_planes, int64_
     VP_CHECK(dvx != 0.0 && dvy != 0.0, "vp_kick2d: zero velocity spacing");
     VP_CHECK(!moments || (vx && vy), "vp_kick2d: moments need vx and vy");
     const int rc = run_kick2d(dtype, f_in, f_out, n_planes, nvx, nvy, Ex, Ey, dt, dvx, dvy, window, vx, vy, moments,
-                              S(stream));
+                              EQ_NONE, S(stream));
     if (rc == VP_ERR_UNSUPPORTED) return set_error(rc, "vp_kick2d: nvy too wide for one warp per plane row");
     return rc;
 }
@@ -310,6 +311,12 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     const bool want_rho = phys || want_diag;
     // both kicks in one pass when a plane row fits one warp, else two sweeps
     const bool fused = kick2d_fits(d->dtype, nvy, d->f_in, d->f_out, d->f_tmp);
+    const bool eq_on = d->eq_vx || d->eq_vy;
+    VP_CHECK(!eq_on || (d->eq_vx && d->eq_vy), "vp_step2d: the equilibrium split needs eq_vx and eq_vy");
+    if (eq_on && phys && !fused)
+        return set_error(VP_ERR_UNSUPPORTED, "vp_step2d: the equilibrium split needs the fused kick (nvy <= 128)");
+    const EqSplit eqs{d->eq_vx, d->eq_vy, nvx, nvy};
+    const EqSplit* EQ = eq_on ? &eqs : EQ_NONE;
     const int n_sweeps = phys ? (fused ? 5 : 6) : 4;
     int i = 0;
     auto dst_of = [&](int k) -> void* { return ((n_sweeps - 1 - k) % 2 == 0) ? d->f_out : d->f_tmp; };
@@ -320,7 +327,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     if ((rc = mk.begin(VP_PHASE_DRIFT_X1))) return rc;
     void* dst = dst_of(i++);
     rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_spread_x, d->shift_x, d->W_x, nullptr, 0, 1,
-                     0.0, 1.0, -1, nullptr, nullptr, st);
+                     0.0, 1.0, -1, nullptr, nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
     src = dst;
     // y drift (dt/2), fused with rho when needed
@@ -329,12 +336,12 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     if (want_rho) {
         int tiles = 0;
         rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_spread_y, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
-                         1.0, -1, w.part, &tiles, st);
+                         1.0, -1, w.part, &tiles, EQ, st);
         if (rc) return rc;
-        rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, w.rho, st);
+        rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, eq_on ? d->eq_moment : 0.0, w.rho, st);
     } else {
         rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_spread_y, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
-                         1.0, -1, nullptr, nullptr, st);
+                         1.0, -1, nullptr, nullptr, EQ, st);
     }
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
     src = dst;
@@ -350,17 +357,18 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
             moments = (want_diag && d->diagnostics >= 2) ? w.moments : nullptr;
             dst = dst_of(i++);
             rc = run_kick2d(d->dtype, src, dst, nx * ny, nvx, nvy, ex, ey, d->dt, d->dvx, d->dvy, d->window, d->vx,
-                            d->vy, moments, st);
+                            d->vy, moments, EQ, st);
             if (rc) return rc;
             src = dst;
         } else {
             dst = dst_of(i++);
             rc = run_strided(d->dtype, src, dst, nx * ny, nvx, nvy, true, 1, 1, -1, nullptr, nullptr, ex, 1, 1, d->dt,
-                             d->dvx, d->window, nullptr, nullptr, st);
+                             d->dvx, d->window, nullptr, nullptr, EQ_NONE, st);
             if (rc) return rc;
             src = dst;
             dst = dst_of(i++);
-            rc = run_kick_contig(d->dtype, src, dst, nx * ny * nvx, nvy, ey, 1, nvx, d->dt, d->dvy, d->window, st);
+            rc = run_kick_contig(d->dtype, src, dst, nx * ny * nvx, nvy, ey, 1, nvx, d->dt, d->dvy, d->window,
+                                 EQ_NONE, st);
             if (rc) return rc;
             src = dst;
         }
@@ -381,14 +389,14 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     if ((rc = mk.begin(VP_PHASE_DRIFT_Y2))) return rc;
     dst = dst_of(i++);
     rc = run_strided(d->dtype, src, dst, nx, ny, nvx * nvy, false, 1, nvy, d->shift_spread_y, d->shift_y, d->W_y, nullptr, 0, 1, 0.0,
-                     1.0, -1, nullptr, nullptr, st);
+                     1.0, -1, nullptr, nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_Y2))) return rc;
     src = dst;
     // x drift (dt/2)
     if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
     dst = dst_of(i++);
     rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_spread_x, d->shift_x, d->W_x, nullptr, 0, 1,
-                     0.0, 1.0, -1, nullptr, nullptr, st);
+                     0.0, 1.0, -1, nullptr, nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     if (want_diag) {
         const double dV = d->dx * d->dy * d->dvx * d->dvy;
@@ -427,6 +435,9 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     const bool phys = d->physics_mode != 0;
     const bool want_diag = d->diagnostics && d->diag;
     const int n_sweeps = phys ? 3 : 2;
+    const bool eq_on = d->eq_v != nullptr;
+    const EqSplit eqs{nullptr, d->eq_v, 1, nv};
+    const EqSplit* EQ = eq_on ? &eqs : EQ_NONE;
     int i = 0;
     auto dst_of = [&](int k) -> void* { return ((n_sweeps - 1 - k) % 2 == 0) ? d->f_out : d->f_tmp; };
     const void* src = d->f_in;
@@ -437,12 +448,12 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     if (phys || want_diag) {
         int tiles = 0;
         rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
-                         w.part, &tiles, st);
+                         w.part, &tiles, EQ, st);
         if (rc) return rc;
-        rc = run_rho_finalize(w.part, 1, nx, tiles, d->dv, w.n, st);
+        rc = run_rho_finalize(w.part, 1, nx, tiles, d->dv, eq_on ? d->eq_moment : 0.0, w.n, st);
     } else {
         rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
-                         nullptr, nullptr, st);
+                         nullptr, nullptr, EQ, st);
     }
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
     if ((rc = mk.begin(VP_PHASE_DRIFT_Y1)) || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
@@ -453,7 +464,7 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
         rc = run_poisson1d(w.n, nx, d->inv_kx, d->inv_kx_sq, e, d->rho, d->phi, w.parts, st);
         if (rc || (rc = mk.end(VP_PHASE_FIELD)) || (rc = mk.begin(VP_PHASE_KICK))) return rc;
         dst = dst_of(i++);
-        rc = run_kick_contig(d->dtype, src, dst, nx, nv, e, 1, 1, d->dt, d->dv, d->window, st);
+        rc = run_kick_contig(d->dtype, src, dst, nx, nv, e, 1, 1, d->dt, d->dv, d->window, EQ, st);
         if (rc || (rc = mk.end(VP_PHASE_KICK))) return rc;
         src = dst;
     } else {
@@ -470,7 +481,7 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
     dst = dst_of(i++);
     rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1, nullptr,
-                     nullptr, st);
+                     nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     if (want_diag) {
         if (phys) {

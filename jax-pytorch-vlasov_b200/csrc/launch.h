@@ -19,6 +19,15 @@ inline int occupancy(K kern, int block, size_t smem) {
     return occupancy_raw(reinterpret_cast<const void*>(kern), block, smem);
 }
 
+// Separable equilibrium of the split storage f = feq + g:
+// feq(ivx, ivy) = A[ivx] * B[ivy] (A == NULL: factor 1, the 1D1V case).
+struct EqSplit {
+    const double* A;
+    const double* B;
+    int64_t nvx, nvy;
+};
+#define EQ_NONE static_cast<const EqSplit*>(nullptr)
+
 struct Pois2dWsView {
     const double* mass_part;
     const double* we_part;
@@ -29,15 +38,17 @@ struct Pois2dWsView {
 // sweeps.cu
 int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner, bool kick,
                 int64_t sel_div, int64_t sel_mod, int spread, const int32_t* shift, const void* W, const void* E, int e_f64,
-                int64_t e_div, double dt, double dv, int window, double* part, int* tiles_out, cudaStream_t st);
-int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double* rho,
+                int64_t e_div, double dt, double dv, int window, double* part, int* tiles_out, const EqSplit* eq,
+                cudaStream_t st);
+int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double offset,
+                     double* rho,
                      cudaStream_t st);
 int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t nvx, int64_t nvy, const double* Ex,
                const double* Ey, double dt, double dvx, double dvy, int window, const double* vx,
-               const double* vy, double* moments, cudaStream_t st);
+               const double* vy, double* moments, const EqSplit* eq, cudaStream_t st);
 bool kick2d_fits(int dtype, int64_t nvy, const void* a, const void* b, const void* c);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
-                    int64_t e_div, double dt, double dv, int window, cudaStream_t st);
+                    int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,
                int64_t vso, int64_t vsl, int64_t vsc, double dt, double dx, int periodic, cudaStream_t st);
 int run_rho(int dtype, const void* f, int64_t n_points, int64_t n_v, double dvx, double dvy, void* rho,

@@ -53,13 +53,17 @@ struct StridedArgs {
     int window;
     // fused moment partials [n_outer][tiles][n_line]
     double* part;
+    // equilibrium split (drifts): column c has feq = eqA[(c / eq_nvy) % eq_nvx] * eqB[c % eq_nvy]
+    const double* eqA;  // NULL: factor 1
+    const double* eqB;  // NULL: no split
+    int64_t eq_nvx, eq_nvy;
 };
 
 // NT = rows of the interpolation window of one output: 6 when the VEC
 // columns of a thread share one shift, 7 when their shifts differ by at most
 // one (the y drift, whose shift follows vy, the contiguous index): each
 // element then gets its own 7-tap weight vector with one zero tap.
-template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE>
+template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ>
 __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
@@ -129,6 +133,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
                 }
             }
         }
+        // equilibrium split: the drift of feq + g leaves g + feq*(sum w - 1)
+        C bias[EQ ? VEC : 1];
+        if constexpr (EQ && !KICK) {
+            {
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) {
+                    const int64_t c = col + e;
+                    const double feq = (a.eqA ? a.eqA[(c / a.eq_nvy) % a.eq_nvx] : 1.0) * a.eqB[c % a.eq_nvy];
+                    double wsum = -1.0;
+#pragma unroll
+                    for (int j = 0; j < NT; ++j) wsum += (double)wt[NT == 6 ? 0 : e][j];
+                    bias[e] = C(feq * wsum);
+                }
+            }
+        }
         const TS* src = in + (o * n) * ni + col;
         TS* dst = out + (o * n) * ni + col;
 
@@ -195,6 +214,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
                     C acc = wt[we][NT - 1] * g(u + NT - 1);
 #pragma unroll
                     for (int j = NT - 2; j >= 0; --j) acc = fma(wt[we][j], g(u + j), acc);
+                    if constexpr (EQ) acc += bias[e];
                     res[u].v[e] = acc;
                 }
             }
@@ -263,14 +283,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
 
 // rho[o*n + l] = scale * sum_t part[o][t][l]
 __global__ void k_rho_finalize(const double* __restrict__ part, int64_t n_outer, int n_line, int tiles,
-                               double scale, double* __restrict__ rho) {
+                               double scale, double offset, double* __restrict__ rho) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_outer * n_line) return;
     const int64_t o = i / n_line;
     const int l = (int)(i % n_line);
     double acc = 0.0;
     for (int t = 0; t < tiles; ++t) acc += part[(o * tiles + t) * (int64_t)n_line + l];
-    rho[i] = acc * scale;
+    rho[i] = acc * scale + offset;
 }
 
 // ---------------------------------------------------------------------------
@@ -328,13 +348,14 @@ static StridedPlan plan_strided(int64_t n_outer, int64_t n_line, int64_t n_inner
     return p;
 }
 
-template <typename TS, int VEC, int NT, bool KICK, bool RHO>
+template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool EQ>
 static int launch_strided_t(StridedArgs a, int sms, cudaStream_t st) {
     // whole periodic lines reuse their first rows for the wrap (not with the
     // moment epilogue, whose prefetched chunk needs the registers)
     const bool full = (a.nseg == 1) && (a.n_line % kU == 0) && (a.n_line >= kU) && !RHO;
     const size_t smem = RHO ? (size_t)(kBlock / 32) * a.seg * sizeof(double) : 0;
-    auto kern = (!KICK && full) ? k_strided<TS, VEC, NT, KICK, RHO, true> : k_strided<TS, VEC, NT, KICK, RHO, false>;
+    auto kern = (!KICK && full) ? k_strided<TS, VEC, NT, KICK, RHO, true, EQ>
+                                : k_strided<TS, VEC, NT, KICK, RHO, false, EQ>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return set_cuda_error("cudaFuncSetAttribute(k_strided)");
@@ -345,24 +366,24 @@ static int launch_strided_t(StridedArgs a, int sms, cudaStream_t st) {
     return check_launch("k_strided");
 }
 
-template <typename TS, bool KICK, bool RHO>
+template <typename TS, bool KICK, bool RHO, bool EQ>
 static int launch_strided_vec(StridedArgs a, int vec, int nt, int sms, cudaStream_t st) {
     constexpr int V = sizeof(TS) == 8 ? 2 : 4;
     if (vec == V) {
         if constexpr (!KICK) {
-            if (nt == 7) return launch_strided_t<TS, V, 7, KICK, RHO>(a, sms, st);
+            if (nt == 7) return launch_strided_t<TS, V, 7, KICK, RHO, EQ>(a, sms, st);
         }
-        return launch_strided_t<TS, V, 6, KICK, RHO>(a, sms, st);
+        return launch_strided_t<TS, V, 6, KICK, RHO, EQ>(a, sms, st);
     }
-    return launch_strided_t<TS, 1, 6, KICK, RHO>(a, sms, st);
+    return launch_strided_t<TS, 1, 6, KICK, RHO, EQ>(a, sms, st);
 }
 
-template <bool KICK, bool RHO>
+template <bool KICK, bool RHO, bool EQ>
 static int launch_strided(int dtype, StridedArgs a, int vec, int nt, int sms, cudaStream_t st) {
     switch (dtype) {
-        case VP_F32: return launch_strided_vec<float, KICK, RHO>(a, vec, nt, sms, st);
-        case VP_F64: return launch_strided_vec<double, KICK, RHO>(a, vec, nt, sms, st);
-        case VP_BF16: return launch_strided_vec<__nv_bfloat16, KICK, RHO>(a, vec, nt, sms, st);
+        case VP_F32: return launch_strided_vec<float, KICK, RHO, EQ>(a, vec, nt, sms, st);
+        case VP_F64: return launch_strided_vec<double, KICK, RHO, EQ>(a, vec, nt, sms, st);
+        case VP_BF16: return launch_strided_vec<__nv_bfloat16, KICK, RHO, EQ>(a, vec, nt, sms, st);
     }
     return set_error(VP_ERR_DTYPE, "unknown dtype");
 }
@@ -370,7 +391,7 @@ static int launch_strided(int dtype, StridedArgs a, int vec, int nt, int sms, cu
 int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner,
                 bool kick, int64_t sel_div, int64_t sel_mod, int spread, const int32_t* shift, const void* W,
                 const void* E, int e_f64, int64_t e_div, double dt, double dv, int window, double* part,
-                int* tiles_out, cudaStream_t st) {
+                int* tiles_out, const EqSplit* eq, cudaStream_t st) {
     const int sms = sm_count();
     const bool rho = part != nullptr || tiles_out != nullptr;
     int vec, nt;
@@ -401,15 +422,28 @@ int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n
     a.dv = dv;
     a.window = window;
     a.part = part;
-    if (kick) return launch_strided<true, false>(dtype, a, vec, nt, sms, st);
-    if (rho) return launch_strided<false, true>(dtype, a, vec, nt, sms, st);
-    return launch_strided<false, false>(dtype, a, vec, nt, sms, st);
+    if (eq && eq->B) {
+        if (kick) return set_error(VP_ERR_UNSUPPORTED, "equilibrium split: the strided kick has no split form");
+        a.eqA = eq->A;
+        a.eqB = eq->B;
+        a.eq_nvx = eq->nvx > 0 ? eq->nvx : 1;
+        a.eq_nvy = eq->nvy;
+    }
+    if (kick) return launch_strided<true, false, false>(dtype, a, vec, nt, sms, st);
+    if (a.eqB) {
+        if (rho) return launch_strided<false, true, true>(dtype, a, vec, nt, sms, st);
+        return launch_strided<false, false, true>(dtype, a, vec, nt, sms, st);
+    }
+    if (rho) return launch_strided<false, true, false>(dtype, a, vec, nt, sms, st);
+    return launch_strided<false, false, false>(dtype, a, vec, nt, sms, st);
 }
 
-int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double* rho,
+int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double offset,
+                     double* rho,
                      cudaStream_t st) {
     const int64_t total = n_outer * n_line;
-    k_rho_finalize<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, n_outer, (int)n_line, tiles, scale, rho);
+    k_rho_finalize<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, n_outer, (int)n_line, tiles, scale, offset,
+                                                                      rho);
     return check_launch("k_rho_finalize");
 }
 
@@ -430,6 +464,9 @@ struct Kick2dArgs {
     const double* vx;
     const double* vy;
     double* moments;
+    // equilibrium split: feq = eqA[ivx] * eqB[ivy] (both NULL: off)
+    const double* eqA;
+    const double* eqB;
 };
 
 // 4 consecutive compute-type values from shared memory (16-byte aligned)
@@ -471,7 +508,7 @@ __device__ __forceinline__ void vy_taps(const C (&t)[12], const C (&wy)[6], C (&
     }
 }
 
-template <typename TS, int VEC, bool DIAG>
+template <typename TS, int VEC, bool DIAG, bool EQ>
 __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
@@ -505,16 +542,50 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
         const bool pv = p < a.n_planes;
         const bool active = pv && lane_ok;
         C wx[6], wy[6];
+        double wxd[6], wyd[6];
         int sx = 0, sy = 0;
         if (pv) {
-            sx = kick_weights<double, C>(a.Ex[p], a.dt, a.dvx, a.window, wx);
-            sy = kick_weights<double, C>(a.Ey[p], a.dt, a.dvy, a.window, wy);
+            sx = kick_weights<double, double>(a.Ex[p], a.dt, a.dvx, a.window, wxd);
+            sy = kick_weights<double, double>(a.Ey[p], a.dt, a.dvy, a.window, wyd);
         } else {
 #pragma unroll
-            for (int k = 0; k < 6; ++k) wx[k] = wy[k] = C(0);
+            for (int k = 0; k < 6; ++k) wxd[k] = wyd[k] = 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            wx[k] = C(wxd[k]);
+            wy[k] = C(wyd[k]);
         }
         sx = max(-(1 << 28), min(1 << 28, sx));
         sy = max(-(1 << 28), min(1 << 28, sy));
+        // equilibrium split: the kicks of feq = A(vx) B(vy) add
+        // (Kx A - A)(vx) B(vy) after the vx kick and A(vx) (Ky B - B)(vy) after
+        // the vy kick (K: the plane's kick operator, zero outside the grid)
+        constexpr bool eq = EQ;
+        double Be[EQ ? VEC : 1], dBe[EQ ? VEC : 1];
+        if constexpr (EQ) {
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+                const int iv = li * VEC + e;
+                Be[e] = (lane_ok && iv < nvy) ? a.eqB[iv] : 0.0;
+                double k_b = 0.0;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const int j = iv - sy + 2 - k;
+                    if (lane_ok && j >= 0 && j < nvy) k_b = fma(wyd[k], a.eqB[j], k_b);
+                }
+                dBe[e] = k_b - Be[e];
+            }
+        }
+        auto dA_row = [&](int row) -> double {
+            double k_a = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const int j = row - sx + 2 - k;
+                if (j >= 0 && j < nvx) k_a = fma(wxd[k], a.eqA[j], k_a);
+            }
+            return k_a - a.eqA[row];
+        };
         // vy window of the lane's first element starts gshift elements away:
         // group offset gd (floor division) and element remainder r in [0, 4)
         const int gshift = -sy - 3;
@@ -530,7 +601,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
                 if (active && rr >= 0 && rr < nvx) {
                     const double vx2 = a.vx[rr] * a.vx[rr];
 #pragma unroll
-                    for (int e = 0; e < VEC; ++e) m_pre += (double)v.v[e] * (vx2 + vy2[e]);
+                    for (int e = 0; e < VEC; ++e) {
+                        double fv = (double)v.v[e];
+                        if constexpr (EQ) fv += a.eqA[rr] * Be[e];
+                        m_pre += fv * (vx2 + vy2[e]);
+                    }
                 }
             }
             return v;
@@ -552,6 +627,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 C rv[VEC];
+                double dA = 0.0;
+                if constexpr (EQ) dA = (l + u < nvx) ? dA_row(l + u) : 0.0;
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
                     auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : nx[j - 5].v[e]; };
@@ -561,6 +638,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
                     acc = fma(wx[3], g(u + 2), acc);
                     acc = fma(wx[4], g(u + 1), acc);
                     acc = fma(wx[5], g(u + 0), acc);
+                    if constexpr (EQ) acc += C(dA * Be[e]);
                     rv[e] = as_stored<TS>(acc);
                 }
                 if (lane_ok) {
@@ -613,13 +691,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
                         rres.v[e] = acc;
                     }
                 }
+                if constexpr (EQ) {
+                    if (l + u < nvx) {
+                        const double A = a.eqA[l + u];
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) rres.v[e] += C(A * dBe[e]);
+                    }
+                }
                 if (active && l + u < nvx) {
                     stv<TS, VEC>(dst + (int64_t)(l + u) * nvy, rres);
                     if constexpr (DIAG) {
                         const double vx2 = a.vx[l + u] * a.vx[l + u];
 #pragma unroll
                         for (int e = 0; e < VEC; ++e) {
-                            const double fv = (double)as_stored<TS>(rres.v[e]);
+                            double fv = (double)as_stored<TS>(rres.v[e]);
+                            if constexpr (EQ) fv += a.eqA[l + u] * Be[e];
                             m_post += fv * (vx2 + vy2[e]);
                             m_l2 += fv * fv;
                             m_sum += fv;
@@ -648,11 +734,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
     }
 }
 
-template <typename TS, int VEC, bool DIAG>
+template <typename TS, int VEC, bool DIAG, bool EQ>
 static int launch_kick2d_t(Kick2dArgs a, cudaStream_t st) {
     const int teams = kBlock / a.team;
     const size_t smem = (size_t)teams * kU * a.nvy * sizeof(compute_t<TS>);
-    auto kern = k_kick2d<TS, VEC, DIAG>;
+    auto kern = k_kick2d<TS, VEC, DIAG, EQ>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return set_cuda_error("cudaFuncSetAttribute(k_kick2d)");
@@ -666,11 +752,13 @@ static int launch_kick2d_t(Kick2dArgs a, cudaStream_t st) {
 
 template <typename TS, bool DIAG>
 static int launch_kick2d_vec(Kick2dArgs a, int vec, cudaStream_t st) {
-    if (vec == 4) return launch_kick2d_t<TS, 4, DIAG>(a, st);
+    const bool eq = a.eqB != nullptr;
+    if (vec == 4) return eq ? launch_kick2d_t<TS, 4, DIAG, true>(a, st) : launch_kick2d_t<TS, 4, DIAG, false>(a, st);
     if constexpr (sizeof(TS) == 8) {
-        if (vec == 2) return launch_kick2d_t<TS, 2, DIAG>(a, st);
+        if (vec == 2)
+            return eq ? launch_kick2d_t<TS, 2, DIAG, true>(a, st) : launch_kick2d_t<TS, 2, DIAG, false>(a, st);
     }
-    return launch_kick2d_t<TS, 1, DIAG>(a, st);
+    return eq ? launch_kick2d_t<TS, 1, DIAG, true>(a, st) : launch_kick2d_t<TS, 1, DIAG, false>(a, st);
 }
 
 // Elements per lane of the fused kick: 4 when rows and buffers allow it (one
@@ -695,7 +783,7 @@ bool kick2d_fits(int dtype, int64_t nvy, const void* a, const void* b, const voi
 
 int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t nvx, int64_t nvy,
                const double* Ex, const double* Ey, double dt, double dvx, double dvy, int window,
-               const double* vx, const double* vy, double* moments, cudaStream_t st) {
+               const double* vx, const double* vy, double* moments, const EqSplit* eq, cudaStream_t st) {
     const int vec = kick2d_vec(dtype, nvy, reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out));
     const int groups = (int)(nvy / vec);
     if (groups > 32) {
@@ -721,6 +809,10 @@ int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t n
     a.vx = vx;
     a.vy = vy;
     a.moments = moments;
+    if (eq && eq->B) {
+        a.eqA = eq->A;
+        a.eqB = eq->B;
+    }
     const bool diag = moments != nullptr;
     switch (dtype) {
         case VP_F32: return diag ? launch_kick2d_vec<float, true>(a, vec, st) : launch_kick2d_vec<float, false>(a, vec, st);
@@ -739,7 +831,9 @@ int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t n
 template <typename TS>
 __global__ void __launch_bounds__(kBlock) k_kick_contig(const TS* __restrict__ in, TS* __restrict__ out,
                                                       int64_t n_rows, int n, const void* E, int e_f64,
-                                                      int64_t e_div, double dt, double dv, int window, int tpr) {
+                                                      int64_t e_div, double dt, double dv, int window, int tpr,
+                                                      const double* __restrict__ eqA,
+                                                      const double* __restrict__ eqB, int64_t eq_arows) {
     using C = compute_t<TS>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int rpb = blockDim.x / tpr;
@@ -749,11 +843,14 @@ __global__ void __launch_bounds__(kBlock) k_kick_contig(const TS* __restrict__ i
         const int64_t o = base + g;
         const bool ok = o < n_rows;
         C w[6];
+        double wd[6];
         int s = 0;
         if (ok) {
             const int64_t ei = o / e_div;
-            s = e_f64 ? kick_weights<double, C>(static_cast<const double*>(E)[ei], dt, dv, window, w)
-                      : kick_weights<float, C>(static_cast<const float*>(E)[ei], dt, dv, window, w);
+            s = e_f64 ? kick_weights<double, double>(static_cast<const double*>(E)[ei], dt, dv, window, wd)
+                      : kick_weights<float, double>(static_cast<const float*>(E)[ei], dt, dv, window, wd);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) w[k] = C(wd[k]);
             s = max(-(1 << 28), min(1 << 28, s));
             for (int i = li; i < n; i += tpr) row[i] = to_c(in[o * n + i]);
         }
@@ -770,6 +867,17 @@ __global__ void __launch_bounds__(kBlock) k_kick_contig(const TS* __restrict__ i
                 acc = fma(w[3], gv(3), acc);
                 acc = fma(w[4], gv(4), acc);
                 acc = fma(w[5], gv(5), acc);
+                if (eqB) {
+                    // equilibrium split: add the kicked equilibrium minus itself
+                    double kb = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        const int j = i - s + 2 - k;
+                        if (j >= 0 && j < n) kb = fma(wd[k], eqB[j], kb);
+                    }
+                    const double Ao = eqA ? eqA[o % eq_arows] : 1.0;
+                    acc += C(Ao * (kb - eqB[i]));
+                }
                 out[o * n + i] = from_c<TS>(acc);
             }
         }
@@ -779,7 +887,8 @@ __global__ void __launch_bounds__(kBlock) k_kick_contig(const TS* __restrict__ i
 
 template <typename TS>
 static int launch_kick_contig_t(const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
-                                int64_t e_div, double dt, double dv, int window, cudaStream_t st) {
+                                int64_t e_div, double dt, double dv, int window, const EqSplit* eq,
+                                cudaStream_t st) {
     int tpr = 32;
     while (tpr < n && tpr < kBlock) tpr <<= 1;
     const int rpb = kBlock / tpr;
@@ -792,18 +901,22 @@ static int launch_kick_contig_t(const void* in, void* out, int64_t n_rows, int64
     }
     const int occ = occupancy(kern, kBlock, smem);
     const int64_t grid = std::min<int64_t>((n_rows + rpb - 1) / rpb, (int64_t)sm_count() * occ);
+    const bool eqon = eq && eq->B;
     kern<<<(unsigned)std::max<int64_t>(grid, 1), kBlock, smem, st>>>(
-        static_cast<const TS*>(in), static_cast<TS*>(out), n_rows, (int)n, E, e_f64, e_div, dt, dv, window, tpr);
+        static_cast<const TS*>(in), static_cast<TS*>(out), n_rows, (int)n, E, e_f64, e_div, dt, dv, window, tpr,
+        eqon ? eq->A : nullptr, eqon ? eq->B : nullptr, eqon && eq->nvx > 0 ? eq->nvx : 1);
     return check_launch("k_kick_contig");
 }
 
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
-                    int64_t e_div, double dt, double dv, int window, cudaStream_t st) {
+                    int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st) {
     switch (dtype) {
-        case VP_F32: return launch_kick_contig_t<float>(in, out, n_rows, n, E, e_f64, e_div, dt, dv, window, st);
-        case VP_F64: return launch_kick_contig_t<double>(in, out, n_rows, n, E, e_f64, e_div, dt, dv, window, st);
+        case VP_F32:
+            return launch_kick_contig_t<float>(in, out, n_rows, n, E, e_f64, e_div, dt, dv, window, eq, st);
+        case VP_F64:
+            return launch_kick_contig_t<double>(in, out, n_rows, n, E, e_f64, e_div, dt, dv, window, eq, st);
         case VP_BF16:
-            return launch_kick_contig_t<__nv_bfloat16>(in, out, n_rows, n, E, e_f64, e_div, dt, dv, window, st);
+            return launch_kick_contig_t<__nv_bfloat16>(in, out, n_rows, n, E, e_f64, e_div, dt, dv, window, eq, st);
     }
     return set_error(VP_ERR_DTYPE, "unknown dtype");
 }

@@ -38,6 +38,37 @@ class _Stepper:
     def empty_f(self) -> torch.Tensor:
         return torch.empty(self.shape, dtype=self.dtype, device=self.device)
 
+    # ---- equilibrium split -------------------------------------------------
+    def _set_equilibrium(self, factors, spacings):
+        """factors: 1D equilibrium factors along each velocity dim (float64),
+        or None. Sets the device copies and the equilibrium density."""
+        if factors is None:
+            self.eq = None
+            self.eq_moment = 0.0
+            return
+        fs = [torch.as_tensor(f, dtype=torch.float64).detach().reshape(-1).cpu() for f in factors]
+        self.eq = [f.to(self.device) for f in fs]
+        m = 1.0
+        for f, dv in zip(fs, spacings):
+            m *= float(f.sum()) * dv
+        self.eq_moment = m
+
+    def feq(self) -> torch.Tensor:
+        """The equilibrium over the velocity grid (float64), broadcastable to f."""
+        if self.eq is None:
+            raise ValueError("no equilibrium split configured")
+        if len(self.eq) == 1:
+            return self.eq[0][None, :]
+        return (self.eq[0][:, None] * self.eq[1][None, :])[None, None]
+
+    def split(self, f: torch.Tensor) -> torch.Tensor:
+        """State g = f - feq in the storage dtype (f given as the full f)."""
+        return (f.to(torch.float64) - self.feq()).to(self.dtype).contiguous()
+
+    def join(self, g: torch.Tensor) -> torch.Tensor:
+        """The full f = feq + g (float64)."""
+        return g.to(torch.float64) + self.feq()
+
     def _check(self, f):
         if (tuple(f.shape) != self.shape or f.dtype != self.dtype or f.device != self.device
                 or not f.is_contiguous()):
@@ -128,20 +159,21 @@ class Stepper2D(_Stepper):
     _lib_fn = "vp_step2d"
 
     def __init__(self, Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt, dtype=torch.float32, device="cuda",
-                 physics_mode=True, window=-1, diagnostics=1, vx=None, vy=None):
+                 physics_mode=True, window=-1, diagnostics=1, vx=None, vy=None, equilibrium=None,
+                 precise_tables=False):
         self._init_common(dtype, device, physics_mode, window, diagnostics)
         self.shape = (int(Nx), int(Ny), int(Nvx), int(Nvy))
         self.Lx, self.Ly = float(Lx), float(Ly)
         self.dx, self.dy = self.Lx / Nx, self.Ly / Ny
-        grid_dt = torch.float64 if dtype == torch.float64 else torch.float32
+        grid_dt = torch.float64 if (dtype == torch.float64 or precise_tables) else torch.float32
         vx_t = (torch.linspace(-Vx_max, Vx_max, Nvx, dtype=grid_dt) if vx is None
                 else torch.as_tensor(vx).detach().cpu())
         vy_t = (torch.linspace(-Vy_max, Vy_max, Nvy, dtype=grid_dt) if vy is None
                 else torch.as_tensor(vy).detach().cpu())
         self.dt = float(dt)
         self.dvx, self.dvy = 2 * Vx_max / (Nvx - 1), 2 * Vy_max / (Nvy - 1)
-        self.tx = ops.DriftTable.from_velocity(vx_t, self.dt / 2.0, self.dx, dtype, self.device)
-        self.ty = ops.DriftTable.from_velocity(vy_t, self.dt / 2.0, self.dy, dtype, self.device)
+        self.tx = ops.DriftTable.from_velocity(vx_t, self.dt / 2.0, self.dx, dtype, self.device, precise_tables)
+        self.ty = ops.DriftTable.from_velocity(vy_t, self.dt / 2.0, self.dy, dtype, self.device, precise_tables)
         self.kx, self.ky, self.inv_ksq = ops.spectral_2d(Nx, Ny, self.Lx, self.Ly, self.device)
         self.vx64 = vx_t.to(torch.float64).to(self.device)
         self.vy64 = vy_t.to(torch.float64).to(self.device)
@@ -150,6 +182,13 @@ class Stepper2D(_Stepper):
         self.f_tmp = self.empty_f()
         z = lambda: torch.zeros((Nx, Ny), dtype=torch.float64, device=self.device)  # noqa: E731
         self.drho, self.phi, self.ex, self.ey = z(), z(), z(), z()
+        if isinstance(equilibrium, str):
+            if equilibrium != "maxwellian":
+                raise ValueError("equilibrium: 'maxwellian', (A(vx), B(vy)) or None")
+            m = lambda v: torch.exp(-0.5 * v.double() ** 2) / (2.0 * torch.pi) ** 0.5  # noqa: E731
+            equilibrium = (m(vx_t), m(vy_t))
+        # split storage f = A(vx) B(vy) + g: the state buffers hold g
+        self._set_equilibrium(equilibrium, (self.dvx, self.dvy))
 
     def _desc(self, f_in, f_out, diag) -> L.Step2dDesc:
         d = L.Step2dDesc()
@@ -169,6 +208,9 @@ class Stepper2D(_Stepper):
                                      self.ey.data_ptr())
         d.diag = diag.data_ptr() if diag is not None else None
         d.workspace, d.workspace_bytes = self.ws.data_ptr(), self.ws.numel()
+        if self.eq is not None:
+            d.eq_vx, d.eq_vy = self.eq[0].data_ptr(), self.eq[1].data_ptr()
+            d.eq_moment = self.eq_moment
         return d
 
 
@@ -179,16 +221,16 @@ class Stepper1D(_Stepper):
     _lib_fn = "vp_step1d"
 
     def __init__(self, Nx, Nv, L_, V_max, dt, dtype=torch.float32, device="cuda", physics_mode=True, window=-1,
-                 diagnostics=1, v=None):
+                 diagnostics=1, v=None, equilibrium=None, precise_tables=False):
         self._init_common(dtype, device, physics_mode, window, diagnostics)
         self.shape = (int(Nx), int(Nv))
         self.L = float(L_)
         self.dx = self.L / Nx
-        grid_dt = torch.float64 if dtype == torch.float64 else torch.float32
+        grid_dt = torch.float64 if (dtype == torch.float64 or precise_tables) else torch.float32
         v_t = torch.linspace(-V_max, V_max, Nv, dtype=grid_dt) if v is None else torch.as_tensor(v).detach().cpu()
         self.dv = 2 * V_max / (Nv - 1)
         self.dt = float(dt)
-        self.table = ops.DriftTable.from_velocity(v_t, self.dt / 2.0, self.dx, dtype, self.device)
+        self.table = ops.DriftTable.from_velocity(v_t, self.dt / 2.0, self.dx, dtype, self.device, precise_tables)
         self.inv_kx, self.inv_kx_sq = ops.spectral_1d(Nx, self.L, self.device)
         self.v64 = v_t.to(torch.float64).to(self.device)
         nb = L.query("vp_step1d_workspace_bytes", *self.shape)
@@ -197,6 +239,11 @@ class Stepper1D(_Stepper):
         self.rho = torch.zeros(Nx, dtype=torch.float64, device=self.device)
         self.phi = torch.zeros_like(self.rho)
         self.e = torch.zeros_like(self.rho)
+        if isinstance(equilibrium, str):
+            if equilibrium != "maxwellian":
+                raise ValueError("equilibrium: 'maxwellian', F(v) or None")
+            equilibrium = torch.exp(-0.5 * v_t.double() ** 2) / (2.0 * torch.pi) ** 0.5
+        self._set_equilibrium(None if equilibrium is None else (equilibrium,), (self.dv,))
 
     def _desc(self, f_in, f_out, diag) -> L.Step1dDesc:
         d = L.Step1dDesc()
@@ -213,4 +260,7 @@ class Stepper1D(_Stepper):
         d.rho, d.phi, d.e = self.rho.data_ptr(), self.phi.data_ptr(), self.e.data_ptr()
         d.diag = diag.data_ptr() if diag is not None else None
         d.workspace, d.workspace_bytes = self.ws.data_ptr(), self.ws.numel()
+        if self.eq is not None:
+            d.eq_v = self.eq[0].data_ptr()
+            d.eq_moment = self.eq_moment
         return d

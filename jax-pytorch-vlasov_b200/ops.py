@@ -93,8 +93,11 @@ class DriftTable:
         self.W = torch.as_tensor(np.ascontiguousarray(W), device=device).to(L.compute_dtype(dtype)).contiguous()
 
     @classmethod
-    def from_velocity(cls, v, dt, dx, dtype, device):
-        s, W = drift_table_np(v, dt, dx, dtype)
+    def from_velocity(cls, v, dt, dx, dtype, device, precise=False):
+        """precise: evaluate shift and weights in float64 and round only the
+        weights to the compute type (the reference evaluates them in the run
+        precision, which for float32 also rounds the velocity grid)."""
+        s, W = drift_table_np(v, dt, dx, torch.float64 if precise else dtype)
         return cls(s, W, dtype, device)
 
 

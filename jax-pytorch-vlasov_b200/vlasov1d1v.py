@@ -212,6 +212,7 @@ def _fused(f, dt, table, grid_inv_kx, grid_inv_kx_sq, grid_dx, grid_dv, physics_
         st.diag = None
         st._graphs = {}
         st._bufs = [None, None]
+        st.eq, st.eq_moment = None, 0.0
         if len(_PLANS) > 16:
             _PLANS.clear()
         _PLANS[key] = st

@@ -325,6 +325,7 @@ def _fused_step(f, dt, tables, spectral, grid_dx, grid_dy, grid_dvx, grid_dvy, p
         st.diag = None
         st._graphs = {}
         st._bufs = [None, None]
+        st.eq, st.eq_moment = None, 0.0
         if len(_PLANS) > 16:
             _PLANS.clear()
         _PLANS[key] = plan = st

@@ -1,0 +1,113 @@
+"""Equilibrium-split storage (f = A(vx) B(vy) + g, the state holds g): in
+FP64 the split step equals the unsplit step to round-off; in FP32, with
+drift tables evaluated in float64 (precise_tables), it keeps the
+field-energy history of the reference's FP64 runs within 1e-5 of its peak."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import core as O
+
+pytestmark = pytest.mark.gpu
+
+
+def maxwell(v):
+    v = torch.as_tensor(v, dtype=torch.float64)
+    return torch.exp(-0.5 * v * v) / math.sqrt(2 * math.pi)
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 16, 12), (16, 16, 32, 32), (12, 10, 24, 20)])
+@pytest.mark.parametrize("kind", ["landau", "two_stream"])
+def test_split_equals_unsplit_fp64(vp, shape, kind):
+    Lx = Ly = 4 * math.pi
+    g = O.make_grid2d(*shape, Lx, Ly, 6.0, 5.0, dtype=np.float64)
+    if kind == "landau":
+        f = O.landau_2d(g, 0.2, 0.5)
+        eq = (maxwell(g.vx), maxwell(g.vy))
+    else:
+        f = O.two_stream_2d(g, 0.2, 0.5, 2.0)
+        eq = (0.5 * (maxwell(g.vx - 2.0) + maxwell(g.vx + 2.0)), maxwell(g.vy))
+    a = vp.Stepper2D(*shape, Lx, Ly, 6.0, 5.0, 0.3, dtype=torch.float64, diagnostics=2, window=-1)
+    b = vp.Stepper2D(*shape, Lx, Ly, 6.0, 5.0, 0.3, dtype=torch.float64, diagnostics=2, window=-1,
+                     equilibrium=eq)
+    fa = torch.from_numpy(f).cuda()
+    gb = b.split(fa)
+    for _ in range(3):
+        fa = a.step(fa)
+        gb = b.step(gb)
+        torch.cuda.synchronize()
+        full = b.join(gb)
+        assert (full - fa).abs().max().item() <= 1e-13 * fa.abs().max().item()
+        assert (b.drho - a.drho).abs().max().item() <= 1e-13
+        assert (b.phi - a.phi).abs().max().item() <= 1e-13
+    da, db = a.diag.cpu().numpy(), b.diag.cpu().numpy()
+    np.testing.assert_allclose(db[:5], da[:5], rtol=1e-12)
+
+
+@pytest.mark.parametrize("shape", [(64, 48), (256, 128)])
+def test_split_equals_unsplit_1d_fp64(vp, shape):
+    L = 4 * math.pi
+    g = O.make_grid1d(*shape, L, 6.0, dtype=np.float64)
+    f = O.landau_1d(g, 0.3, 0.5)
+    a = vp.Stepper1D(*shape, L, 6.0, 0.3, dtype=torch.float64, window=-1)
+    b = vp.Stepper1D(*shape, L, 6.0, 0.3, dtype=torch.float64, window=-1, equilibrium="maxwellian")
+    fa = torch.from_numpy(f).cuda()
+    gb = b.split(fa)
+    for _ in range(3):
+        fa = a.step(fa)
+        gb = b.step(gb)
+    torch.cuda.synchronize()
+    assert (b.join(gb) - fa).abs().max().item() <= 1e-13 * fa.abs().max().item()
+    assert (b.rho - a.rho).abs().max().item() <= 1e-13
+    np.testing.assert_allclose(b.diag[:2].cpu().numpy(), a.diag[:2].cpu().numpy(), rtol=1e-12)
+
+
+def _history(vp, n, L, vmax, dt, steps, f_np, dtype, eq, precise=True):
+    st = vp.Stepper2D(n, n, n, n, L, L, vmax, vmax, dt, dtype=dtype, window=1, equilibrium=eq,
+                      precise_tables=precise)
+    f = torch.from_numpy(f_np).cuda()
+    x = st.split(f) if eq is not None else f.to(dtype)
+    h = torch.zeros((steps, 8), dtype=torch.float64, device="cuda")
+    st.run(x, steps, history=h, graph=True)
+    return h[:, 0].cpu().numpy()
+
+
+def test_split_fp32_c1_within_1e5(vp, golden):
+    """C1 (Landau 32^4, eps 0.01, 100 steps) in FP32 with the Maxwellian
+    split and float64-evaluated tables: the field-energy history within 1e-5
+    of the reference's FP64 run (max error over the history relative to its
+    peak), and no worse than the unsplit FP32 run with the reference's
+    float32 tables."""
+    H = golden("history_c1")
+    n, L = 32, 4 * math.pi
+    g = O.make_grid2d(n, n, n, n, L, L, 6.0, 6.0, dtype=np.float64)
+    f = O.landau_2d(g, 0.01, 0.5)
+    ref = H["W_E"]
+    split = _history(vp, n, L, 6.0, 0.1, 100, f, torch.float32, (maxwell(g.vx), maxwell(g.vy)))
+    plain = _history(vp, n, L, 6.0, 0.1, 100, f, torch.float32, None, precise=False)
+    e_split = np.abs(split - ref).max() / np.abs(ref).max()
+    e_plain = np.abs(plain - ref).max() / np.abs(ref).max()
+    assert e_split < 1e-5, (e_split, e_plain)
+    assert e_split <= e_plain, (e_split, e_plain)
+
+
+def test_split_fp32_c2_within_1e5(vp, golden):
+    """C2 (two-stream 64^4, eps 0.001, 400 steps) in FP32 with the
+    two-beam equilibrium split and float64-evaluated tables: history within
+    1e-5 of the reference's FP64 run relative to its peak, and the same
+    linear growth rate to 1e-3 relative."""
+    H = golden("history_c2")
+    n, L = 64, 10 * math.pi
+    g = O.make_grid2d(n, n, n, n, L, L, 8.0, 8.0, dtype=np.float64)
+    f = O.two_stream_2d(g, 0.001, 0.2, 2.4)
+    eq = (0.5 * (maxwell(g.vx - 2.4) + maxwell(g.vx + 2.4)), maxwell(g.vy))
+    ref = H["W_E"]
+    h = _history(vp, n, L, 8.0, 0.05, 400, f, torch.float32, eq)
+    assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-5
+    t = 0.05 * np.arange(1, 401)
+    sel = slice(40, 240)
+    gr = np.polyfit(t[sel], 0.5 * np.log(h[sel]), 1)[0]
+    gr_ref = np.polyfit(t[sel], 0.5 * np.log(ref[sel]), 1)[0]
+    assert abs(gr - gr_ref) <= 1e-3 * abs(gr_ref)

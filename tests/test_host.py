@@ -30,6 +30,21 @@ def test_drift_tables_match_reference(vp, golden, tag, dt):
     np.testing.assert_array_equal(Wt.numpy(), t[f"{tag}_{dt}_W"])
 
 
+@pytest.mark.parametrize("tag", ["c1", "c2", "c3"])
+def test_precise_tables_are_rounded_f64_tables(vp, golden, tag):
+    """precise_tables: shifts of the float64 table, weights of the float64
+    table rounded once to float32."""
+    t = golden("tables")
+    n, vmax, dx, half_dt = t[f"{tag}_f64_meta"]
+    precise = vp.ops.DriftTable.from_velocity(torch.from_numpy(t[f"{tag}_f64_v"]), half_dt, dx, torch.float32,
+                                              "cpu", precise=True)
+    plain = vp.ops.DriftTable.from_velocity(torch.from_numpy(t[f"{tag}_f32_v"]), half_dt, dx, torch.float32, "cpu")
+    np.testing.assert_array_equal(precise.shift.numpy(), t[f"{tag}_f64_shift"])
+    np.testing.assert_array_equal(precise.W.numpy(), t[f"{tag}_f64_W"].astype(np.float32))
+    np.testing.assert_array_equal(plain.W.numpy(), t[f"{tag}_f32_W"])
+    assert precise.W.dtype == plain.W.dtype == torch.float32
+
+
 @pytest.mark.parametrize("dt", ["f64", "f32"])
 def test_lagrange_weights_host(vp, golden, dt):
     t = golden("tables")
