@@ -11,9 +11,11 @@ device); f is 1 GiB per buffer, 8x the 126 MB L2, so no flush is needed.
 Other workloads (--workload): c1 (Landau 32^4 FP64), c2 (two-stream 64^4
 FP32), oned (1D1V Landau 4096 x 4096 FP32, the reference's 1D benchmark
 grid). These are small enough to be launch-bound and run as CUDA graphs.
+c4: 64 seeded independent runs of uneven size advanced by the batched step
+(one launch per substep for all runs), graph-replayed; 272M cells in all.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c3|c1|c2|oned] [--dtype float32|bfloat16|float64]
+                  [--workload c3|c1|c2|c4|oned] [--dtype float32|bfloat16|float64]
 
 --impl reference times the CPU restatement of the reference's algorithm (the
 oracle: C + OpenMP over all host threads) on a bounded sample of the same
@@ -33,6 +35,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -49,6 +53,9 @@ WORKLOADS = {
            "2D2V two-stream 64^4, eps=0.001, k=0.2, v0=2.4, v in [-8,8], dt=0.05"),
     "oned": ("1d", (4096, 4096), 4 * math.pi, 5.0, 0.05, "landau", (0.001, 0.5), "float32",
              "1D1V Landau 4096x4096, eps=0.001, k=0.5, v in [-5,5], dt=0.05"),
+    "c4": ("batch", None, None, None, 0.05, None, None, "float32",
+           "64 independent 2D2V runs of uneven size (seed 20261203: Nx=Ny in {16,24,32,48,64}, Nvx=Nvy in "
+           "{32,48,64}, eps~U[0.001,0.05], k~U[0.3,1], v0~U[0,3], Landau or two-stream), dt=0.05"),
 }
 
 
@@ -69,6 +76,8 @@ def parse():
     wl = WORKLOADS[a.workload]
     a.kind, a.grid, a.L, a.vmax, a.dt, a.ic, a.icp, dflt, a.desc = wl
     a.dtype = a.dtype or dflt
+    if a.kind == "batch" and a.size:
+        raise SystemExit("--size does not apply to the batched workload")
     if a.size:
         if a.kind != "2d":
             raise SystemExit("--size applies to 2D2V workloads")
@@ -490,8 +499,213 @@ def run_e2e(a, f_dev, dev, dtype, world, dist, torch, vp):
             "steps": a.e2e_steps, "path": path}
 
 
+# ---------------------------------------------------------------------------
+# the batched workload (64 uneven runs, one launch per substep for all)
+# ---------------------------------------------------------------------------
+def _batch_oracle_sample(budget_s):
+    """The oracle on runs of the batch in their drawn order, one step each,
+    until budget_s of host time is spent: (cells stepped, seconds, runs used)."""
+    from oracle import core as O
+
+    wl = importlib.import_module("jax-pytorch-vlasov_b200.workloads")
+    runs = wl.batch_runs()
+    done = 0
+    spent = 0.0
+    used = 0
+    for p in runs:
+        g = O.make_grid2d(p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"], p["Vx_max"], p["Vy_max"],
+                          dtype=np.float32)
+        if p["kind"] == "landau":
+            f = O.landau_2d(g, p["eps"], p["k"])
+        else:
+            f = O.two_stream_2d(g, p["eps"], p["k"], p["v0"])
+        st = O.Stepper2D(g, p["dt"], window=1)
+        st.step(f)  # warm-up
+        t0 = time.perf_counter()
+        st.step(f)
+        spent += time.perf_counter() - t0
+        done += p["Nx"] * p["Ny"] * p["Nvx"] * p["Nvy"]
+        used += 1
+        if spent >= budget_s:
+            break
+    return done, spent, used
+
+
+def run_batch_reference(a):
+    if int(os.environ.get("RANK", 0)) != 0:
+        return 0
+    from oracle import core as O
+
+    per_step = max(0.5, 150.0 / max(1, a.steps + a.warmup))
+    cells = 0
+    sec = 0.0
+    used = 0
+    for i in range(a.warmup + a.steps):
+        c, t, u = _batch_oracle_sample(per_step)
+        if i >= a.warmup:
+            cells += c
+            sec += t
+            used = u
+    value = cells / sec
+    sample = (f"oracle Strang step (C + OpenMP restatement of the reference's vlasov_step_gather_free) over the "
+              f"first {used} runs of the batch per step, {a.steps} steps after {a.warmup} warm-up")
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": short_dtype(a.dtype),
+        "data": "synthetic", "config": {"workload": a.desc + f", {a.dtype} storage", "sample_runs": used},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(a):
+    import torch
+
+    vp = importlib.import_module("jax-pytorch-vlasov_b200")
+    dist = importlib.import_module("jax-pytorch-vlasov_b200.dist")
+    wl = importlib.import_module("jax-pytorch-vlasov_b200.workloads")
+    L = vp._lib
+
+    rank, local, world = dist.init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dtype = {"float32": torch.float32, "bfloat16": torch.bfloat16, "float64": torch.float64}[a.dtype]
+    esz = {torch.float32: 4, torch.bfloat16: 2, torch.float64: 8}[dtype]
+    runs = wl.batch_runs()
+    diag = 1 if a.diagnostics else 0
+    st = vp.BatchStepper2D(runs, dtype=dtype, device=dev, window=1, diagnostics=diag, graph_slots=10)
+    for r, p in enumerate(runs):  # each rank advances its own replica of the batch
+        st.set_state(r, wl.initial_2d(p["kind"], p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"],
+                                      p["Vx_max"], p["Vy_max"], p["eps"] * (1.0 + 0.01 * rank), p["k"], p["v0"],
+                                      dtype=dtype, device=dev))
+    cells = st.cells
+    n = len(runs)
+    K = max(a.steps, 1)
+    hist = torch.zeros((K, n, L.DIAG_COUNT), dtype=torch.float64, device=dev)
+    nph = len(PHASES)
+    with ClockSampler(local) as clk:
+        c0 = L.load().vp_launch_count()
+        st.step(0)
+        per_step_launches = L.load().vp_launch_count() - c0
+        st.run(max(a.warmup, 3) + 10, graph=True)  # captures the graph, then replays it
+        torch.cuda.synchronize(dev)
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        h0 = time.monotonic()
+        t_start.record()
+        st.run(K, history=hist, graph=True)
+        t_end.record()
+        torch.cuda.synchronize(dev)
+        clk.mark(h0, time.monotonic())
+        # per-substep times from eager steps with events (after the timed region)
+        n_ev = 5
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * nph)] for _ in range(n_ev)]
+        for row in evs:
+            for e in row:
+                e.record()
+        torch.cuda.synchronize(dev)
+        for row in evs:
+            arr = (ctypes.c_void_p * (2 * nph))(*[e.cuda_event for e in row])
+            st.step(0, events=arr)
+        torch.cuda.synchronize(dev)
+    dist.barrier()
+    ms = t_start.elapsed_time(t_end)
+    ms_max = dist.max_over_ranks(ms)
+    value = world * cells * K / (ms_max / 1e3)
+    ms_step = ms_max / K
+    sweep_bytes = 2.0 * esz * cells
+    peak, peak_kind = measured_peak()
+    ph = {p: sum(row[2 * j].elapsed_time(row[2 * j + 1]) for row in evs) / n_ev for j, p in enumerate(PHASES)}
+    groups = {"drift_x": ph["drift_x1"] + ph["drift_x2"], "drift_y_rho": ph["drift_y1_rho"],
+              "kick_vx_vy": ph["kick_vx_vy"], "drift_y": ph["drift_y2"]}
+    dom = max(groups, key=groups.get)
+    dom_ms = groups[dom] / (2 if dom == "drift_x" else 1)
+    achieved = sweep_bytes / (dom_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom + " (batched, all runs)", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": ncu_traffic(f"batch_{dom}_{a.dtype}"), "algorithmic_bytes_per_launch": sweep_bytes}
+    phase_gbs = {p: (sweep_bytes / (ph[p] * 1e-3) / 1e9 if ph[p] > 0 and p not in ("field", "diag") else None)
+                 for p in PHASES}
+    h = hist.cpu()
+    finite = bool(torch.isfinite(h[:, :, :2]).all())
+
+    e2e = None
+    if a.e2e_steps > 0:
+        # end to end through the public API: every step copies every run's f
+        # from pinned host memory, steps the batch, and copies f and the
+        # diagnostics back
+        arena = st._arenas[0]
+        h_in = arena.cpu().pin_memory()
+        h_out = torch.empty_like(h_in).pin_memory()
+        h_diag = torch.empty((n, L.DIAG_COUNT), dtype=torch.float64).pin_memory()
+
+        def e2e_step():
+            arena.copy_(h_in, non_blocking=True)
+            st.step(0)
+            h_out.copy_(arena, non_blocking=True)
+            h_diag.copy_(st.stage[0], non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        e_ms = dist.max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * cells * a.e2e_steps / (e_ms / 1e3), "unit": "cell-updates/s",
+               "h2d_bytes_per_step": int(arena.numel()), "d2h_bytes_per_step": int(arena.numel() + h_diag.numel() * 8),
+               "steps": a.e2e_steps, "path": "BatchStepper2D.step with every run's f copied from/to pinned host memory"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        from oracle import core as O
+
+        c, t, used = _batch_oracle_sample(a.cpu_budget / 2)
+        cpu = {"value": c / t, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"oracle Strang step over the first {used} runs of the batch, one step each, {t:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": K, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": short_dtype(a.dtype), "data": "synthetic",
+            "config": {"workload": a.desc + f", {a.dtype} storage", "runs": n, "cells": cells,
+                       "global_batch": n * world,
+                       "parallelism": f"{world} independent replicas of the batch" if world > 1 else "one batch",
+                       "l2_flush": "not needed: the batch state (all runs) exceeds the L2 several times",
+                       "diagnostics_level": diag, "graph": "10 steps per CUDA graph, replayed"},
+            "roofline": roof,
+            "step_gbs": 5 * sweep_bytes / (ms_step * 1e-3) / 1e9,
+            "gpu_launches": int(per_step_launches * K),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "diagnostics": {"mass_drift_rel_max": float(((h[-1, :, 1] - h[0, :, 1]) / h[0, :, 1]).abs().max()),
+                            "finite": finite},
+            "phases_ms": ph,
+            "phases_gbs": phase_gbs,
+        }
+        clk_s = clk.summary()
+        if clk_s:
+            line["clocks"] = clk_s
+        print(json.dumps(line), flush=True)
+    dist.finalize()
+    return 0
+
+
 def main():
     a = parse()
+    if a.kind == "batch":
+        return run_batch_reference(a) if a.impl == "reference" else run_batch(a)
     if a.impl == "reference":
         return run_reference(a)
     return run_ours(a)

@@ -285,6 +285,61 @@ typedef struct vp_step1d_desc {
 int vp_step1d(const vp_step1d_desc* desc, void* stream);
 size_t vp_step1d_workspace_bytes(int64_t nx, int64_t nv);
 
+/* ---- batched 2D2V steps ---------------------------------------------------
+ * Many independent runs of uneven sizes and parameters advanced together,
+ * one launch per substep for all of them (no reference counterpart: the
+ * reference advances one run per Vlasov object, vlasov2D2V.py:1392-1435;
+ * each run of a batch follows vp_step2d's schedule and arithmetic).
+ *
+ * Usage: fill one vp_batch2d_run per run; vp_batch2d_plan writes a table of
+ * vp_batch2d_table_bytes(n) bytes into host memory; copy it unchanged to a
+ * device buffer; then every vp_batch2d_step(table, table_dev, slot, stream)
+ * advances all runs by one step. The step only launches kernels (no copies,
+ * no allocation), so a sequence of steps can be captured in a CUDA graph.
+ * Each run's state is advanced in place: f -> s1 -> s2 -> s1 -> s2 -> f. */
+typedef struct vp_batch2d_run {
+    int32_t nx, ny, nvx, nvy;
+    double dt, dx, dy, dvx, dvy;
+    int32_t window;         /* kick window S (<0: exact kick) */
+    int32_t shift_spread_x; /* see vp_drift */
+    int32_t shift_spread_y;
+    int32_t reserved;       /* 0 */
+    void* f;                /* [nx][ny][nvx][nvy] state, advanced in place */
+    void* s1;               /* scratch of the size of f */
+    void* s2;               /* scratch of the size of f */
+    const int32_t* shift_x; /* [nvx] */
+    const void* W_x;        /* compute type [6][nvx] */
+    const int32_t* shift_y; /* [nvy] */
+    const void* W_y;        /* compute type [6][nvy] */
+    const double* kx;       /* [nx] */
+    const double* ky;       /* [ny/2+1] */
+    const double* inv_ksq;  /* [nx][ny/2+1] */
+    double* drho;           /* [nx][ny] mid-step rho - 1 (may be NULL) */
+    double* phi;            /* [nx][ny] (may be NULL) */
+    double* diag;           /* VP_DIAG_COUNT doubles at diag + slot * diag_slot_stride (may be NULL) */
+    int64_t diag_slot_stride;
+    void* workspace;        /* vp_step2d_workspace_bytes(nx, ny, nvx, nvy) bytes */
+    size_t workspace_bytes;
+} vp_batch2d_run;
+
+/* Tile shapes of the batched sweeps, per sweep kind (0: x drifts, 1: y
+ * drifts, 2: fused kick). Zeros select the defaults. */
+#define VP_BATCH_KINDS 3
+typedef struct vp_batch_tiles {
+    int32_t block[VP_BATCH_KINDS];       /* threads per CTA (one tile of columns): 128 or 256 */
+    int32_t ctas_per_sm[VP_BATCH_KINDS]; /* persistent CTAs per SM, <= the occupancy limit */
+    int32_t segments[VP_BATCH_KINDS];    /* CTAs per line of the drifts: 1, 2 or 4 (ignored for the kick) */
+} vp_batch_tiles;
+
+size_t vp_batch2d_table_bytes(int32_t n_runs);
+/* physics_mode must be 1 when diagnostics is 1; diagnostics: 0 or 1 (field
+ * energy, mass, max shift). All runs share dtype. */
+int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, const vp_batch2d_run* runs,
+                    int32_t n_runs, const vp_batch_tiles* tiles, void* table, size_t table_bytes);
+/* events: optional [2*VP_PHASE_COUNT] cudaEvent_t around the substeps of
+ * all runs (VP_PHASE_DRIFT_Y1 includes the rho finalize), NULL to skip. */
+int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void* const* events, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,7 +5,9 @@ Modules:
   vlasov2d2v  -- the 2D2V API (Grid, advect_*, compute_rho, compute_poisson_real,
                  vlasov_step_*, Vlasov), same names and signatures as the reference
   vlasov1d1v  -- the 1D1V API
-  engine      -- Stepper2D / Stepper1D: one library call per Strang step, CUDA graphs
+  engine      -- Stepper2D / Stepper1D: one library call per Strang step, CUDA graphs;
+                 BatchStepper2D: many uneven runs, one launch per substep for all
+  workloads   -- seeded initial conditions and the batched-runs parameter draws
   ops         -- tensor-level wrappers of the C ABI (include/vlasov_b200.h)
   build       -- compiles csrc/*.cu into libvlasov_b200.so for sm_100a
 
@@ -14,14 +16,14 @@ importlib.import_module("jax-pytorch-vlasov_b200").
 """
 from . import _lib, build, ops  # noqa: F401
 from ._lib import DIAG_NAMES, VlasovError, load  # noqa: F401
-from .engine import Stepper1D, Stepper2D  # noqa: F401
+from .engine import BatchStepper2D, Stepper1D, Stepper2D  # noqa: F401
 
-__all__ = ["Stepper1D", "Stepper2D", "VlasovError", "load", "ops", "build", "DIAG_NAMES", "vlasov2d2v",
+__all__ = ["BatchStepper2D", "Stepper1D", "Stepper2D", "VlasovError", "load", "ops", "build", "DIAG_NAMES", "vlasov2d2v",
            "vlasov1d1v"]
 
 
 def __getattr__(name):
-    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot"):
+    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads"):
         import importlib
 
         return importlib.import_module(f"{__name__}.{name}")

@@ -71,6 +71,26 @@ class Step1dDesc(ctypes.Structure):
     ]
 
 
+class BatchRun(ctypes.Structure):
+    _fields_ = [
+        ("nx", I32), ("ny", I32), ("nvx", I32), ("nvy", I32),
+        ("dt", D), ("dx", D), ("dy", D), ("dvx", D), ("dvy", D),
+        ("window", I32), ("shift_spread_x", I32), ("shift_spread_y", I32), ("reserved", I32),
+        ("f", P), ("s1", P), ("s2", P),
+        ("shift_x", P), ("W_x", P), ("shift_y", P), ("W_y", P),
+        ("kx", P), ("ky", P), ("inv_ksq", P),
+        ("drho", P), ("phi", P), ("diag", P), ("diag_slot_stride", I64),
+        ("workspace", P), ("workspace_bytes", SZ),
+    ]
+
+
+BATCH_KINDS = 3
+
+
+class BatchTiles(ctypes.Structure):
+    _fields_ = [("block", I32 * BATCH_KINDS), ("ctas_per_sm", I32 * BATCH_KINDS), ("segments", I32 * BATCH_KINDS)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "vp_version": (ctypes.c_char_p, []),
@@ -89,6 +109,10 @@ SIGNATURES = {
     "vp_poisson1d": (ctypes.c_int, [P, I64, P, P, D, P, P, P, P, P, SZ, P]),
     "vp_poisson1d_workspace_bytes": (SZ, [I64]),
     "vp_step2d": (ctypes.c_int, [ctypes.POINTER(Step2dDesc), P]),
+    "vp_batch2d_table_bytes": (SZ, [I32]),
+    "vp_batch2d_plan": (ctypes.c_int, [I32, I32, I32, ctypes.POINTER(BatchRun), I32, ctypes.POINTER(BatchTiles), P,
+                                       SZ]),
+    "vp_batch2d_step": (ctypes.c_int, [P, P, I32, P, P]),
     "vp_step2d_workspace_bytes": (SZ, [I64, I64, I64, I64]),
     "vp_step1d": (ctypes.c_int, [ctypes.POINTER(Step1dDesc), P]),
     "vp_step1d_workspace_bytes": (SZ, [I64, I64]),

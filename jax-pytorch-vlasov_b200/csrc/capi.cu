@@ -90,16 +90,11 @@ static size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 static bool dtype_ok(int d) { return d == VP_F32 || d == VP_F64 || d == VP_BF16; }
 
 static size_t drift_rho_part_bytes(int64_t n_outer, int64_t n_line, int64_t n_inner) {
-    const int64_t tiles = (n_inner + 255) / 256;  // one column per thread, 256 threads per tile
+    const int64_t tiles = (n_inner + 127) / 128;  // worst case: one column per thread, 128 threads per tile
     return al((size_t)n_outer * tiles * n_line * sizeof(double));
 }
 
-struct Step2dWs {
-    double *part, *rho, *ex, *ey, *moments;
-    void* pois;
-};
-
-static size_t step2d_layout(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, char* base, Step2dWs* w) {
+size_t step2d_layout(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, char* base, Step2dWs* w) {
     size_t off = 0;
     auto take = [&](size_t b) {
         char* p = base ? base + off : nullptr;

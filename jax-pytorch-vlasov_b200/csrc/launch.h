@@ -28,12 +28,108 @@ struct EqSplit {
 };
 #define EQ_NONE static_cast<const EqSplit*>(nullptr)
 
+// ---------------------------------------------------------------------------
+// Kernel argument blocks (plain data, also stored in device-resident tables
+// by the batched step)
+// ---------------------------------------------------------------------------
+struct StridedArgs {
+    const void* in;
+    void* out;
+    int64_t n_outer;
+    int n_line;
+    int64_t n_inner;
+    int64_t ncg;    // column groups (of VEC elements) per outer row
+    int tiles;      // ceil(ncg / blockDim.x)
+    int seg;        // outputs per line segment
+    int nseg;       // segments per line
+    int64_t items;  // n_outer * tiles * nseg
+    // drift table
+    int64_t sel_div;
+    int sel_mod;
+    const int32_t* shift;
+    const void* W;
+    // kick field
+    const void* E;
+    int e_f64;
+    int64_t e_div;
+    double dt, dv;
+    int window;
+    // fused moment partials [n_outer][tiles][n_line]
+    double* part;
+    // equilibrium split (drifts): column c has feq = eqA[(c / eq_nvy) % eq_nvx] * eqB[c % eq_nvy]
+    const double* eqA;  // NULL: factor 1
+    const double* eqB;  // NULL: no split
+    int64_t eq_nvx, eq_nvy;
+};
+
+struct Kick2dArgs {
+    const void* in;
+    void* out;
+    int64_t n_planes;
+    int nvx, nvy;
+    int team;   // lanes per plane (power of two, <= 32)
+    int groups; // nvy / VEC
+    const double* Ex;
+    const double* Ey;
+    double dt, dvx, dvy;
+    int window;
+    const double* vx;
+    const double* vy;
+    double* moments;
+    // equilibrium split: feq = eqA[ivx] * eqB[ivy] (both NULL: off)
+    const double* eqA;
+    const double* eqB;
+};
+
+// Poisson solve of one run (workspace pointers from the 2D layout).
+struct Pois2dRun {
+    const double* rho;
+    int nx, ny;
+    const double *kx, *ky, *inv_ksq;
+    double *drho, *phi, *ex, *ey;
+    double2 *R, *Zp, *Zx, *Zy;
+    double *mass_part, *we_part, *emax_part;
+};
+
+// rho[o*n_line + l] = scale * sum_t part[o][t][l] + offset for one run.
+struct RhoFinRun {
+    const double* part;
+    int64_t n_outer;
+    int n_line, tiles;
+    double scale, offset;
+    double* rho;
+};
+
+struct DiagArgs {
+    const double* mass_part;  // [n_mass]
+    int n_mass;
+    const double* we_part;  // [n_we]
+    int n_we;
+    const double* emax_part;  // [n_emax][2]
+    int n_emax;
+    const double* moments;  // [n_mom][4]
+    int64_t n_mom;
+    double mass_scale, we_scale, dv_scale;  // dx*dy, 0.5*dx*dy, dV
+    double shift_x, shift_y;                // dt/dvx, dt/dvy
+    double* energy;                         // optional [2]: {W_E, mass}
+    double* diag;                           // optional [VP_DIAG_COUNT]
+    int64_t slot_stride;                    // batched form: doubles between history slots
+};
+
 struct Pois2dWsView {
     const double* mass_part;
     const double* we_part;
     const double* emax_part;
     int n_lines;
 };
+
+// Workspace of one 2D2V step (capi.cu): rho partials, rho, fields, kick
+// moments, Poisson scratch.
+struct Step2dWs {
+    double *part, *rho, *ex, *ey, *moments;
+    void* pois;
+};
+size_t step2d_layout(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, char* base, Step2dWs* w);
 
 // sweeps.cu
 int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner, bool kick,
@@ -54,6 +150,22 @@ int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n,
 int run_rho(int dtype, const void* f, int64_t n_points, int64_t n_v, double dvx, double dvy, void* rho,
             int out_dtype, cudaStream_t st);
 
+// batched step (sweeps.cu)
+int strided_batch_args(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                       int64_t sel_div, int64_t sel_mod, int spread, const int32_t* shift, const void* W,
+                       double* part, int block, StridedArgs* a, int* vec, int* nt);
+void strided_batch_finish(StridedArgs* a, int vec, int block);
+int strided_batch_pref_vec(int dtype);
+int launch_strided_batch(int dtype, int vec, int nt, bool rho, bool wrap, const StridedArgs* runs,
+                         const int64_t* start, int n_runs, int block, int grid_cap, int max_line, cudaStream_t st);
+int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int64_t max_points, cudaStream_t st);
+int kick2d_batch_args(int dtype, const void* in, void* out, int64_t n_planes, int64_t nvx, int64_t nvy,
+                      const double* Ex, const double* Ey, double dt, double dvx, double dvy, int window,
+                      Kick2dArgs* a, int* vec);
+int64_t kick2d_batch_finish(Kick2dArgs* a, int dtype, int vec, int block, int64_t* items);
+int launch_kick2d_batch(int dtype, int vec, const Kick2dArgs* runs, const int64_t* start, int n_runs, int block,
+                        int grid_cap, size_t smem, cudaStream_t st);
+
 // poisson.cu
 size_t poisson2d_ws_bytes(int64_t nx, int64_t ny);
 int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
@@ -65,6 +177,11 @@ int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_m
 int run_poisson2d_static(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
                          const double* inv_ksq, double dx, double dy, double* ex, double* ey, double* drho,
                          double* phi, double* energy, cudaStream_t st);
+void pois2d_run_args(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                     const double* inv_ksq, double* ex, double* ey, double* drho, double* phi, void* ws,
+                     Pois2dRun* a, Pois2dWsView* view);
+int launch_poisson2d_batch(const Pois2dRun* runs, int n_runs, int max_nx, int max_ny, cudaStream_t st);
+int launch_diag_finalize_batch(const DiagArgs* runs, int n_runs, int slot, cudaStream_t st);
 size_t poisson1d_ws_bytes(int64_t nx);
 int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double* e,
                   double* rho, double* phi, double* parts, cudaStream_t st);

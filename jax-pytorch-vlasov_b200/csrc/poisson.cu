@@ -62,14 +62,12 @@ __device__ double block_max(double v, double* scratch) {
 }
 
 // ---- 2D: rows, forward ------------------------------------------------------
-__global__ void __launch_bounds__(kPBlock) k_p2_rows_fwd(const double* __restrict__ rho, int nx, int ny,
-                                                       double* __restrict__ drho, double2* __restrict__ R,
-                                                       double* __restrict__ mass_part) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void p2_rows_fwd(const double* __restrict__ rho, int nx, int ny, double* __restrict__ drho,
+                                            double2* __restrict__ R, double* __restrict__ mass_part, const int ix,
+                                            unsigned char* smem_raw) {
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double* row = reinterpret_cast<double*>(tw + ny);
     double* scratch = row + ny;
-    const int ix = blockIdx.x;
     const int nyh = ny / 2 + 1;
     fill_twiddles(tw, ny);
     double m = 0.0;
@@ -96,19 +94,24 @@ __global__ void __launch_bounds__(kPBlock) k_p2_rows_fwd(const double* __restric
     }
 }
 
-// ---- 2D: columns ------------------------------------------------------------
-__global__ void __launch_bounds__(kPBlock) k_p2_cols(const double2* __restrict__ R, int nx, int ny,
-                                                   const double* __restrict__ kx, const double* __restrict__ ky,
-                                                   const double* __restrict__ inv_ksq, double2* __restrict__ Zp,
-                                                   double2* __restrict__ Zx, double2* __restrict__ Zy) {
+__global__ void __launch_bounds__(kPBlock) k_p2_rows_fwd(const double* __restrict__ rho, int nx, int ny,
+                                                       double* __restrict__ drho, double2* __restrict__ R,
+                                                       double* __restrict__ mass_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    p2_rows_fwd(rho, nx, ny, drho, R, mass_part, blockIdx.x, smem_raw);
+}
+
+// ---- 2D: columns ------------------------------------------------------------
+__device__ __forceinline__ void p2_cols(const double2* __restrict__ R, int nx, int ny, const double* __restrict__ kx,
+                                        const double* __restrict__ ky, const double* __restrict__ inv_ksq,
+                                        double2* __restrict__ Zp, double2* __restrict__ Zx, double2* __restrict__ Zy,
+                                        const int k, unsigned char* smem_raw) {
     const int nyh = ny / 2 + 1;
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* col = tw + nx;
     double2* P = col + nx;
     double2* X = P + nx;
     double2* Y = X + nx;
-    const int k = blockIdx.x;  // ky index
     fill_twiddles(tw, nx);
     for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) col[ix] = R[(int64_t)ix * nyh + k];
     __syncthreads();
@@ -156,21 +159,26 @@ __global__ void __launch_bounds__(kPBlock) k_p2_cols(const double2* __restrict__
     }
 }
 
-// ---- 2D: rows, complex-to-real inverse ------------------------------------------
-__global__ void __launch_bounds__(kPBlock) k_p2_rows_inv(const double2* __restrict__ Zp,
-                                                       const double2* __restrict__ Zx,
-                                                       const double2* __restrict__ Zy, int nx, int ny,
-                                                       double* __restrict__ phi, double* __restrict__ ex,
-                                                       double* __restrict__ ey, double* __restrict__ we_part,
-                                                       double* __restrict__ emax_part) {
+__global__ void __launch_bounds__(kPBlock) k_p2_cols(const double2* __restrict__ R, int nx, int ny,
+                                                   const double* __restrict__ kx, const double* __restrict__ ky,
+                                                   const double* __restrict__ inv_ksq, double2* __restrict__ Zp,
+                                                   double2* __restrict__ Zx, double2* __restrict__ Zy) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    p2_cols(R, nx, ny, kx, ky, inv_ksq, Zp, Zx, Zy, blockIdx.x, smem_raw);  // block = ky index
+}
+
+// ---- 2D: rows, complex-to-real inverse ------------------------------------------
+__device__ __forceinline__ void p2_rows_inv(const double2* __restrict__ Zp, const double2* __restrict__ Zx,
+                                            const double2* __restrict__ Zy, int nx, int ny, double* __restrict__ phi,
+                                            double* __restrict__ ex, double* __restrict__ ey,
+                                            double* __restrict__ we_part, double* __restrict__ emax_part,
+                                            const int ix, unsigned char* smem_raw) {
     const int nyh = ny / 2 + 1;
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* zp = tw + ny;
     double2* zx = zp + nyh;
     double2* zy = zx + nyh;
     double* scratch = reinterpret_cast<double*>(zy + nyh);
-    const int ix = blockIdx.x;
     fill_twiddles(tw, ny);
     for (int q = threadIdx.x; q < nyh; q += blockDim.x) {
         const int64_t o = (int64_t)ix * nyh + q;
@@ -224,24 +232,41 @@ __global__ void __launch_bounds__(kPBlock) k_p2_rows_inv(const double2* __restri
     }
 }
 
-// ---- diagnostics finalize (one block, fixed order) -------------------------------
-struct DiagArgs {
-    const double* mass_part;  // [n_mass]
-    int n_mass;
-    const double* we_part;  // [n_we]
-    int n_we;
-    const double* emax_part;  // [n_emax][2]
-    int n_emax;
-    const double* moments;  // [n_mom][4]
-    int64_t n_mom;
-    double mass_scale, we_scale, dv_scale;  // dx*dy, 0.5*dx*dy, dV
-    double shift_x, shift_y;                // dt/dvx, dt/dvy
-    double* energy;                         // optional [2]: {W_E, mass}
-    double* diag;                           // optional [VP_DIAG_COUNT]
-};
+__global__ void __launch_bounds__(kPBlock) k_p2_rows_inv(const double2* __restrict__ Zp,
+                                                       const double2* __restrict__ Zx,
+                                                       const double2* __restrict__ Zy, int nx, int ny,
+                                                       double* __restrict__ phi, double* __restrict__ ex,
+                                                       double* __restrict__ ey, double* __restrict__ we_part,
+                                                       double* __restrict__ emax_part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    p2_rows_inv(Zp, Zx, Zy, nx, ny, phi, ex, ey, we_part, emax_part, blockIdx.x, smem_raw);
+}
 
-__global__ void __launch_bounds__(kPBlock) k_diag_finalize(DiagArgs a) {
-    __shared__ double scratch[kPBlock];
+// ---- 2D, many runs: blockIdx.y = run, blockIdx.x = line (blocks past the
+// run's line count leave at once) --------------------------------------------
+__global__ void __launch_bounds__(kPBlock) k_p2_rows_fwd_batch(const Pois2dRun* __restrict__ runs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Pois2dRun a = runs[blockIdx.y];
+    if ((int)blockIdx.x >= a.nx) return;
+    p2_rows_fwd(a.rho, a.nx, a.ny, a.drho, a.R, a.mass_part, blockIdx.x, smem_raw);
+}
+
+__global__ void __launch_bounds__(kPBlock) k_p2_cols_batch(const Pois2dRun* __restrict__ runs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Pois2dRun a = runs[blockIdx.y];
+    if ((int)blockIdx.x >= a.ny / 2 + 1) return;
+    p2_cols(a.R, a.nx, a.ny, a.kx, a.ky, a.inv_ksq, a.Zp, a.Zx, a.Zy, blockIdx.x, smem_raw);
+}
+
+__global__ void __launch_bounds__(kPBlock) k_p2_rows_inv_batch(const Pois2dRun* __restrict__ runs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Pois2dRun a = runs[blockIdx.y];
+    if ((int)blockIdx.x >= a.nx) return;
+    p2_rows_inv(a.Zp, a.Zx, a.Zy, a.nx, a.ny, a.phi, a.ex, a.ey, a.we_part, a.emax_part, blockIdx.x, smem_raw);
+}
+
+// ---- diagnostics finalize (one block, fixed order) -------------------------------
+__device__ __forceinline__ void diag_finalize(const DiagArgs& a, double* scratch) {
     double m = 0.0, w = 0.0, ex = 0.0, ey = 0.0, pre = 0.0, post = 0.0, l2 = 0.0;
     for (int i = threadIdx.x; i < a.n_mass; i += blockDim.x) m += a.mass_part[i];
     for (int i = threadIdx.x; i < a.n_we; i += blockDim.x) w += a.we_part[i];
@@ -279,6 +304,19 @@ __global__ void __launch_bounds__(kPBlock) k_diag_finalize(DiagArgs a) {
             a.diag[7] = 0.0;
         }
     }
+}
+
+__global__ void __launch_bounds__(kPBlock) k_diag_finalize(const __grid_constant__ DiagArgs a) {
+    __shared__ double scratch[kPBlock];
+    diag_finalize(a, scratch);
+}
+
+// one block per run; run r's diagnostics land at diag + slot * slot_stride
+__global__ void __launch_bounds__(kPBlock) k_diag_finalize_batch(const DiagArgs* __restrict__ runs, int slot) {
+    __shared__ double scratch[kPBlock];
+    DiagArgs a = runs[blockIdx.x];
+    if (a.diag) a.diag += (int64_t)slot * a.slot_stride;
+    diag_finalize(a, scratch);
 }
 
 // ---- 2D host ------------------------------------------------------------------
@@ -348,6 +386,60 @@ int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, c
         view->n_lines = (int)nx;
     }
     return VP_OK;
+}
+
+// Poisson arguments of one run of a batch (workspace of poisson2d_ws_bytes).
+void pois2d_run_args(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
+                     const double* inv_ksq, double* ex, double* ey, double* drho, double* phi, void* ws,
+                     Pois2dRun* a, Pois2dWsView* view) {
+    Pois2dWs w;
+    pois2d_layout(nx, ny, static_cast<char*>(ws), &w);
+    *a = Pois2dRun{};
+    a->rho = rho;
+    a->nx = (int)nx;
+    a->ny = (int)ny;
+    a->kx = kx;
+    a->ky = ky;
+    a->inv_ksq = inv_ksq;
+    a->drho = drho;
+    a->phi = phi;
+    a->ex = ex;
+    a->ey = ey;
+    a->R = w.R;
+    a->Zp = w.Zp;
+    a->Zx = w.Zx;
+    a->Zy = w.Zy;
+    a->mass_part = w.mass_part;
+    a->we_part = w.we_part;
+    a->emax_part = w.emax_part;
+    if (view) {
+        view->mass_part = w.mass_part;
+        view->we_part = w.we_part;
+        view->emax_part = w.emax_part;
+        view->n_lines = (int)nx;
+    }
+}
+
+int launch_poisson2d_batch(const Pois2dRun* runs, int n_runs, int max_nx, int max_ny, cudaStream_t st) {
+    const int max_nyh = max_ny / 2 + 1;
+    int rc;
+    const size_t s1 = max_ny * sizeof(double2) + max_ny * sizeof(double) + kPBlock * sizeof(double);
+    if ((rc = set_smem((const void*)k_p2_rows_fwd_batch, s1))) return rc;
+    k_p2_rows_fwd_batch<<<dim3((unsigned)max_nx, (unsigned)n_runs), kPBlock, s1, st>>>(runs);
+    if ((rc = check_launch("k_p2_rows_fwd_batch"))) return rc;
+    const size_t s2 = 5 * max_nx * sizeof(double2);
+    if ((rc = set_smem((const void*)k_p2_cols_batch, s2))) return rc;
+    k_p2_cols_batch<<<dim3((unsigned)max_nyh, (unsigned)n_runs), kPBlock, s2, st>>>(runs);
+    if ((rc = check_launch("k_p2_cols_batch"))) return rc;
+    const size_t s3 = max_ny * sizeof(double2) + 3 * max_nyh * sizeof(double2) + kPBlock * sizeof(double);
+    if ((rc = set_smem((const void*)k_p2_rows_inv_batch, s3))) return rc;
+    k_p2_rows_inv_batch<<<dim3((unsigned)max_nx, (unsigned)n_runs), kPBlock, s3, st>>>(runs);
+    return check_launch("k_p2_rows_inv_batch");
+}
+
+int launch_diag_finalize_batch(const DiagArgs* runs, int n_runs, int slot, cudaStream_t st) {
+    k_diag_finalize_batch<<<(unsigned)n_runs, kPBlock, 0, st>>>(runs, slot);
+    return check_launch("k_diag_finalize_batch");
 }
 
 int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_mom, double mass_scale,

@@ -29,42 +29,16 @@ namespace vp {
 constexpr int kU = 8;        // rows per chunk of the sliding window
 constexpr int kBlock = 256;  // threads per block of the sweep kernels
 
-struct StridedArgs {
-    const void* in;
-    void* out;
-    int64_t n_outer;
-    int n_line;
-    int64_t n_inner;
-    int64_t ncg;    // column groups (of VEC elements) per outer row
-    int tiles;      // ceil(ncg / blockDim.x)
-    int seg;        // outputs per line segment
-    int nseg;       // segments per line
-    int64_t items;  // n_outer * tiles * nseg
-    // drift table
-    int64_t sel_div;
-    int sel_mod;
-    const int32_t* shift;
-    const void* W;
-    // kick field
-    const void* E;
-    int e_f64;
-    int64_t e_div;
-    double dt, dv;
-    int window;
-    // fused moment partials [n_outer][tiles][n_line]
-    double* part;
-    // equilibrium split (drifts): column c has feq = eqA[(c / eq_nvy) % eq_nvx] * eqB[c % eq_nvy]
-    const double* eqA;  // NULL: factor 1
-    const double* eqB;  // NULL: no split
-    int64_t eq_nvx, eq_nvy;
-};
 
 // NT = rows of the interpolation window of one output: 6 when the VEC
 // columns of a thread share one shift, 7 when their shifts differ by at most
 // one (the y drift, whose shift follows vy, the contiguous index): each
 // element then gets its own 7-tap weight vector with one zero tap.
+// One work item of a strided sweep: a segment of output rows of one tile of
+// blockDim.x * VEC columns of one outer row. All threads of the block call it
+// with the same item (the moment epilogue synchronises the block).
 template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ>
-__global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
+__device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t item, unsigned char* smem_raw) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
     constexpr int NW = NT - 1;  // window rows carried from chunk to chunk
@@ -72,14 +46,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
     static_assert(NT == 6 || (NT == 7 && !KICK), "7-row windows are for drifts");
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
     double* wpart = reinterpret_cast<double*>(smem_raw);  // [nwarps][seg] per-warp row sums
     const int n = a.n_line;
     const int64_t ni = a.n_inner;
-
-    for (int64_t item = blockIdx.x; item < a.items; item += gridDim.x) {
+    {
         int64_t t_ = item;
         const int sg = (int)(t_ % a.nseg);
         t_ /= a.nseg;
@@ -281,6 +253,29 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(StridedArgs a) {
     }
 }
 
+template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ>
+__global__ void __launch_bounds__(kBlock, 2) k_strided(const __grid_constant__ StridedArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int64_t item = blockIdx.x; item < a.items; item += gridDim.x)
+        strided_item<TS, VEC, NT, KICK, RHO, WRAPREUSE, EQ>(a, item, smem_raw);
+}
+
+// The same sweep over the items of many runs: run r owns the global items
+// [start[r], start[r+1]); a block's items only increase, so its run index
+// only moves forward.
+template <typename TS, int VEC, int NT, bool RHO, bool WRAPREUSE>
+__global__ void __launch_bounds__(kBlock, 2)
+    k_strided_batch(const StridedArgs* __restrict__ runs, const int64_t* __restrict__ start, int n_runs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t total = start[n_runs];
+    int r = 0;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        while (r + 1 < n_runs && start[r + 1] <= g) ++r;
+        const StridedArgs a = runs[r];
+        strided_item<TS, VEC, NT, false, RHO, WRAPREUSE, false>(a, g - start[r], smem_raw);
+    }
+}
+
 // rho[o*n + l] = scale * sum_t part[o][t][l]
 __global__ void k_rho_finalize(const double* __restrict__ part, int64_t n_outer, int n_line, int tiles,
                                double scale, double offset, double* __restrict__ rho) {
@@ -450,24 +445,6 @@ int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int ti
 // ---------------------------------------------------------------------------
 // fused vx + vy kick over [n_planes][nvx][nvy]
 // ---------------------------------------------------------------------------
-struct Kick2dArgs {
-    const void* in;
-    void* out;
-    int64_t n_planes;
-    int nvx, nvy;
-    int team;   // lanes per plane (power of two, <= 32)
-    int groups; // nvy / VEC
-    const double* Ex;
-    const double* Ey;
-    double dt, dvx, dvy;
-    int window;
-    const double* vx;
-    const double* vy;
-    double* moments;
-    // equilibrium split: feq = eqA[ivx] * eqB[ivy] (both NULL: off)
-    const double* eqA;
-    const double* eqB;
-};
 
 // 4 consecutive compute-type values from shared memory (16-byte aligned)
 template <typename C>
@@ -508,13 +485,14 @@ __device__ __forceinline__ void vy_taps(const C (&t)[12], const C (&wy)[6], C (&
     }
 }
 
+// Planes [base, base + teams per block) of a fused kick: one team of lanes
+// per plane. All threads of the block call it with the same base.
 template <typename TS, int VEC, bool DIAG, bool EQ>
-__global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
+__device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t base, unsigned char* smem_raw) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int team = a.team;
     const int teams_per_block = blockDim.x / team;
     const int tid_team = threadIdx.x / team;
@@ -536,8 +514,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
 #pragma unroll
     for (int e = 0; e < VEC; ++e) zero.v[e] = C(0);
 
-    const int64_t stride = (int64_t)gridDim.x * teams_per_block;
-    for (int64_t base = (int64_t)blockIdx.x * teams_per_block; base < a.n_planes; base += stride) {
+    (void)teams_per_block;
+    {
         const int64_t p = base + tid_team;
         const bool pv = p < a.n_planes;
         const bool active = pv && lane_ok;
@@ -735,6 +713,35 @@ __global__ void __launch_bounds__(kBlock, 2) k_kick2d(Kick2dArgs a) {
 }
 
 template <typename TS, int VEC, bool DIAG, bool EQ>
+__global__ void __launch_bounds__(kBlock, 2) k_kick2d(const __grid_constant__ Kick2dArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int teams_per_block = blockDim.x / a.team;
+    const int64_t stride = (int64_t)gridDim.x * teams_per_block;
+    for (int64_t base = (int64_t)blockIdx.x * teams_per_block; base < a.n_planes; base += stride)
+        kick2d_item<TS, VEC, DIAG, EQ>(a, base, smem_raw);
+}
+
+// The fused kick over the planes of many runs: item g of run r (start[r] <=
+// g < start[r+1]) covers planes [(g - start[r]) * teams, ...) of that run,
+// teams = blockDim.x / team of the run.
+template <typename TS, int VEC>
+__global__ void __launch_bounds__(kBlock, 2)
+    k_kick2d_batch(const Kick2dArgs* __restrict__ runs, const int64_t* __restrict__ start, int n_runs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int64_t total = start[n_runs];
+    int r = 0;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        while (r + 1 < n_runs && start[r + 1] <= g) ++r;
+        const Kick2dArgs a = runs[r];
+        // runs differ in team width, so a warp's row buffers move between
+        // items: every warp must be done with the previous item's buffers
+        __syncthreads();
+        const int64_t teams = blockDim.x / a.team;
+        kick2d_item<TS, VEC, false, false>(a, (g - start[r]) * teams, smem_raw);
+    }
+}
+
+template <typename TS, int VEC, bool DIAG, bool EQ>
 static int launch_kick2d_t(Kick2dArgs a, cudaStream_t st) {
     const int teams = kBlock / a.team;
     const size_t smem = (size_t)teams * kU * a.nvy * sizeof(compute_t<TS>);
@@ -820,6 +827,170 @@ int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t n
         case VP_BF16:
             return diag ? launch_kick2d_vec<__nv_bfloat16, true>(a, vec, st)
                         : launch_kick2d_vec<__nv_bfloat16, false>(a, vec, st);
+    }
+    return set_error(VP_ERR_DTYPE, "unknown dtype");
+}
+
+// ---------------------------------------------------------------------------
+// many runs per launch (the batched step): argument blocks of every run live
+// in a device table; one launch per sweep covers the items of all runs
+// ---------------------------------------------------------------------------
+__global__ void k_rho_finalize_batch(const RhoFinRun* __restrict__ runs) {
+    const RhoFinRun a = runs[blockIdx.y];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_outer * a.n_line) return;
+    const int64_t o = i / a.n_line;
+    const int l = (int)(i % a.n_line);
+    double acc = 0.0;
+    for (int t = 0; t < a.tiles; ++t) acc += a.part[(o * a.tiles + t) * (int64_t)a.n_line + l];
+    a.rho[i] = acc * a.scale + a.offset;
+}
+
+int strided_batch_args(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                       int64_t sel_div, int64_t sel_mod, int spread, const int32_t* shift, const void* W,
+                       double* part, int block, StridedArgs* a, int* vec, int* nt) {
+    pick_vec(dtype, n_inner, sel_div, sel_mod, false, spread, in, out, vec, nt);
+    *a = StridedArgs{};
+    a->in = in;
+    a->out = out;
+    a->n_outer = n_outer;
+    a->n_line = (int)n_line;
+    a->n_inner = n_inner;
+    a->sel_div = sel_div;
+    a->sel_mod = (int)sel_mod;
+    a->shift = shift;
+    a->W = W;
+    a->part = part;
+    a->e_div = 1;
+    a->dv = 1.0;
+    a->window = -1;
+    a->seg = (int)n_line;  // whole lines
+    a->nseg = 1;
+    (void)block;
+    return VP_OK;
+}
+
+void strided_batch_finish(StridedArgs* a, int vec, int block) {
+    a->ncg = a->n_inner / vec;
+    a->tiles = (int)((a->ncg + block - 1) / block);
+    a->items = a->n_outer * a->tiles;
+}
+
+int strided_batch_pref_vec(int dtype) { return dtype == VP_F64 ? 2 : 4; }
+
+template <typename TS, int VEC, int NT, bool RHO, bool WRAP>
+static int launch_sb_t(const StridedArgs* runs, const int64_t* start, int n_runs, int block, int grid_cap,
+                       size_t smem, cudaStream_t st) {
+    auto kern = k_strided_batch<TS, VEC, NT, RHO, WRAP>;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return set_cuda_error("cudaFuncSetAttribute(k_strided_batch)");
+    const int occ = occupancy(kern, block, smem);
+    const int grid = std::max(1, std::min(grid_cap, sm_count() * occ));
+    kern<<<grid, block, smem, st>>>(runs, start, n_runs);
+    return check_launch("k_strided_batch");
+}
+
+template <typename TS, bool RHO, bool WRAP>
+static int launch_sb_v(int vec, int nt, const StridedArgs* runs, const int64_t* start, int n_runs, int block,
+                       int grid_cap, size_t smem, cudaStream_t st) {
+    constexpr int V = sizeof(TS) == 8 ? 2 : 4;
+    if (vec == V && nt == 7) return launch_sb_t<TS, V, 7, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, st);
+    if (vec == V) return launch_sb_t<TS, V, 6, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, st);
+    return launch_sb_t<TS, 1, 6, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, st);
+}
+
+template <bool RHO, bool WRAP>
+static int launch_sb_d(int dtype, int vec, int nt, const StridedArgs* runs, const int64_t* start, int n_runs,
+                       int block, int grid_cap, size_t smem, cudaStream_t st) {
+    switch (dtype) {
+        case VP_F32: return launch_sb_v<float, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+        case VP_F64: return launch_sb_v<double, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+        case VP_BF16:
+            return launch_sb_v<__nv_bfloat16, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+    }
+    return set_error(VP_ERR_DTYPE, "unknown dtype");
+}
+
+int launch_strided_batch(int dtype, int vec, int nt, bool rho, bool wrap, const StridedArgs* runs,
+                         const int64_t* start, int n_runs, int block, int grid_cap, int max_line, cudaStream_t st) {
+    if (block != 128 && block != 256) return set_error(VP_ERR_ARG, "batched sweep: block must be 128 or 256");
+    if (rho) {
+        const size_t smem = (size_t)(block / 32) * max_line * sizeof(double);
+        return launch_sb_d<true, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+    }
+    if (wrap) return launch_sb_d<false, true>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, st);
+    return launch_sb_d<false, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, st);
+}
+
+int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int64_t max_points, cudaStream_t st) {
+    const dim3 grid((unsigned)((max_points + 255) / 256), (unsigned)n_runs);
+    k_rho_finalize_batch<<<grid, 256, 0, st>>>(runs);
+    return check_launch("k_rho_finalize_batch");
+}
+
+int kick2d_batch_args(int dtype, const void* in, void* out, int64_t n_planes, int64_t nvx, int64_t nvy,
+                      const double* Ex, const double* Ey, double dt, double dvx, double dvy, int window,
+                      Kick2dArgs* a, int* vec) {
+    *vec = kick2d_vec(dtype, nvy, reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out));
+    *a = Kick2dArgs{};
+    a->in = in;
+    a->out = out;
+    a->n_planes = n_planes;
+    a->nvx = (int)nvx;
+    a->nvy = (int)nvy;
+    a->Ex = Ex;
+    a->Ey = Ey;
+    a->dt = dt;
+    a->dvx = dvx;
+    a->dvy = dvy;
+    a->window = window;
+    return VP_OK;
+}
+
+// team and item count of a run once the batch's common VEC is known;
+// returns the run's shared-memory need per block
+int64_t kick2d_batch_finish(Kick2dArgs* a, int dtype, int vec, int block, int64_t* items) {
+    a->groups = a->nvy / vec;
+    int team = 1;
+    while (team < a->groups) team <<= 1;
+    a->team = team;
+    const int teams = block / team;
+    *items = (a->n_planes + teams - 1) / teams;
+    const int64_t csz = dtype == VP_F64 ? 8 : 4;
+    return (int64_t)teams * kU * a->nvy * csz;
+}
+
+template <typename TS, int VEC>
+static int launch_kb_t(const Kick2dArgs* runs, const int64_t* start, int n_runs, int block, int grid_cap,
+                       size_t smem, cudaStream_t st) {
+    auto kern = k_kick2d_batch<TS, VEC>;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return set_cuda_error("cudaFuncSetAttribute(k_kick2d_batch)");
+    const int occ = occupancy(kern, block, smem);
+    const int grid = std::max(1, std::min(grid_cap, sm_count() * occ));
+    kern<<<grid, block, smem, st>>>(runs, start, n_runs);
+    return check_launch("k_kick2d_batch");
+}
+
+template <typename TS>
+static int launch_kb_v(int vec, const Kick2dArgs* runs, const int64_t* start, int n_runs, int block, int grid_cap,
+                       size_t smem, cudaStream_t st) {
+    if (vec == 4) return launch_kb_t<TS, 4>(runs, start, n_runs, block, grid_cap, smem, st);
+    if constexpr (sizeof(TS) == 8) {
+        if (vec == 2) return launch_kb_t<TS, 2>(runs, start, n_runs, block, grid_cap, smem, st);
+    }
+    return launch_kb_t<TS, 1>(runs, start, n_runs, block, grid_cap, smem, st);
+}
+
+int launch_kick2d_batch(int dtype, int vec, const Kick2dArgs* runs, const int64_t* start, int n_runs, int block,
+                        int grid_cap, size_t smem, cudaStream_t st) {
+    if (block != 128 && block != 256) return set_error(VP_ERR_ARG, "batched kick: block must be 128 or 256");
+    switch (dtype) {
+        case VP_F32: return launch_kb_v<float>(vec, runs, start, n_runs, block, grid_cap, smem, st);
+        case VP_F64: return launch_kb_v<double>(vec, runs, start, n_runs, block, grid_cap, smem, st);
+        case VP_BF16: return launch_kb_v<__nv_bfloat16>(vec, runs, start, n_runs, block, grid_cap, smem, st);
     }
     return set_error(VP_ERR_DTYPE, "unknown dtype");
 }

@@ -264,3 +264,158 @@ class Stepper1D(_Stepper):
             d.eq_v = self.eq[0].data_ptr()
             d.eq_moment = self.eq_moment
         return d
+
+
+class BatchStepper2D:
+    """Independent 2D2V runs of uneven sizes and parameters advanced in
+    lockstep: vp_batch2d_step launches one kernel per substep for all runs
+    (9 launches per step whatever their number) and the state of run r is
+    advanced in place in self.f[r]. Each run's step is vp_step2d's.
+
+    runs: sequence of dicts with Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt
+    (other keys are ignored). tiles: None or a dict with 3-tuples "block",
+    "ctas_per_sm", "segments" per sweep kind (x drifts, y drifts, kick).
+    diagnostics 1: field energy, mass and max shift of every run per step.
+    """
+
+    def __init__(self, runs, dtype=torch.float32, device="cuda", physics_mode=True, window=-1, diagnostics=1,
+                 tiles=None, precise_tables=False, graph_slots=10):
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("BatchStepper2D runs on a CUDA device only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.dtype = dtype
+        self.physics_mode = bool(physics_mode)
+        self.diagnostics = int(diagnostics)
+        self.window = int(window)
+        self.params = [dict(r) for r in runs]
+        n = len(self.params)
+        if n == 0:
+            raise ValueError("no runs")
+        self.n_runs = n
+        esz = torch.empty((), dtype=dtype).element_size()
+        al = lambda b: (b + 255) // 256 * 256  # noqa: E731
+        self.shapes, offs, wsoffs = [], [], []
+        fbytes = wsbytes = 0
+        for p in self.params:
+            shape = (int(p["Nx"]), int(p["Ny"]), int(p["Nvx"]), int(p["Nvy"]))
+            self.shapes.append(shape)
+            offs.append(fbytes)
+            fbytes += al(esz * shape[0] * shape[1] * shape[2] * shape[3])
+            wsoffs.append(wsbytes)
+            wsbytes += al(L.query("vp_step2d_workspace_bytes", *shape))
+        # three arenas (state, two scratch) holding every run at 256-byte offsets
+        self._arenas = [torch.empty(fbytes, dtype=torch.uint8, device=self.device) for _ in range(3)]
+        self._ws = torch.empty(max(wsbytes, 256), dtype=torch.uint8, device=self.device)
+
+        def view(arena, off, shape):
+            nb = esz * shape[0] * shape[1] * shape[2] * shape[3]
+            return arena[off: off + nb].view(dtype).view(shape)
+
+        self.f = [view(self._arenas[0], o, s) for o, s in zip(offs, self.shapes)]
+        self._s1 = [view(self._arenas[1], o, s) for o, s in zip(offs, self.shapes)]
+        self._s2 = [view(self._arenas[2], o, s) for o, s in zip(offs, self.shapes)]
+        self.slots = max(1, int(graph_slots))
+        self.stage = torch.zeros((self.slots, n, L.DIAG_COUNT), dtype=torch.float64, device=self.device)
+        self.drho, self.phi, self.tables = [], [], []
+        runs_c = (L.BatchRun * n)()
+        for r, (p, shape) in enumerate(zip(self.params, self.shapes)):
+            Nx, Ny, Nvx, Nvy = shape
+            Lx, Ly, dt = float(p["Lx"]), float(p["Ly"]), float(p["dt"])
+            dx, dy = Lx / Nx, Ly / Ny
+            dvx, dvy = 2 * p["Vx_max"] / (Nvx - 1), 2 * p["Vy_max"] / (Nvy - 1)
+            grid_dt = torch.float64 if (dtype == torch.float64 or precise_tables) else torch.float32
+            vx_t = torch.linspace(-p["Vx_max"], p["Vx_max"], Nvx, dtype=grid_dt)
+            vy_t = torch.linspace(-p["Vy_max"], p["Vy_max"], Nvy, dtype=grid_dt)
+            tx = ops.DriftTable.from_velocity(vx_t, dt / 2.0, dx, dtype, self.device, precise_tables)
+            ty = ops.DriftTable.from_velocity(vy_t, dt / 2.0, dy, dtype, self.device, precise_tables)
+            kx, ky, inv_ksq = ops.spectral_2d(Nx, Ny, Lx, Ly, self.device)
+            drho = torch.zeros((Nx, Ny), dtype=torch.float64, device=self.device)
+            phi = torch.zeros_like(drho)
+            self.tables.append((tx, ty, kx, ky, inv_ksq))
+            self.drho.append(drho)
+            self.phi.append(phi)
+            c = runs_c[r]
+            c.nx, c.ny, c.nvx, c.nvy = Nx, Ny, Nvx, Nvy
+            c.dt, c.dx, c.dy, c.dvx, c.dvy = dt, dx, dy, dvx, dvy
+            c.window, c.shift_spread_x, c.shift_spread_y = self.window, tx.spread, ty.spread
+            c.f, c.s1, c.s2 = self.f[r].data_ptr(), self._s1[r].data_ptr(), self._s2[r].data_ptr()
+            c.shift_x, c.W_x = tx.shift.data_ptr(), tx.W.data_ptr()
+            c.shift_y, c.W_y = ty.shift.data_ptr(), ty.W.data_ptr()
+            c.kx, c.ky, c.inv_ksq = kx.data_ptr(), ky.data_ptr(), inv_ksq.data_ptr()
+            c.drho, c.phi = drho.data_ptr(), phi.data_ptr()
+            c.diag = self.stage[0, r].data_ptr()
+            c.diag_slot_stride = n * L.DIAG_COUNT
+            c.workspace = self._ws.data_ptr() + wsoffs[r]
+            c.workspace_bytes = L.query("vp_step2d_workspace_bytes", *shape)
+        self.dx = [c.dx for c in runs_c]
+        self.dy = [c.dy for c in runs_c]
+        self.dvx = [c.dvx for c in runs_c]
+        self.dvy = [c.dvy for c in runs_c]
+        t = None
+        if tiles is not None:
+            t = L.BatchTiles()
+            for key in ("block", "ctas_per_sm", "segments"):
+                vals = tiles.get(key, (0, 0, 0))
+                for i in range(L.BATCH_KINDS):
+                    getattr(t, key)[i] = int(vals[i])
+        self.tiles = tiles
+        nb = L.query("vp_batch2d_table_bytes", n)
+        self._table_host = ctypes.create_string_buffer(nb)
+        L.call("vp_batch2d_plan", L.dtype_code(dtype), 1 if self.physics_mode else 0, self.diagnostics, runs_c, n,
+               ctypes.byref(t) if t is not None else None, self._table_host, nb)
+        host = torch.frombuffer(bytearray(self._table_host.raw), dtype=torch.uint8)
+        self._table_dev = host.to(self.device)
+        self._runs_c = runs_c
+        self._graphs = {}
+
+    @property
+    def cells(self) -> int:
+        return int(sum(s[0] * s[1] * s[2] * s[3] for s in self.shapes))
+
+    def set_state(self, r: int, f: torch.Tensor):
+        self.f[r].copy_(f.to(self.dtype))
+
+    def step(self, slot: int = 0, events=None):
+        """One Strang step of every run; diagnostics into self.stage[slot].
+        events: optional ctypes array of 2*VP_PHASE_COUNT cudaEvent_t handles
+        recorded around the substeps."""
+        if not 0 <= slot < self.slots:
+            raise ValueError(f"slot must be in [0, {self.slots})")
+        L.call("vp_batch2d_step", self._table_host, ctypes.c_void_p(self._table_dev.data_ptr()), int(slot),
+               ctypes.cast(events, ctypes.c_void_p) if events is not None else None,
+               ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+
+    def run(self, nsteps: int, history: torch.Tensor | None = None, graph: bool = True):
+        """Advance every run by nsteps. history: optional float64
+        [nsteps, n_runs, VP_DIAG_COUNT]. With graph=True, chunks of `slots`
+        steps are captured once and replayed."""
+        done = 0
+        k = self.slots
+        if graph and nsteps >= k:
+            g = self._graphs.get(k)
+            if g is None:
+                s = torch.cuda.Stream(self.device)
+                s.wait_stream(torch.cuda.current_stream(self.device))
+                with torch.cuda.stream(s):  # the first launches outside the capture
+                    self.step(0)
+                torch.cuda.current_stream(self.device).wait_stream(s)
+                if history is not None:
+                    history[0].copy_(self.stage[0])
+                done = 1
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    for i in range(k):
+                        self.step(i)
+                self._graphs[k] = g
+            while nsteps - done >= k:
+                g.replay()
+                if history is not None:
+                    history[done: done + k].copy_(self.stage)
+                done += k
+        while done < nsteps:
+            self.step(0)
+            if history is not None:
+                history[done].copy_(self.stage[0])
+            done += 1

@@ -40,7 +40,8 @@ def test_every_declared_symbol_is_exported(lib, vp):
 
 
 def test_descriptor_layout_matches_c(vp, tmp_path):
-    fields = {"vp_step2d_desc": vp._lib.Step2dDesc, "vp_step1d_desc": vp._lib.Step1dDesc}
+    fields = {"vp_step2d_desc": vp._lib.Step2dDesc, "vp_step1d_desc": vp._lib.Step1dDesc,
+              "vp_batch2d_run": vp._lib.BatchRun, "vp_batch_tiles": vp._lib.BatchTiles}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, cls in fields.items():
         lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
@@ -87,6 +88,47 @@ def test_argument_errors_without_gpu(lib, vp):
     d.f_out = 0x1000
     assert lib.vp_step2d(ctypes.byref(d), None) == 1  # aliasing buffers
     assert lib.vp_step2d_workspace_bytes(128, 128, 128, 128) > 128 * 128 * 8
+
+
+def _fake_run(L, lib, k, nx=16, ny=16, nvx=32, nvy=32):
+    r = L.BatchRun()
+    r.nx, r.ny, r.nvx, r.nvy = nx, ny, nvx, nvy
+    r.dt, r.dx, r.dy, r.dvx, r.dvy = 0.05, 0.1, 0.1, 0.2, 0.2
+    r.window, r.shift_spread_x, r.shift_spread_y = -1, 1, 1
+    base = 0x10000000 * (k + 1)
+    r.f, r.s1, r.s2 = base, base + 0x1000000, base + 0x2000000
+    r.shift_x = r.W_x = r.shift_y = r.W_y = r.kx = r.ky = r.inv_ksq = base + 0x3000000
+    r.workspace = base + 0x4000000
+    r.workspace_bytes = lib.vp_step2d_workspace_bytes(nx, ny, nvx, nvy)
+    return r
+
+
+def test_batch_plan_on_host(lib, vp):
+    """The batch plan is pure host work: it validates every run and fills the
+    table without touching a device."""
+    L = vp._lib
+    runs = (L.BatchRun * 3)(*[_fake_run(L, lib, k, 16 + 8 * k, 16, 32 + 16 * (k % 2), 32) for k in range(3)])
+    nb = lib.vp_batch2d_table_bytes(3)
+    assert nb > 3 * 4 * 100
+    tab = ctypes.create_string_buffer(nb)
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, None, tab, nb) == 0, lib.vp_last_error()
+    assert tab.raw[:8] == b"VPBATCH1"
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, None, tab, nb - 1) == 3
+    assert lib.vp_batch2d_plan(L.VP_F32, 0, 1, runs, 3, None, tab, nb) == 5  # diagnostics need the field
+    tiles = L.BatchTiles()
+    tiles.block[0] = 64
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, ctypes.byref(tiles), tab, nb) == 1
+    tiles.block[0], tiles.segments[1] = 128, 3
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, ctypes.byref(tiles), tab, nb) == 1
+    tiles.segments[1] = 2
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, ctypes.byref(tiles), tab, nb) == 0
+    runs[1].s1 = runs[1].f
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, None, tab, nb) == 1
+    runs[1].s1 = runs[1].f + 0x1000000
+    runs[2].workspace_bytes = 64
+    assert lib.vp_batch2d_plan(L.VP_F32, 1, 1, runs, 3, None, tab, nb) == 3
+    bad = ctypes.create_string_buffer(nb)
+    assert lib.vp_batch2d_step(bad, bad, 0, None, None) == 1 and b"not a batch table" in lib.vp_last_error()
 
 
 def test_workspace_queries(lib):

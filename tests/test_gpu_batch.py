@@ -1,0 +1,141 @@
+"""Batched uneven runs (vp_batch2d_*): every run of a batch follows the
+single-run step exactly. With the default tile shapes the batch reproduces
+Stepper2D bit for bit (same item bodies, same reduction order); other tile
+shapes only reorder the FP64 charge sums."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import core as O
+
+pytestmark = pytest.mark.gpu
+
+RUNS = [
+    dict(Nx=16, Ny=24, Nvx=32, Nvy=48, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=6.0, dt=0.1),
+    dict(Nx=32, Ny=16, Nvx=48, Nvy=32, Lx=10 * math.pi, Ly=6 * math.pi, Vx_max=8.0, Vy_max=7.0, dt=0.05),
+    dict(Nx=24, Ny=24, Nvx=64, Nvy=64, Lx=2 * math.pi / 0.7, Ly=2 * math.pi / 0.7, Vx_max=7.5, Vy_max=7.5,
+         dt=0.05),
+    dict(Nx=8, Ny=8, Nvx=16, Nvy=12, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=5.0, dt=0.3),
+    dict(Nx=12, Ny=40, Nvx=20, Nvy=24, Lx=8.0, Ly=9.0, Vx_max=5.0, Vy_max=6.0, dt=0.2),
+]
+
+
+def _ic(vp, p, r, dtype):
+    kind = "landau" if r % 2 == 0 else "two_stream"
+    return vp.workloads.initial_2d(kind, p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"], p["Vx_max"],
+                                   p["Vy_max"], 0.05, 2 * math.pi / p["Lx"], 1.5, dtype=dtype)
+
+
+def _single(vp, p, dtype):
+    return vp.Stepper2D(p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"], p["Vx_max"], p["Vy_max"], p["dt"],
+                        dtype=dtype, window=-1, diagnostics=1)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
+def test_batch_equals_single_runs(vp, dtype):
+    b = vp.BatchStepper2D(RUNS, dtype=dtype, window=-1, diagnostics=1)
+    ref = []
+    for r, p in enumerate(RUNS):
+        f0 = _ic(vp, p, r, dtype)
+        b.set_state(r, f0)
+        ref.append((_single(vp, p, dtype), f0.clone()))
+    hist = []
+    for s in range(3):
+        b.step(0)
+        hist.append(b.stage[0].clone())
+        for r, (st, f) in enumerate(ref):
+            ref[r] = (st, st.step(f))
+            assert torch.equal(b.f[r], ref[r][1]), (r, s)
+            assert torch.equal(b.drho[r], st.drho) and torch.equal(b.phi[r], st.phi)
+            d = hist[-1][r].cpu().numpy()
+            np.testing.assert_array_equal(d[[0, 1, 5]], st.diag.cpu().numpy()[[0, 1, 5]])
+
+
+def test_batch_tile_shapes(vp):
+    """Other tile shapes: 128-thread tiles, split lines, one CTA per SM. The
+    drifts and kicks are unchanged; only the FP64 charge sums are reordered."""
+    dtype = torch.float64
+    a = vp.BatchStepper2D(RUNS, dtype=dtype)
+    b = vp.BatchStepper2D(RUNS, dtype=dtype, tiles=dict(block=(128, 128, 128), ctas_per_sm=(1, 1, 1),
+                                                        segments=(2, 4, 1)))
+    c = vp.BatchStepper2D(RUNS, dtype=dtype, tiles=dict(block=(256, 256, 256), ctas_per_sm=(2, 1, 2),
+                                                        segments=(4, 2, 1)))
+    for r, p in enumerate(RUNS):
+        f0 = _ic(vp, p, r, dtype)
+        for s in (a, b, c):
+            s.set_state(r, f0)
+    for _ in range(3):
+        a.step(0)
+        b.step(0)
+        c.step(0)
+    torch.cuda.synchronize()
+    for r in range(len(RUNS)):
+        scale = a.f[r].abs().max().item()
+        assert (b.f[r] - a.f[r]).abs().max().item() <= 1e-13 * scale
+        assert torch.equal(c.f[r], a.f[r])  # same tiles width: identical sums
+    np.testing.assert_allclose(b.stage[0].cpu().numpy()[:, :2], a.stage[0].cpu().numpy()[:, :2], rtol=1e-12)
+
+
+def test_batch_graph_history(vp):
+    """A graph-captured run equals eager steps, history included."""
+    dtype = torch.float32
+    a = vp.BatchStepper2D(RUNS, dtype=dtype, graph_slots=4)
+    b = vp.BatchStepper2D(RUNS, dtype=dtype, graph_slots=4)
+    for r, p in enumerate(RUNS):
+        f0 = _ic(vp, p, r, dtype)
+        a.set_state(r, f0)
+        b.set_state(r, f0)
+    n = 11
+    ha = torch.zeros((n, len(RUNS), 8), dtype=torch.float64, device="cuda")
+    hb = torch.zeros_like(ha)
+    a.run(n, history=ha, graph=True)
+    b.run(n, history=hb, graph=False)
+    torch.cuda.synchronize()
+    for r in range(len(RUNS)):
+        assert torch.equal(a.f[r], b.f[r])
+    assert torch.equal(ha[:, :, :2], hb[:, :, :2])
+    a.run(5, graph=True)  # replays the cached graph, then eager steps
+    b.run(5, graph=False)
+    for r in range(len(RUNS)):
+        assert torch.equal(a.f[r], b.f[r])
+
+
+def test_batch_against_oracle_fp64(vp):
+    """Two runs of the batch against the CPU oracle's step (FP64)."""
+    runs = [RUNS[0], RUNS[3]]
+    b = vp.BatchStepper2D(runs, dtype=torch.float64, window=-1)
+    fs = []
+    for r, p in enumerate(runs):
+        g = O.make_grid2d(p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"], p["Vx_max"], p["Vy_max"],
+                          dtype=np.float64)
+        f = O.landau_2d(g, 0.1, 2 * math.pi / p["Lx"])
+        b.set_state(r, torch.from_numpy(f).cuda())
+        fs.append((g, f))
+    b.step(0)
+    torch.cuda.synchronize()
+    for r, (g, f) in enumerate(fs):
+        fo = O.Stepper2D(g, runs[r]["dt"], window=-1).step(f).f
+        err = np.abs(b.f[r].cpu().numpy() - fo).max() / np.abs(fo).max()
+        assert err <= 1e-12, (r, err)
+
+
+def test_batch_seeded_draws(vp):
+    """The 64 seeded uneven runs: two batched steps equal four of the runs
+    stepped alone, and every run keeps its mass."""
+    runs = vp.workloads.batch_runs()
+    b = vp.BatchStepper2D(runs, dtype=torch.float32)
+    for r, p in enumerate(runs):
+        b.set_state(r, vp.workloads.initial_2d(p["kind"], p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"],
+                                               p["Vx_max"], p["Vy_max"], p["eps"], p["k"], p["v0"]))
+    pick = [0, 17, 40, 63]
+    singles = {r: (_single(vp, runs[r], torch.float32), b.f[r].clone()) for r in pick}
+    h = torch.zeros((2, len(runs), 8), dtype=torch.float64, device="cuda")
+    b.run(2, history=h, graph=False)
+    for r, (st, f) in singles.items():
+        f = st.step(st.step(f))
+        assert torch.equal(b.f[r], f), r
+    m = h[:, :, 1].cpu().numpy()
+    np.testing.assert_allclose(m[1], m[0], rtol=1e-5)
+    assert np.isfinite(h[:, :, 0].cpu().numpy()).all()
