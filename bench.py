@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
+    ap.add_argument("--tiles", choices=["default", "auto", "tune"], default="auto",
+                    help="batched workload: default tile shapes, the autotuner's cache, or tune now")
     a = ap.parse_args()
     wl = WORKLOADS[a.workload]
     a.kind, a.grid, a.L, a.vmax, a.dt, a.ic, a.icp, dflt, a.desc = wl
@@ -577,7 +579,15 @@ def run_batch(a):
     esz = {torch.float32: 4, torch.bfloat16: 2, torch.float64: 8}[dtype]
     runs = wl.batch_runs()
     diag = 1 if a.diagnostics else 0
-    st = vp.BatchStepper2D(runs, dtype=dtype, device=dev, window=1, diagnostics=diag, graph_slots=10)
+    st = vp.BatchStepper2D(runs, dtype=dtype, device=dev, window=1, diagnostics=diag, graph_slots=10,
+                           tiles=None if a.tiles == "default" else "auto")
+    if a.tiles == "tune":  # on a scratch state, before the initial condition is set
+        at = importlib.import_module("jax-pytorch-vlasov_b200.autotune")
+        for r, p in enumerate(runs):
+            st.set_state(r, wl.initial_2d(p["kind"], p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"],
+                                          p["Vx_max"], p["Vy_max"], p["eps"], p["k"], p["v0"], dtype=dtype,
+                                          device=dev))
+        at.tune(st)  # writes the cache ($VLASOV_B200_TUNE_CACHE or the package's tune_b200.json)
     for r, p in enumerate(runs):  # each rank advances its own replica of the batch
         st.set_state(r, wl.initial_2d(p["kind"], p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"],
                                       p["Vx_max"], p["Vy_max"], p["eps"] * (1.0 + 0.01 * rank), p["k"], p["v0"],
@@ -683,7 +693,9 @@ def run_batch(a):
                        "global_batch": n * world,
                        "parallelism": f"{world} independent replicas of the batch" if world > 1 else "one batch",
                        "l2_flush": "not needed: the batch state (all runs) exceeds the L2 several times",
-                       "diagnostics_level": diag, "graph": "10 steps per CUDA graph, replayed"},
+                       "diagnostics_level": diag, "graph": "10 steps per CUDA graph, replayed",
+                       "tiles": {k: v for k, v in (st.tiles or {}).items() if k != "run_segments"},
+                       "tiles_source": a.tiles},
             "roofline": roof,
             "step_gbs": 5 * sweep_bytes / (ms_step * 1e-3) / 1e9,
             "gpu_launches": int(per_step_launches * K),

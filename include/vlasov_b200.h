@@ -303,6 +303,8 @@ typedef struct vp_batch2d_run {
     int32_t window;         /* kick window S (<0: exact kick) */
     int32_t shift_spread_x; /* see vp_drift */
     int32_t shift_spread_y;
+    int32_t segments_x;     /* CTAs per x line of this run: 1, 2, 4 (0: the batch's tile shape) */
+    int32_t segments_y;     /* CTAs per y line of this run (0: the batch's tile shape) */
     int32_t reserved;       /* 0 */
     void* f;                /* [nx][ny][nvx][nvy] state, advanced in place */
     void* s1;               /* scratch of the size of f */

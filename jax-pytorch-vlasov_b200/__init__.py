@@ -8,6 +8,7 @@ Modules:
   engine      -- Stepper2D / Stepper1D: one library call per Strang step, CUDA graphs;
                  BatchStepper2D: many uneven runs, one launch per substep for all
   workloads   -- seeded initial conditions and the batched-runs parameter draws
+  autotune    -- tile shapes of the batched sweeps, measured and cached in JSON
   ops         -- tensor-level wrappers of the C ABI (include/vlasov_b200.h)
   build       -- compiles csrc/*.cu into libvlasov_b200.so for sm_100a
 
@@ -23,7 +24,7 @@ __all__ = ["BatchStepper2D", "Stepper1D", "Stepper2D", "VlasovError", "load", "o
 
 
 def __getattr__(name):
-    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads"):
+    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune"):
         import importlib
 
         return importlib.import_module(f"{__name__}.{name}")

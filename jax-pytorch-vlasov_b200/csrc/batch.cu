@@ -144,7 +144,7 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     RhoFinRun* rf = at<RhoFinRun>(table, L.off_rfin);
     DiagArgs* dg = at<DiagArgs>(table, L.off_diag);
     int vx_min = 4, ntx_min = 7, vy_min = 4, nty_min = 7, vk_min = 4;
-    bool wrap_x = true, wrap_y = true;
+    bool wrap_x = false, wrap_y = false;  // some run sweeps whole lines of a multiple of 8 rows
     for (int r = 0; r < n_runs; ++r) {
         const vp_batch2d_run& d = runs[r];
         if (d.nx <= 0 || d.ny <= 0 || d.nvx <= 1 || d.nvy <= 1)
@@ -156,6 +156,9 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         if (phys && (!d.kx || !d.ky || !d.inv_ksq))
             return set_error(VP_ERR_ARG, "vp_batch2d_plan: null spectral arrays");
         if (d.dvx == 0.0 || d.dvy == 0.0) return set_error(VP_ERR_ARG, "vp_batch2d_plan: zero velocity spacing");
+        for (int sg : {d.segments_x, d.segments_y})
+            if (sg != 0 && sg != 1 && sg != 2 && sg != 4)
+                return set_error(VP_ERR_ARG, "vp_batch2d_plan: run segments must be 0, 1, 2 or 4");
         if (d.nx > 4096 || d.ny > 1024)
             return set_error(VP_ERR_ARG, "vp_batch2d_plan: nx must be <= 4096 and ny <= 1024");
         const size_t need = step2d_layout(d.nx, d.ny, d.nvx, d.nvy, nullptr, nullptr);
@@ -219,8 +222,10 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         h.max_nx = std::max<int32_t>(h.max_nx, d.nx);
         h.max_ny = std::max<int32_t>(h.max_ny, d.ny);
         h.max_points = std::max<int64_t>(h.max_points, nx * ny);
-        wrap_x = wrap_x && segs[0] == 1 && nx % 8 == 0;
-        wrap_y = wrap_y && segs[1] == 1 && ny % 8 == 0;
+        const int sgx = d.segments_x ? d.segments_x : segs[0];
+        const int sgy = d.segments_y ? d.segments_y : segs[1];
+        wrap_x = wrap_x || (sgx == 1 && nx % 8 == 0);
+        wrap_y = wrap_y || (sgy == 1 && ny % 8 == 0);
     }
     // one kernel variant per sweep kind: the widest form every run supports
     const int pref = strided_batch_pref_vec(dtype);
@@ -240,15 +245,17 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     sx[0] = sy1[0] = sy2[0] = sk[0] = 0;
     int64_t kick_smem = 0;
     for (int r = 0; r < n_runs; ++r) {
+        const int sgx = runs[r].segments_x ? runs[r].segments_x : segs[0];
+        const int sgy = runs[r].segments_y ? runs[r].segments_y : segs[1];
         for (StridedArgs* a : {&x1[r], &x2[r]}) {
             strided_batch_finish(a, h.vec_x, block[0]);
-            a->seg = (a->n_line + segs[0] - 1) / segs[0];
+            a->seg = (a->n_line + sgx - 1) / sgx;
             a->nseg = (a->n_line + a->seg - 1) / a->seg;
             a->items *= a->nseg;
         }
         for (StridedArgs* a : {&y1[r], &y2[r]}) {
             strided_batch_finish(a, h.vec_y, block[1]);
-            a->seg = (a->n_line + segs[1] - 1) / segs[1];
+            a->seg = (a->n_line + sgy - 1) / sgy;
             a->nseg = (a->n_line + a->seg - 1) / a->seg;
             a->items *= a->nseg;
         }

@@ -156,7 +156,8 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
         // rows of the chunk whose first output row is lc (U loads in flight)
         V nx[kU];
         auto load_chunk = [&](int lc) {
-            const bool last = WRAPREUSE && (lc + kU >= l_end);
+            // whole lines of a multiple of kU rows end on the rows they began with
+            const bool last = WRAPREUSE && a.nseg == 1 && (n % kU) == 0 && (lc + kU >= l_end);
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 if constexpr (!KICK) {

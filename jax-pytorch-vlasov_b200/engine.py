@@ -273,8 +273,10 @@ class BatchStepper2D:
     advanced in place in self.f[r]. Each run's step is vp_step2d's.
 
     runs: sequence of dicts with Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt
-    (other keys are ignored). tiles: None or a dict with 3-tuples "block",
-    "ctas_per_sm", "segments" per sweep kind (x drifts, y drifts, kick).
+    (other keys are ignored). tiles: None (defaults), "auto" (the autotuner's
+    cached choices, see autotune.py), or a dict with 3-tuples "block",
+    "ctas_per_sm", "segments" per sweep kind (x drifts, y drifts, kick) and
+    optionally "run_segments": one (x, y) pair per run.
     diagnostics 1: field energy, mass and max shift of every run per step.
     """
 
@@ -353,22 +355,59 @@ class BatchStepper2D:
         self.dy = [c.dy for c in runs_c]
         self.dvx = [c.dvx for c in runs_c]
         self.dvy = [c.dvy for c in runs_c]
+        self._runs_c = runs_c
+        self._table_dev = None
+        if isinstance(tiles, str):
+            if tiles != "auto":
+                raise ValueError("tiles: None, 'auto' or a dict")
+            from . import autotune
+
+            tiles = autotune.cached_tiles(self.shapes, dtype)
+        self.retile(tiles)
+
+    def retile(self, tiles=None):
+        """Re-plan the batch with other tile shapes (drops captured graphs)."""
+        n = self.n_runs
         t = None
+        seg = (tiles or {}).get("run_segments")
+        for r in range(n):
+            sx, sy = (seg[r] if seg is not None else (0, 0))
+            self._runs_c[r].segments_x, self._runs_c[r].segments_y = int(sx), int(sy)
         if tiles is not None:
             t = L.BatchTiles()
             for key in ("block", "ctas_per_sm", "segments"):
                 vals = tiles.get(key, (0, 0, 0))
                 for i in range(L.BATCH_KINDS):
                     getattr(t, key)[i] = int(vals[i])
-        self.tiles = tiles
         nb = L.query("vp_batch2d_table_bytes", n)
-        self._table_host = ctypes.create_string_buffer(nb)
-        L.call("vp_batch2d_plan", L.dtype_code(dtype), 1 if self.physics_mode else 0, self.diagnostics, runs_c, n,
-               ctypes.byref(t) if t is not None else None, self._table_host, nb)
-        host = torch.frombuffer(bytearray(self._table_host.raw), dtype=torch.uint8)
+        table = ctypes.create_string_buffer(nb)
+        L.call("vp_batch2d_plan", L.dtype_code(self.dtype), 1 if self.physics_mode else 0, self.diagnostics,
+               self._runs_c, n, ctypes.byref(t) if t is not None else None, table, nb)
+        host = torch.frombuffer(bytearray(table.raw), dtype=torch.uint8)
+        if self._table_dev is not None:
+            torch.cuda.current_stream(self.device).synchronize()  # no step may still read the old table
+        self._table_host = table
         self._table_dev = host.to(self.device)
-        self._runs_c = runs_c
+        self.tiles = tiles
         self._graphs = {}
+
+    def phase_ms(self, steps: int = 3):
+        """Mean per-substep device times (ms) of `steps` eager steps, keyed by
+        the phase names of the step (drift_x1, drift_y1_rho, field, kick,
+        drift_y2, drift_x2, diag). The state advances."""
+        nph = 7
+        rows = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * nph)] for _ in range(steps)]
+        for row in rows:
+            for e in row:
+                e.record()
+        torch.cuda.synchronize(self.device)
+        for row in rows:
+            arr = (ctypes.c_void_p * (2 * nph))(*[e.cuda_event for e in row])
+            self.step(0, events=arr)
+        torch.cuda.synchronize(self.device)
+        names = ("drift_x1", "drift_y1_rho", "field", "kick", "drift_y2", "drift_x2", "diag")
+        return {nm: sum(row[2 * j].elapsed_time(row[2 * j + 1]) for row in rows) / steps
+                for j, nm in enumerate(names)}
 
     @property
     def cells(self) -> int:

@@ -139,3 +139,30 @@ def test_batch_seeded_draws(vp):
     m = h[:, :, 1].cpu().numpy()
     np.testing.assert_allclose(m[1], m[0], rtol=1e-5)
     assert np.isfinite(h[:, :, 0].cpu().numpy()).all()
+
+
+def test_autotune_small_batch(vp, tmp_path):
+    """The autotuner runs on a small batch, records its choices, and the tuned
+    batch computes the same steps (FP64: only the charge sums reorder)."""
+    at = vp.autotune
+    dtype = torch.float64
+    a = vp.BatchStepper2D(RUNS, dtype=dtype)
+    t = vp.BatchStepper2D(RUNS, dtype=dtype)
+    for r, p in enumerate(RUNS):
+        t.set_state(r, _ic(vp, p, r, dtype))
+    cache = str(tmp_path / "tune.json")
+    tiles = at.tune(t, reps=1, steps=1, cache_file=cache)
+    assert len(tiles["run_segments"]) == len(RUNS)
+    saved = at.load_cache(cache)
+    assert at.launch_key(t.shapes, dtype) in saved
+    assert at.cached_tiles(t.shapes, dtype, cache=saved)["run_segments"] == [tuple(s) for s in tiles["run_segments"]]
+    for r, p in enumerate(RUNS):
+        f0 = _ic(vp, p, r, dtype)
+        a.set_state(r, f0)
+        t.set_state(r, f0)
+    for _ in range(2):
+        a.step(0)
+        t.step(0)
+    torch.cuda.synchronize()
+    for r in range(len(RUNS)):
+        assert (t.f[r] - a.f[r]).abs().max().item() <= 1e-13 * a.f[r].abs().max().item()

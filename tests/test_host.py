@@ -134,3 +134,22 @@ def test_dist_gloo_world2():
         p.join(120)
         assert p.exitcode == 0
     assert out[0] == (2, 11.0, 2.0) and out[1] == (2, 11.0, 2.0)
+
+
+def test_autotune_cache_keys(vp, tmp_path):
+    """Cache entries per (kind, N_axis, N_contig, dtype) and per batch
+    signature; missing entries fall back to the default tile shapes."""
+    at = importlib.import_module(PACKAGE + ".autotune")
+    shapes = [(16, 16, 32, 32), (64, 64, 48, 48), (16, 16, 32, 32)]
+    assert at.segment_key("x", shapes[1], torch.float32) == "segments:x:64:147456:float32"
+    assert at.segment_key("y", shapes[1], torch.float32) == "segments:y:64:2304:float32"
+    assert at.launch_key(shapes, torch.float32) == at.launch_key(shapes[::-1], torch.float32)
+    t = at.cached_tiles(shapes, torch.float32, cache={})
+    assert t["block"] == [256, 256, 256] and t["run_segments"] == [(1, 1)] * 3
+    cache = {at.segment_key("y", shapes[1], torch.float32): 2,
+             at.launch_key(shapes, torch.float32): {"block": [128, 256, 128], "ctas_per_sm": [1, 2, 2]}}
+    path = tmp_path / "tune.json"
+    at.save_cache(cache, str(path))
+    t = at.cached_tiles(shapes, torch.float32, cache=at.load_cache(str(path)))
+    assert t["block"] == [128, 256, 128] and t["ctas_per_sm"] == [1, 2, 2]
+    assert t["run_segments"] == [(1, 1), (1, 2), (1, 1)]
