@@ -342,6 +342,35 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
  * all runs (VP_PHASE_DRIFT_Y1 includes the rho finalize), NULL to skip. */
 int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void* const* events, void* stream);
 
+/* ---- learned drift correction (BF16 tensor cores) ------------------------
+ * No reference counterpart. A per-cell network corrects the 6 Lagrange
+ * weights of a periodic drift (the sweep of vp_drift, FP32 storage):
+ *   x  = [f_k / max|f| (k < 6), alpha - 1/2, 1, 0...]  (16 inputs)
+ *   h1 = relu(W1 x), h2 = relu(W2 [h1, 1, 0...]), o = W3 [h2, 1, 0...]
+ *   out = sum_k (W[k][j] + o_k - mean(o_0..o_5)) f_k
+ * with f_k the stencil values of vp_drift, j the table column of the cell
+ * and alpha[j] its fractional shift. Matrix products run on tcgen05 tensor
+ * cores with BF16 operands and FP32 accumulation.
+ * net: bf16 row-major, packed W1 [64][16] (column 7 = bias), W2 [64][80]
+ * (column 64 = bias), W3 [16][80] (rows 6..15 zero), then the transposed
+ * copies W3T [64][16] (W3T[h][o] = W3[o][h]) and W2T [64][64]
+ * (W2T[i][m] = W2[m][i]) used by the backward pass.
+ * status: device int32, set to 1 when a tensor-core completion wait timed out
+ * (the results are then invalid). */
+#define VP_MLP_NET_ELEMS (64 * 16 + 64 * 80 + 16 * 80 + 64 * 16 + 64 * 64)
+#define VP_MLP_GRAD_ELEMS (64 * 16 + 64 * 80 + 16 * 80)
+int vp_mlp_drift(const float* f_in, float* f_out, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                 int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W,
+                 const float* alpha, const void* net, int32_t* status, void* stream);
+/* Training pass over every cell of one drift: r = (out - target) * inv_scale;
+ * *loss += sum r^2 and grad (float [VP_MLP_GRAD_ELEMS]: dW1, dW2, dW3 in the
+ * layout of net) += the gradient of sum r^2 (both accumulated, not
+ * overwritten). */
+int vp_mlp_train(const float* f_in, const float* target, int64_t n_outer, int64_t n_line,
+                 int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift,
+                 const float* W, const float* alpha, const void* net, double inv_scale, float* grad,
+                 double* loss, int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,8 @@ Modules:
                  BatchStepper2D: many uneven runs, one launch per substep for all
   workloads   -- seeded initial conditions and the batched-runs parameter draws
   autotune    -- tile shapes of the batched sweeps, measured and cached in JSON
+  corrector   -- learned drift-weight correction on tcgen05 tensor cores: network,
+                 training on coarse / refined pairs, LearnedStepper2D
   ops         -- tensor-level wrappers of the C ABI (include/vlasov_b200.h)
   build       -- compiles csrc/*.cu into libvlasov_b200.so for sm_100a
 
@@ -24,7 +26,7 @@ __all__ = ["BatchStepper2D", "Stepper1D", "Stepper2D", "VlasovError", "load", "o
 
 
 def __getattr__(name):
-    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune"):
+    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune", "corrector"):
         import importlib
 
         return importlib.import_module(f"{__name__}.{name}")

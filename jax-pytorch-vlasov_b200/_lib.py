@@ -114,6 +114,8 @@ SIGNATURES = {
     "vp_batch2d_plan": (ctypes.c_int, [I32, I32, I32, ctypes.POINTER(BatchRun), I32, ctypes.POINTER(BatchTiles), P,
                                        SZ]),
     "vp_batch2d_step": (ctypes.c_int, [P, P, I32, P, P]),
+    "vp_mlp_drift": (ctypes.c_int, [P, P, I64, I64, I64, I64, I64, P, P, P, P, P, P]),
+    "vp_mlp_train": (ctypes.c_int, [P, P, I64, I64, I64, I64, I64, P, P, P, P, D, P, P, P, P]),
     "vp_step2d_workspace_bytes": (SZ, [I64, I64, I64, I64]),
     "vp_step1d": (ctypes.c_int, [ctypes.POINTER(Step1dDesc), P]),
     "vp_step1d_workspace_bytes": (SZ, [I64, I64]),

@@ -1,0 +1,577 @@
+// Learned correction of the drift interpolation weights on tensor cores.
+//
+// A per-cell network proposes a correction dw to the 6 Lagrange weights of
+// a periodic drift (the x / y sweeps of the 2D2V step):
+//   x  = [f_k / s (k < 6), alpha - 1/2, 1, 0 x 8]          s = max_k |f_k|
+//   h1 = relu(W1 x)            W1: [64][16]  (column 7 = bias)
+//   h2 = relu(W2 [h1, 1, 0])   W2: [64][80]  (column 64 = bias)
+//   o  = W3 [h2, 1, 0]         W3: [16][80]  (rows >= 6 zero)
+//   dw = o[0:6] - mean(o[0:6])        (the weights keep summing to one)
+//   out = sum_k (w_k + dw_k) f_k
+// x, h1, h2 and the weights are BF16 operands of tcgen05.mma (kind::f16,
+// FP32 accumulators in tensor memory); dw and the output are FP32.
+//
+// One CTA of 128 threads owns one tile of 128 cells (the MMA M) at a time,
+// thread t <-> cell t <-> accumulator lane t. Every operand lives in shared
+// memory in the canonical K-major layout without swizzle (8 x 16-byte core
+// matrices, K chunks 128 bytes apart, 8-row groups (K/8)*128 bytes apart).
+// A single thread issues the MMAs; completion is signalled through one
+// mbarrier (tcgen05.commit) that every thread waits on, with a time limit:
+// a wait that runs out sets *status and the kernel leaves after releasing
+// its tensor memory.
+//
+// Training (TRAIN = true) adds, per tile, the residual against a target,
+//   r = (out - target) * inv_scale,  loss += sum r^2,
+// the backward deltas on tensor cores
+//   do  = P (2 r inv_scale f)           (P: the zero-mean projection)
+//   dz2 = (do  W3)[0:64] * [z2 > 0]     (MMA with W3 transposed)
+//   dz1 = (dz2 W2)[0:64] * [z1 > 0]     (MMA with W2 transposed)
+// and the weight gradients accumulated in tensor memory over all tiles of
+// the CTA (reduction over cells = the MMA K):
+//   [dW2; dW1] = [dz2^T; dz1^T] [h1', x]      (one M=128, N=96 chain)
+//   dW3^T      = h2'^T do                     (M=128, N=16)
+// added to the global FP32 gradient once per CTA.
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace vp {
+namespace mlp {
+
+constexpr int TM = 128;  // cells per tile = MMA M = threads per CTA
+constexpr int K1 = 16;   // layer-1 input width
+constexpr int HID = 64;  // hidden width
+constexpr int K2 = 80;   // hidden + constant + zero pad
+constexpr int NO = 16;   // layer-3 outputs (6 used)
+constexpr int KW = 128;  // cells per weight-gradient chain (= TM)
+
+// bf16 element offsets of the packed network (see include/vlasov_b200.h)
+constexpr int OFF_W1 = 0;
+constexpr int OFF_W2 = OFF_W1 + HID * K1;
+constexpr int OFF_W3 = OFF_W2 + HID * K2;
+constexpr int OFF_W3T = OFF_W3 + NO * K2;
+constexpr int OFF_W2T = OFF_W3T + HID * NO;
+constexpr int NET_ELEMS = OFF_W2T + HID * HID;
+// FP32 gradient offsets
+constexpr int G_W1 = 0;
+constexpr int G_W2 = G_W1 + HID * K1;
+constexpr int G_W3 = G_W2 + HID * K2;
+constexpr int GRAD_ELEMS = G_W3 + NO * K2;
+
+// ---------------------------------------------------------------------------
+// tcgen05 / mbarrier primitives (inline PTX)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// byte offset of element (r, k) of a [R][K] K-major bf16 matrix
+__device__ __forceinline__ uint32_t kmaj(int r, int k, int K) {
+    return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory descriptor of the 16-wide K slice starting at k0
+__device__ __forceinline__ uint64_t kdesc(uint32_t base, int k0, int K) {
+    const uint32_t start = base + (uint32_t)(k0 >> 3) * 128u;
+    const uint64_t lbo = 128u >> 4;                          // next 8-wide K chunk
+    const uint64_t sbo = ((uint32_t)(K >> 3) * 128u) >> 4;  // next 8-row group
+    return (uint64_t)((start >> 4) & 0x3FFFu) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+// instruction descriptor: BF16 x BF16 -> F32, A and B K-major, M x N
+__host__ __device__ constexpr uint32_t idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(id), "r"(acc)
+        : "memory");
+}
+
+// D[TM][N] (+)= A[TM][K] B[N][K]^T, K a multiple of 16
+__device__ __forceinline__ void gemm(uint32_t d_tmem, uint32_t a_base, uint32_t b_base, int K, int N,
+                                     bool accumulate) {
+    const uint32_t id = idesc(TM, N);
+    for (int k0 = 0; k0 < K; k0 += 16)
+        mma(d_tmem, kdesc(a_base, k0, K), kdesc(b_base, k0, K), id, (accumulate || k0 > 0) ? 1u : 0u);
+}
+
+__device__ __forceinline__ void commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait for the mbarrier phase with the given parity; false after ~1 s
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    const uint64_t t0 = now_ns();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (now_ns() - t0 > 1000000000ull) return false;
+    }
+}
+
+// 16 consecutive FP32 columns of this thread's accumulator lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v) {
+    *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory plan (bytes)
+// ---------------------------------------------------------------------------
+struct Smem {
+    uint32_t x, h1, h2, w1, w2, w3, w3t, w2t;  // both modes
+    uint32_t dO, dz2, aw, bw, h2t, doT;        // training only
+    uint32_t bar, tslot, loss, total;
+};
+
+__host__ __device__ constexpr uint32_t al128(uint32_t b) { return (b + 127u) & ~127u; }
+
+__host__ __device__ constexpr Smem plan(bool train) {
+    Smem s{};
+    uint32_t o = 0;
+    auto take = [&](uint32_t b) {
+        const uint32_t r = o;
+        o += al128(b);
+        return r;
+    };
+    s.x = take(TM * K1 * 2);
+    s.h1 = take(TM * K2 * 2);
+    s.h2 = take(TM * K2 * 2);
+    s.w1 = take(HID * K1 * 2);
+    s.w2 = take(HID * K2 * 2);
+    s.w3 = take(NO * K2 * 2);
+    s.w3t = take(HID * NO * 2);
+    s.w2t = take(HID * HID * 2);
+    if (train) {
+        s.dO = take(TM * NO * 2);    // [cell][16]   A of dh2
+        s.dz2 = take(TM * HID * 2);  // [cell][64]   A of dh1
+        s.aw = take(128 * KW * 2);   // [dz2^T; dz1^T] [128][cells]
+        s.bw = take(96 * KW * 2);    // [h1'^T; x^T]   [96][cells]
+        s.h2t = take(128 * KW * 2);  // h2'^T (80 rows, rest zero) [128][cells]
+        s.doT = take(NO * KW * 2);   // do^T [16][cells]
+    }
+    s.bar = take(8);
+    s.tslot = take(4);
+    s.loss = take(TM * 8);
+    s.total = o;
+    return s;
+}
+
+// tensor-memory columns
+constexpr uint32_t T_D1 = 0, T_D2 = 64, T_D3 = 128;  // forward (D3: 16 used of 32)
+constexpr uint32_t T_G2 = 160, T_G1 = 224;           // backward deltas
+constexpr uint32_t T_WA = 288, T_WB = 384;           // [dW2 | dW1] (96), dW3^T (16)
+constexpr uint32_t TMEM_TRAIN = 512, TMEM_INFER = 256;
+
+struct SweepArgs {
+    const float* in;
+    const float* target;  // training only
+    float* out;           // inference only
+    int64_t n_outer, n_inner;
+    int n_line;
+    int64_t sel_div;
+    int sel_mod;
+    const int32_t* shift;
+    const float* W;      // [6][sel_mod] Lagrange weights
+    const float* alpha;  // [sel_mod] fractional shifts
+    const __nv_bfloat16* net;
+    float* grad;      // training: [GRAD_ELEMS]
+    double* loss;     // training: sum of r^2
+    float inv_scale;  // training: residual scale
+    int64_t tiles;    // n_outer * n_line * ceil(n_inner / TM)
+    int* status;
+};
+
+// copy a row-major [R][K] bf16 matrix from global into the K-major layout
+__device__ void load_matrix(unsigned char* sm, uint32_t dst, const __nv_bfloat16* src, int R, int K) {
+    for (int i = threadIdx.x; i < R * K; i += blockDim.x) {
+        const int r = i / K, k = i % K;
+        *reinterpret_cast<__nv_bfloat16*>(sm + dst + kmaj(r, k, K)) = src[i];
+    }
+}
+
+template <bool TRAIN>
+__global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ SweepArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    constexpr Smem S = plan(TRAIN);
+    const int t = threadIdx.x;
+    const uint32_t base = smem_u32(sm);
+    const uint32_t bar = base + S.bar;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + S.tslot);
+    const uint32_t ncols = TRAIN ? TMEM_TRAIN : TMEM_INFER;
+
+    // zero every operand buffer once: padding rows / columns stay zero
+    for (uint32_t i = t * 16; i < S.bar; i += TM * 16) *reinterpret_cast<uint4*>(sm + i) = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    load_matrix(sm, S.w1, a.net + OFF_W1, HID, K1);
+    load_matrix(sm, S.w2, a.net + OFF_W2, HID, K2);
+    load_matrix(sm, S.w3, a.net + OFF_W3, NO, K2);
+    if (TRAIN) {
+        load_matrix(sm, S.w3t, a.net + OFF_W3T, HID, NO);
+        load_matrix(sm, S.w2t, a.net + OFF_W2T, HID, HID);
+    }
+    // constant-one columns of the layer inputs (bias columns)
+    st_bf16(sm, S.x + kmaj(t, 7, K1), 1.0f);
+    st_bf16(sm, S.h1 + kmaj(t, HID, K2), 1.0f);
+    st_bf16(sm, S.h2 + kmaj(t, HID, K2), 1.0f);
+    if (TRAIN) {
+        // the transposed copies hold the constant rows: h1'^T row 64 and h2'^T row 64
+        st_bf16(sm, S.bw + kmaj(HID, t, KW), 1.0f);
+        st_bf16(sm, S.h2t + kmaj(HID, t, KW), 1.0f);
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (t < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tm = *tslot;
+    const uint32_t lane_base = tm + ((uint32_t)(t & ~31) << 16);  // this warp's 32 lanes
+    uint32_t phase = 0;
+    bool ok = true;
+    double loss_acc = 0.0;
+    bool wacc = false;  // weight-gradient accumulators hold data
+
+    // one MMA group issued by thread 0, completion awaited by all threads
+    auto run = [&](auto&& issue) -> bool {
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (t == 0) {
+            issue();
+            commit(bar);
+        }
+        const bool done = mbar_wait(bar, phase & 1u);
+        phase++;
+        const bool all = __syncthreads_and(done) != 0;  // every thread takes the same exit
+        fence_after();
+        return all;
+    };
+
+    const int64_t cblocks = (a.n_inner + TM - 1) / TM;
+    for (int64_t tile = blockIdx.x; tile < a.tiles && ok; tile += gridDim.x) {
+        const int64_t cb = tile % cblocks;
+        const int64_t ol = tile / cblocks;
+        const int l = (int)(ol % a.n_line);
+        const int64_t o = ol / a.n_line;
+        const int64_t c = cb * TM + t;
+        const bool act = c < a.n_inner;
+        const int n = a.n_line;
+        // stencil of this cell: f_k = in[o, (l - s - (k - 2)) mod n, c]
+        float f[6], w[6];
+        float al = 0.0f;
+        if (act) {
+            const int j = (int)((c / a.sel_div) % a.sel_mod);
+            const int s = a.shift[j];
+            al = a.alpha[j];
+            int r = (int)(((int64_t)l - s + 2) % n);
+            if (r < 0) r += n;
+            const float* col = a.in + (o * n) * a.n_inner + c;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                f[k] = col[(int64_t)r * a.n_inner];
+                w[k] = a.W[k * a.sel_mod + j];
+                r = r == 0 ? n - 1 : r - 1;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) f[k] = w[k] = 0.0f;
+        }
+        float sc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sc = fmaxf(sc, fabsf(f[k]));
+        const float inv = sc > 0.0f ? 1.0f / sc : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) st_bf16(sm, S.x + kmaj(t, k, K1), f[k] * inv);
+        st_bf16(sm, S.x + kmaj(t, 6, K1), act ? al - 0.5f : 0.0f);
+        if (TRAIN) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) st_bf16(sm, S.bw + kmaj(K2 + k, t, KW), f[k] * inv);
+            st_bf16(sm, S.bw + kmaj(K2 + 6, t, KW), act ? al - 0.5f : 0.0f);
+            st_bf16(sm, S.bw + kmaj(K2 + 7, t, KW), act ? 1.0f : 0.0f);
+        }
+        // layer 1
+        if (!(ok = run([&] { gemm(tm + T_D1, base + S.x, base + S.w1, K1, HID, false); }))) break;
+        uint32_t m1[2] = {0u, 0u}, m2[2] = {0u, 0u};  // relu masks of z1, z2
+#pragma unroll
+        for (int q = 0; q < HID / 16; ++q) {
+            float v[16];
+            tmem_ld16(lane_base + T_D1 + q * 16, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int h = q * 16 + i;
+                const bool pos = v[i] > 0.0f;
+                if (pos) m1[h >> 5] |= 1u << (h & 31);
+                const float y = act && pos ? v[i] : 0.0f;
+                st_bf16(sm, S.h1 + kmaj(t, h, K2), y);
+                if (TRAIN) st_bf16(sm, S.bw + kmaj(h, t, KW), y);
+            }
+        }
+        // layer 2
+        if (!(ok = run([&] { gemm(tm + T_D2, base + S.h1, base + S.w2, K2, HID, false); }))) break;
+#pragma unroll
+        for (int q = 0; q < HID / 16; ++q) {
+            float v[16];
+            tmem_ld16(lane_base + T_D2 + q * 16, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int h = q * 16 + i;
+                const bool pos = v[i] > 0.0f;
+                if (pos) m2[h >> 5] |= 1u << (h & 31);
+                const float y = act && pos ? v[i] : 0.0f;
+                st_bf16(sm, S.h2 + kmaj(t, h, K2), y);
+                if (TRAIN) st_bf16(sm, S.h2t + kmaj(h, t, KW), y);
+            }
+        }
+        if (TRAIN) st_bf16(sm, S.h2t + kmaj(HID, t, KW), act ? 1.0f : 0.0f);
+        // layer 3
+        if (!(ok = run([&] { gemm(tm + T_D3, base + S.h2, base + S.w3, K2, NO, false); }))) break;
+        float ov[16];
+        tmem_ld16(lane_base + T_D3, ov);
+        tmem_wait_ld();
+        float mean = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) mean += ov[k];
+        mean *= (1.0f / 6.0f);
+        float y = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) y = fmaf(w[k] + (ov[k] - mean), f[k], y);
+        if (!TRAIN) {
+            if (act) a.out[(o * n + l) * a.n_inner + c] = y;
+            continue;
+        }
+        // ---- training: residual, deltas, weight gradients ----
+        const float tg = act ? a.target[(o * n + l) * a.n_inner + c] : 0.0f;
+        const float r = act ? (y - tg) * a.inv_scale : 0.0f;
+        loss_acc += (double)r * r;
+        const float gy = 2.0f * r * a.inv_scale;  // dL/dy
+        float g6[6], gm = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            g6[k] = gy * f[k];
+            gm += g6[k];
+        }
+        gm *= (1.0f / 6.0f);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float d = act ? g6[k] - gm : 0.0f;
+            st_bf16(sm, S.dO + kmaj(t, k, NO), d);
+            st_bf16(sm, S.doT + kmaj(k, t, KW), d);
+        }
+        // dh2 = do W3 (B = W3^T [64][16])
+        if (!(ok = run([&] { gemm(tm + T_G2, base + S.dO, base + S.w3t, NO, HID, false); }))) break;
+#pragma unroll
+        for (int q = 0; q < HID / 16; ++q) {
+            float v[16];
+            tmem_ld16(lane_base + T_G2 + q * 16, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int h = q * 16 + i;
+                const float d = (m2[h >> 5] >> (h & 31)) & 1u ? v[i] : 0.0f;
+                st_bf16(sm, S.dz2 + kmaj(t, h, HID), act ? d : 0.0f);
+                st_bf16(sm, S.aw + kmaj(h, t, KW), act ? d : 0.0f);
+            }
+        }
+        // dh1 = dz2 W2 (B = W2^T [64][64])
+        if (!(ok = run([&] { gemm(tm + T_G1, base + S.dz2, base + S.w2t, HID, HID, false); }))) break;
+#pragma unroll
+        for (int q = 0; q < HID / 16; ++q) {
+            float v[16];
+            tmem_ld16(lane_base + T_G1 + q * 16, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int h = q * 16 + i;
+                const float d = (m1[h >> 5] >> (h & 31)) & 1u ? v[i] : 0.0f;
+                st_bf16(sm, S.aw + kmaj(HID + h, t, KW), act ? d : 0.0f);
+            }
+        }
+        // weight gradients over this tile's cells (K = the 128 cells)
+        const bool acc_w = wacc;
+        if (!(ok = run([&] {
+                  gemm(tm + T_WA, base + S.aw, base + S.bw, KW, 96, acc_w);
+                  gemm(tm + T_WB, base + S.h2t, base + S.doT, KW, NO, acc_w);
+              })))
+            break;
+        wacc = true;
+    }
+
+    if (TRAIN && ok && wacc) {
+        // lanes 0-63: dW2 (columns 0-79 of WA); lanes 64-127: dW1 (columns 80-95)
+        if (t < HID) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                float v[16];
+                tmem_ld16(lane_base + T_WA + q * 16, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) atomicAdd(&a.grad[G_W2 + t * K2 + q * 16 + i], v[i]);
+            }
+        } else {
+            float v[16];
+            tmem_ld16(lane_base + T_WA + 80, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) atomicAdd(&a.grad[G_W1 + (t - HID) * K1 + i], v[i]);
+        }
+        // dW3^T: lane h (< 80) holds dW3[o][h] in column o
+        {
+            float v[16];
+            tmem_ld16(lane_base + T_WB, v);
+            tmem_wait_ld();
+            if (t < K2) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) atomicAdd(&a.grad[G_W3 + i * K2 + t], v[i]);
+            }
+        }
+    }
+    if (TRAIN) {
+        double* red = reinterpret_cast<double*>(sm + S.loss);
+        red[t] = loss_acc;
+        __syncthreads();
+        if (t == 0) {
+            double sum = 0.0;
+            for (int i = 0; i < TM; ++i) sum += red[i];
+            atomicAdd(a.loss, sum);
+        }
+    }
+    if (!ok && t == 0) atomicExch(a.status, 1);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (t < 32) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(ncols) : "memory");
+    }
+}
+
+}  // namespace mlp
+
+size_t mlp_smem_bytes(bool train) { return mlp::plan(train).total; }
+
+int run_mlp_sweep(bool train, const float* in, const float* target, float* out, int64_t n_outer, int64_t n_line,
+                  int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W,
+                  const float* alpha, const void* net, float* grad, double* loss, double inv_scale, int* status,
+                  cudaStream_t st) {
+    mlp::SweepArgs a{};
+    a.in = in;
+    a.target = target;
+    a.out = out;
+    a.n_outer = n_outer;
+    a.n_inner = n_inner;
+    a.n_line = (int)n_line;
+    a.sel_div = sel_div;
+    a.sel_mod = (int)sel_mod;
+    a.shift = shift;
+    a.W = W;
+    a.alpha = alpha;
+    a.net = static_cast<const __nv_bfloat16*>(net);
+    a.grad = grad;
+    a.loss = loss;
+    a.inv_scale = (float)inv_scale;
+    a.tiles = n_outer * n_line * ((n_inner + mlp::TM - 1) / mlp::TM);
+    a.status = status;
+    // inference asks for at least 100 KB so that no more than two CTAs (2 x 256
+    // tensor-memory columns) share an SM
+    const size_t smem = train ? mlp_smem_bytes(true) : std::max<size_t>(mlp_smem_bytes(false), 100 * 1024);
+    auto kern = train ? mlp::k_mlp_sweep<true> : mlp::k_mlp_sweep<false>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return set_cuda_error("cudaFuncSetAttribute(k_mlp_sweep)");
+    // training holds all 512 tensor-memory columns: one CTA per SM;
+    // inference holds 256: two CTAs per SM
+    const int64_t per_sm = train ? 1 : 2;
+    const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)sm_count() * per_sm);
+    kern<<<(unsigned)std::max<int64_t>(grid, 1), mlp::TM, smem, st>>>(a);
+    return check_launch("k_mlp_sweep");
+}
+
+int mlp_net_elems() { return mlp::NET_ELEMS; }
+int mlp_grad_elems() { return mlp::GRAD_ELEMS; }
+
+}  // namespace vp
+
+using namespace vp;
+
+extern "C" {
+
+static int mlp_check(const float* in, const void* net, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                     int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha,
+                     const int32_t* status, const char* who) {
+    if (!in || !net || !shift || !W || !alpha || !status) return set_error(VP_ERR_ARG, who);
+    if (n_outer <= 0 || n_line <= 0 || n_inner <= 0 || sel_div <= 0 || sel_mod <= 0 || n_line >= (1 << 30))
+        return set_error(VP_ERR_ARG, "vp_mlp: bad size");
+    return VP_OK;
+}
+
+int vp_mlp_drift(const float* f_in, float* f_out, int64_t n_outer, int64_t n_line, int64_t n_inner, int64_t sel_div,
+                 int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha, const void* net,
+                 int32_t* status, void* stream) {
+    int rc = mlp_check(f_in, net, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha, status,
+                       "vp_mlp_drift: null pointer");
+    if (rc) return rc;
+    if (!f_out || f_out == f_in) return set_error(VP_ERR_ARG, "vp_mlp_drift: f_out null or aliasing f_in");
+    return run_mlp_sweep(false, f_in, nullptr, f_out, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha,
+                         net, nullptr, nullptr, 1.0, reinterpret_cast<int*>(status), static_cast<cudaStream_t>(stream));
+}
+
+int vp_mlp_train(const float* f_in, const float* target, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                 int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha,
+                 const void* net, double inv_scale, float* grad, double* loss, int32_t* status, void* stream) {
+    int rc = mlp_check(f_in, net, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha, status,
+                       "vp_mlp_train: null pointer");
+    if (rc) return rc;
+    if (!target || !grad || !loss) return set_error(VP_ERR_ARG, "vp_mlp_train: null target, grad or loss");
+    return run_mlp_sweep(true, f_in, target, nullptr, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha,
+                         net, grad, loss, inv_scale, reinterpret_cast<int*>(status), static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

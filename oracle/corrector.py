@@ -1,0 +1,117 @@
+"""CPU restatement of the learned drift correction (test infrastructure: the
+checker of the tensor-core kernels vp_mlp_drift / vp_mlp_train, never part
+of the product path).
+
+The network and its use follow the kernel's specification (no reference
+counterpart: the reference interpolates with plain Lagrange weights,
+vlasov2D2V.py:210-285, and this corrects those weights):
+  x  = [bf16(f_k * (1/s)) for k < 6, bf16(alpha - 1/2), 1, 0 x 8],  s = max|f_k|
+  z1 = W1 x,            h1 = bf16(relu(z1))
+  z2 = W2 [h1, 1, 0],   h2 = bf16(relu(z2))
+  o  = W3 [h2, 1, 0]
+  y  = sum_k (w_k + o_k - mean(o_0..5)) f_k
+BF16 values are rounded to nearest even exactly as the device does; the
+matrix products are summed in float64 here (FP32 on the device), so the two
+agree to accumulation round-off, not bit for bit.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+HID, K1, K2, NO = 64, 16, 80, 16
+
+
+def bf16(x) -> np.ndarray:
+    """Round float32 values to the nearest bfloat16 (ties to even), as float32."""
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    u = a.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).reshape(a.shape)
+
+
+def bf16_bits(x) -> np.ndarray:
+    """bfloat16 bit patterns (uint16) of float32 values, ties to even."""
+    return (bf16(x).view(np.uint32) >> 16).astype(np.uint16)
+
+
+def pack_net(W1: np.ndarray, W2: np.ndarray, W3: np.ndarray) -> np.ndarray:
+    """The packed bf16 network of vp_mlp_*: W1, W2, W3, W3T, W2T (uint16 bits)."""
+    W1 = np.asarray(W1, np.float32).reshape(HID, K1)
+    W2 = np.asarray(W2, np.float32).reshape(HID, K2)
+    W3 = np.asarray(W3, np.float32).reshape(NO, K2)
+    W3T = np.ascontiguousarray(W3[:, :HID].T)  # [64][16]
+    W2T = np.ascontiguousarray(W2[:, :HID].T)  # [64][64]
+    return np.concatenate([bf16_bits(m).reshape(-1) for m in (W1, W2, W3, W3T, W2T)])
+
+
+def stencil(f: np.ndarray, shift: np.ndarray, axis: int, vel_axis: int):
+    """f_k (k = 0..5) of every cell of a periodic drift along axis, with the
+    table column j of each cell given by its index along vel_axis:
+    f_k = f[..., (l - s_j - (k - 2)) mod n, ...]. Returns (F [6, ...], j index array)."""
+    n = f.shape[axis]
+    idx = np.arange(n)
+    shp = [1] * f.ndim
+    shp[vel_axis] = f.shape[vel_axis]
+    s = np.asarray(shift).reshape(shp)
+    F = []
+    for k in range(6):
+        src = (idx.reshape([-1 if d == axis else 1 for d in range(f.ndim)]) - s - (k - 2)) % n
+        F.append(np.take_along_axis(f, np.broadcast_to(src, f.shape), axis=axis))
+    jj = np.broadcast_to(np.arange(f.shape[vel_axis]).reshape(shp), f.shape)
+    return np.stack(F), jj
+
+
+def forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3):
+    """Corrected drift of f (float32) and the intermediates of every cell."""
+    f = np.asarray(f, np.float32)
+    F, jj = stencil(f, shift, axis, vel_axis)
+    F = F.reshape(6, -1).T  # [cells][6]
+    j = jj.reshape(-1)
+    w = np.asarray(W, np.float32)[:, j].T  # [cells][6]
+    al = np.asarray(alpha, np.float32)[j]
+    s = np.abs(F).max(axis=1)
+    inv = np.where(s > 0, np.float32(1.0) / np.where(s > 0, s, 1).astype(np.float32), np.float32(0.0))
+    inv = inv.astype(np.float32)
+    N = F.shape[0]
+    x = np.zeros((N, K1), np.float32)
+    x[:, :6] = bf16(F * inv[:, None])
+    x[:, 6] = bf16(al - np.float32(0.5))
+    x[:, 7] = 1.0
+    W1b, W2b, W3b = bf16(W1).reshape(HID, K1), bf16(W2).reshape(HID, K2), bf16(W3).reshape(NO, K2)
+    z1 = x.astype(np.float64) @ W1b.T.astype(np.float64)
+    h1 = np.zeros((N, K2), np.float32)
+    h1[:, :HID] = bf16(np.maximum(z1, 0).astype(np.float32))
+    h1[:, HID] = 1.0
+    z2 = h1.astype(np.float64) @ W2b.T.astype(np.float64)
+    h2 = np.zeros((N, K2), np.float32)
+    h2[:, :HID] = bf16(np.maximum(z2, 0).astype(np.float32))
+    h2[:, HID] = 1.0
+    o = (h2.astype(np.float64) @ W3b.T.astype(np.float64)).astype(np.float32)
+    mean = o[:, :6].sum(axis=1, dtype=np.float32) * np.float32(1.0 / 6.0)
+    y = np.zeros(N, np.float32)
+    for k in range(6):  # fused multiply-add: exact product, one rounding
+        a = (w[:, k] + (o[:, k] - mean)).astype(np.float32)
+        y = (a.astype(np.float64) * F[:, k].astype(np.float64) + y.astype(np.float64)).astype(np.float32)
+    cache = dict(F=F, x=x, z1=z1, h1=h1, z2=z2, h2=h2, o=o, W1b=W1b, W2b=W2b, W3b=W3b)
+    return y.reshape(f.shape), cache
+
+
+def train_grad(f, target, shift, W, alpha, axis, vel_axis, W1, W2, W3, inv_scale):
+    """(sum r^2, dW1, dW2, dW3) of r = (y - target) * inv_scale."""
+    y, c = forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3)
+    r = ((y.reshape(-1) - np.asarray(target, np.float32).reshape(-1)) * np.float32(inv_scale)).astype(np.float32)
+    loss = float(np.sum(r.astype(np.float64) ** 2))
+    gy = (np.float32(2.0) * r * np.float32(inv_scale)).astype(np.float32)
+    g = gy[:, None] * c["F"]
+    gm = g.sum(axis=1, dtype=np.float32) * np.float32(1.0 / 6.0)
+    N = g.shape[0]
+    do = np.zeros((N, NO), np.float32)
+    do[:, :6] = bf16(g - gm[:, None])
+    dh2 = do.astype(np.float64) @ c["W3b"][:, :HID].astype(np.float64)
+    dz2 = bf16(np.where(c["z2"] > 0, dh2, 0).astype(np.float32))
+    dh1 = dz2.astype(np.float64) @ c["W2b"][:, :HID].astype(np.float64)
+    dz1 = bf16(np.where(c["z1"] > 0, dh1, 0).astype(np.float32))
+    dW1 = dz1.T.astype(np.float64) @ c["x"].astype(np.float64)
+    dW2 = dz2.T.astype(np.float64) @ c["h1"].astype(np.float64)
+    dW3 = do.T.astype(np.float64) @ c["h2"].astype(np.float64)
+    return loss, dW1, dW2, dW3

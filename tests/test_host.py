@@ -153,3 +153,16 @@ def test_autotune_cache_keys(vp, tmp_path):
     t = at.cached_tiles(shapes, torch.float32, cache=at.load_cache(str(path)))
     assert t["block"] == [128, 256, 128] and t["ctas_per_sm"] == [1, 2, 2]
     assert t["run_segments"] == [(1, 1), (1, 2), (1, 1)]
+
+
+def test_corrector_packing_matches_oracle(vp):
+    """The packed BF16 network (W1, W2, W3, W3T, W2T) has the layout the
+    kernels and the oracle use."""
+    C = importlib.import_module(PACKAGE + ".corrector")
+    from oracle import corrector as OC
+
+    net = C.Corrector("cpu", seed=5, out_scale=0.1)
+    bits = net.net.view(torch.int16).numpy().view(np.uint16)
+    ref = OC.pack_net(net.W1.numpy(), net.W2.numpy(), net.W3.numpy())
+    np.testing.assert_array_equal(bits, ref)
+    assert bits.size == C.NET_ELEMS
