@@ -53,6 +53,10 @@ WORKLOADS = {
            "2D2V two-stream 64^4, eps=0.001, k=0.2, v0=2.4, v in [-8,8], dt=0.05"),
     "oned": ("1d", (4096, 4096), 4 * math.pi, 5.0, 0.05, "landau", (0.001, 0.5), "float32",
              "1D1V Landau 4096x4096, eps=0.001, k=0.5, v in [-5,5], dt=0.05"),
+    "c5": ("learned", (32, 32, 32, 32), 4 * math.pi, 6.0, 0.1, None, None, "float32",
+           "learned kick correction on a 32^4 grid (L = 4 pi, v in [-6,6], dt = 0.1): trained on seeded "
+           "coarse / 2x-refined pairs of Landau and two-stream runs, evaluated on held-out seeds against plain 32^4 "
+           "and plain 2x-refined runs, errors against a 4x-refined run"),
     "c4": ("batch", None, None, None, 0.05, None, None, "float32",
            "64 independent 2D2V runs of uneven size (seed 20261203: Nx=Ny in {16,24,32,48,64}, Nvx=Nvy in "
            "{32,48,64}, eps~U[0.001,0.05], k~U[0.3,1], v0~U[0,3], Landau or two-stream), dt=0.05"),
@@ -72,13 +76,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
+    ap.add_argument("--train-ics", type=int, default=125, help="learned workload: training initial conditions")
+    ap.add_argument("--train-iters", type=int, default=1500, help="learned workload: Adam steps")
+    ap.add_argument("--eval-ics", type=int, default=4, help="learned workload: held-out initial conditions")
     ap.add_argument("--tiles", choices=["default", "auto", "tune"], default="auto",
                     help="batched workload: default tile shapes, the autotuner's cache, or tune now")
     a = ap.parse_args()
     wl = WORKLOADS[a.workload]
     a.kind, a.grid, a.L, a.vmax, a.dt, a.ic, a.icp, dflt, a.desc = wl
     a.dtype = a.dtype or dflt
-    if a.kind == "batch" and a.size:
+    if a.kind in ("batch", "learned") and a.size:
         raise SystemExit("--size does not apply to the batched workload")
     if a.size:
         if a.kind != "2d":
@@ -714,8 +721,168 @@ def run_batch(a):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the learned corrector: training on coarse / refined pairs, held-out runs
+# ---------------------------------------------------------------------------
+def run_learned(a):
+    import torch
+
+    vp = importlib.import_module("jax-pytorch-vlasov_b200")
+    C = vp.corrector
+    L = vp._lib
+    rank, local, world = importlib.import_module("jax-pytorch-vlasov_b200.dist").init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N, _, Nv, _ = a.grid
+    Lb, V, dt = a.L, a.vmax, a.dt
+    K = max(a.steps, 10)
+    # the plain 2x-refined run and the 4x-refined truth (the nested grids with
+    # Nv = 2 Nv - 1 only serve the training pairs)
+    fine_shape = (2 * N, 2 * N, 2 * Nv, 2 * Nv)
+    truth_shape = (4 * N, 4 * N, 4 * Nv, 4 * Nv)
+
+    def stepper(shape):
+        return vp.Stepper2D(*shape, Lb, Lb, V, V, dt, dtype=torch.float32, device=dev, window=-1, diagnostics=1,
+                            precise_tables=True)
+
+    with ClockSampler(local) as clk:
+        # training pairs: seeded initial conditions, 8 snapshots of the refined run each, two kicks per snapshot
+        t0 = time.perf_counter()
+        src = C.PairSource(N, N, Nv, Nv, Lb, Lb, V, V, dt, device=dev)
+        rng = np.random.default_rng(20261203)
+        ics = [C.draw_ic(rng, Lb) for _ in range(a.train_ics)]
+        pairs = C.collect_kick_pairs(src, ics, tuple(range(10, 81, 10)), Lb, V)
+        torch.cuda.synchronize(dev)
+        t_pairs = time.perf_counter() - t0
+        net = C.Corrector(dev, seed=0)
+        t0 = time.perf_counter()
+        losses = C.train_kicks(net, pairs, src.coarse, iters=a.train_iters, batch=16, lr=1e-3)
+        w3_scale = net.w3_scale
+        torch.cuda.synchronize(dev)
+        t_train = time.perf_counter() - t0
+        cells_trained = a.train_iters * 16 * math.prod(a.grid)
+        del pairs
+        # held-out runs: E-energy histories against the 4x-refined run
+        erng = np.random.default_rng(20261204)
+        eval_ics = [C.draw_ic(erng, Lb) for _ in range(a.eval_ics)]
+        coarse, fine, truth = stepper(a.grid), stepper(fine_shape), stepper(truth_shape)
+        learned = C.LearnedStepper2D(net, N, N, Nv, Nv, Lb, Lb, V, V, dt, device=dev)
+        zero = C.LearnedStepper2D(C.Corrector(dev), N, N, Nv, Nv, Lb, Lb, V, V, dt, device=dev)
+        res = []
+        for ic in eval_ics:
+            hist = {}
+            for name, st, shape in (("truth", truth, truth_shape), ("plain_coarse", coarse, a.grid),
+                                    ("plain_refined", fine, fine_shape)):
+                h = torch.zeros((K, L.DIAG_COUNT), dtype=torch.float64, device=dev)
+                st.run(C.initial(ic, shape, Lb, V, dev), K, history=h, graph=True)
+                hist[name] = h[:, :2].cpu().numpy()
+            for name, st in (("learned_coarse", learned), ("plain_coarse_separate_kicks", zero)):
+                h = torch.zeros((K, 2), dtype=torch.float64, device=dev)
+                st.run(C.initial(ic, a.grid, Lb, V, dev), K, history=h, graph=True)
+                hist[name] = h.cpu().numpy()
+            ref = hist["truth"][:, 0]
+            t = dt * np.arange(1, K + 1)
+            row = {"ic": ic}
+            for name, h in hist.items():
+                we = h[:, 0]
+                row[name] = {"we_err": float(np.abs(we - ref).max() / np.abs(ref).max()),
+                             "we_err_rms_log": float(np.sqrt(np.mean(np.log(np.maximum(we, 1e-300) / ref) ** 2))),
+                             "rate": float(np.polyfit(t, 0.5 * np.log(np.maximum(we, 1e-300)), 1)[0]),
+                             "mass_drift": float(h[-1, 1] / h[0, 1] - 1)}
+            res.append(row)
+        # device time per step, graph-replayed, after warm-up
+        def timed(run, steps):
+            run(steps)  # captures the graphs of this buffer
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run(steps)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            return e0.elapsed_time(e1) / steps
+
+        f_c = C.initial(eval_ics[0], a.grid, Lb, V, dev)
+        f_f = C.initial(eval_ics[0], fine_shape, Lb, V, dev)
+        ms = {"plain_coarse": timed(lambda k: coarse.run(f_c, k, graph=True), K),
+              "learned_coarse": timed(lambda k: learned.run(f_c, k, graph=True), K),
+              "plain_refined": timed(lambda k: fine.run(f_f, k, graph=True), K)}
+        # the corrected kick alone (tensor-core roofline)
+        Ex = coarse.ex
+        out = torch.empty_like(f_c)
+        net.kick(f_c, Ex, 2, dt, coarse.dvx, out=out)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record()
+        for _ in range(reps):
+            net.kick(f_c, Ex, 2, dt, coarse.dvx, out=out)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        kick_ms = e0.elapsed_time(e1) / reps
+        c0 = L.load().vp_launch_count()
+        learned.step(f_c, out)
+        launches_per_step = L.load().vp_launch_count() - c0
+        torch.cuda.synchronize(dev)
+        net.check()
+
+    def mean(key, field):
+        return float(np.mean([r[key][field] for r in res]))
+
+    err = {k: mean(k, "we_err") for k in ("plain_coarse", "learned_coarse", "plain_refined",
+                                           "plain_coarse_separate_kicks")}
+    err_log = {k: mean(k, "we_err_rms_log") for k in ("plain_coarse", "learned_coarse", "plain_refined")}
+    rate_err = {k: float(np.mean([abs(r[k]["rate"] - r["truth"]["rate"]) for r in res]))
+                for k in ("plain_coarse", "learned_coarse", "plain_refined")}
+    ratio = ms["learned_coarse"] / ms["plain_refined"]
+    flops_cell = 2 * (16 * 64 + 80 * 64 + 80 * 16)  # one forward pass, padded shapes
+    achieved = flops_cell * math.prod(a.grid) / (kick_ms * 1e-3) / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak, pk = float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, pk = 1590.0, "fallback"
+    if rank == 0:
+        line = {
+            "metric": "wall time per step, learned 32^4 / plain 2x-refined (lower is better; meaningful where "
+                      "the learned E-energy error reaches the refined run's)",
+            "value": ratio, "unit": "ratio", "n_gpus": world, "steps": K, "warmup": 4,
+            "ms_per_step": ms["learned_coarse"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 state, bf16 network (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": a.desc, "grid": list(a.grid), "refined_grid": list(fine_shape),
+                       "truth_grid": list(truth_shape), "pair_grid": [2 * N, 2 * N, 2 * Nv - 1, 2 * Nv - 1],
+                       "train_ics": a.train_ics, "train_pairs": 16 * a.train_ics,
+                       "train_iters": a.train_iters, "batch_pairs": 16, "eval_ics": a.eval_ics,
+                       "steps_per_eval_run": K},
+            "errors_we_vs_truth": err, "errors_rms_log_we_vs_truth": err_log, "rate_error_vs_truth": rate_err,
+            "learned_reaches_refined_error": bool(err["learned_coarse"] <= err["plain_refined"]),
+            "learned_improves_on_plain_coarse": bool(err["learned_coarse"] < err["plain_coarse"]),
+            "ms_per_step_each": ms,
+            "training": {"pairs_s": t_pairs, "train_s": t_train, "loss_first": losses[0],
+                         "loss_last_20_mean": float(np.mean(losses[-20:])), "w3_scale": w3_scale,
+                         "cell_samples": cells_trained},
+            "eval_runs": res,
+            "roofline": {"bound": "tensor", "kernel": "corrected kick (forward network per cell)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_kind": pk, "traffic": None, "kick_ms": kick_ms,
+                         "flops_per_launch": flops_cell * math.prod(a.grid)},
+            "gpu_launches": int(launches_per_step * K),
+            "e2e": None, "cpu_baseline": None,
+        }
+        clk_s = clk.summary()
+        if clk_s:
+            line["clocks"] = clk_s
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.kind == "learned":
+        if a.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned interpolation "
+                              "corrector (its interpolation is plain Lagrange only)"}), flush=True)
+            return 0
+        return run_learned(a)
     if a.kind == "batch":
         return run_batch_reference(a) if a.impl == "reference" else run_batch(a)
     if a.impl == "reference":

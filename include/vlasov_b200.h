@@ -342,9 +342,10 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
  * all runs (VP_PHASE_DRIFT_Y1 includes the rho finalize), NULL to skip. */
 int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void* const* events, void* stream);
 
-/* ---- learned drift correction (BF16 tensor cores) ------------------------
+/* ---- learned interpolation correction (BF16 tensor cores) ----------------
  * No reference counterpart. A per-cell network corrects the 6 Lagrange
- * weights of a periodic drift (the sweep of vp_drift, FP32 storage):
+ * weights of a periodic drift (the sweep of vp_drift, FP32 storage) or of a
+ * kick (the sweep of vp_kick with the exact window):
  *   x  = [f_k / max|f| (k < 6), alpha - 1/2, 1, 0...]  (16 inputs)
  *   h1 = relu(W1 x), h2 = relu(W2 [h1, 1, 0...]), o = W3 [h2, 1, 0...]
  *   out = sum_k (W[k][j] + o_k - mean(o_0..o_5)) f_k
@@ -370,6 +371,17 @@ int vp_mlp_train(const float* f_in, const float* target, int64_t n_outer, int64_
                  int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift,
                  const float* W, const float* alpha, const void* net, double inv_scale, float* grad,
                  double* loss, int32_t* status, void* stream);
+/* The same correction applied to the kick of vp_kick (window < 0): row o of
+ * [n_outer][n_line][n_inner] moves by E[o / e_div] * dt / dv cells, zero
+ * outside the line; the shift, the fraction alpha and the plain weights are
+ * those of vp_kick. */
+int vp_mlp_kick(const float* f_in, float* f_out, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                const double* E, int64_t e_div, double dt, double dv, const void* net, int32_t* status,
+                void* stream);
+int vp_mlp_train_kick(const float* f_in, const float* target, int64_t n_outer, int64_t n_line,
+                      int64_t n_inner, const double* E, int64_t e_div, double dt, double dv,
+                      const void* net, double inv_scale, float* grad, double* loss, int32_t* status,
+                      void* stream);
 
 #ifdef __cplusplus
 }

@@ -116,6 +116,8 @@ SIGNATURES = {
     "vp_batch2d_step": (ctypes.c_int, [P, P, I32, P, P]),
     "vp_mlp_drift": (ctypes.c_int, [P, P, I64, I64, I64, I64, I64, P, P, P, P, P, P]),
     "vp_mlp_train": (ctypes.c_int, [P, P, I64, I64, I64, I64, I64, P, P, P, P, D, P, P, P, P]),
+    "vp_mlp_kick": (ctypes.c_int, [P, P, I64, I64, I64, P, I64, D, D, P, P, P]),
+    "vp_mlp_train_kick": (ctypes.c_int, [P, P, I64, I64, I64, P, I64, D, D, P, D, P, P, P, P]),
     "vp_step2d_workspace_bytes": (SZ, [I64, I64, I64, I64]),
     "vp_step1d": (ctypes.c_int, [ctypes.POINTER(Step1dDesc), P]),
     "vp_step1d_workspace_bytes": (SZ, [I64, I64]),

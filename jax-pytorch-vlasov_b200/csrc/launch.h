@@ -170,10 +170,8 @@ int launch_kick2d_batch(int dtype, int vec, const Kick2dArgs* runs, const int64_
 size_t mlp_smem_bytes(bool train);
 int mlp_net_elems();
 int mlp_grad_elems();
-int run_mlp_sweep(bool train, const float* in, const float* target, float* out, int64_t n_outer, int64_t n_line,
-                  int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W,
-                  const float* alpha, const void* net, float* grad, double* loss, double inv_scale, int* status,
-                  cudaStream_t st);
+struct MlpSweepArgs;
+int run_mlp_sweep(bool train, bool kick, const MlpSweepArgs& args, cudaStream_t st);
 
 // poisson.cu
 size_t poisson2d_ws_bytes(int64_t nx, int64_t ny);

@@ -1,7 +1,9 @@
 // Learned correction of the drift interpolation weights on tensor cores.
 //
 // A per-cell network proposes a correction dw to the 6 Lagrange weights of
-// a periodic drift (the x / y sweeps of the 2D2V step):
+// a sweep: a periodic drift (x / y, shift and weights from the drift table)
+// or a Dirichlet kick (vx / vy, shift and weights from the plane's field E,
+// the arithmetic of the plain kick):
 //   x  = [f_k / s (k < 6), alpha - 1/2, 1, 0 x 8]          s = max_k |f_k|
 //   h1 = relu(W1 x)            W1: [64][16]  (column 7 = bias)
 //   h2 = relu(W2 [h1, 1, 0])   W2: [64][80]  (column 64 = bias)
@@ -11,8 +13,11 @@
 // x, h1, h2 and the weights are BF16 operands of tcgen05.mma (kind::f16,
 // FP32 accumulators in tensor memory); dw and the output are FP32.
 //
-// One CTA of 128 threads owns one tile of 128 cells (the MMA M) at a time,
-// thread t <-> cell t <-> accumulator lane t. Every operand lives in shared
+// Each tile is 128 consecutive cells of the flattened
+// [n_outer][n_line][n_inner] array (the MMA M), thread <-> cell <->
+// accumulator lane; an inference CTA of 256 threads runs two tiles per MMA
+// round trip (tensor-memory columns 0-127 and 128-255), a training CTA of
+// 128 threads one. Every operand lives in shared
 // memory in the canonical K-major layout without swizzle (8 x 16-byte core
 // matrices, K chunks 128 bytes apart, 8-row groups (K/8)*128 bytes apart).
 // A single thread issues the MMAs; completion is signalled through one
@@ -41,7 +46,12 @@
 namespace vp {
 namespace mlp {
 
-constexpr int TM = 128;  // cells per tile = MMA M = threads per CTA
+constexpr int TM = 128;  // cells per tile = MMA M
+// tiles per CTA: inference keeps two tiles (256 threads) in each MMA round
+// trip, training one (its tensor memory holds the weight gradients)
+__host__ __device__ constexpr int subtiles(bool train) { return train ? 1 : 2; }
+constexpr int XS = TM * 16 * 2;  // bytes of one tile's layer-1 input [TM][16]
+constexpr int HS = TM * 80 * 2;  // bytes of one tile's hidden layer [TM][80]
 constexpr int K1 = 16;   // layer-1 input width
 constexpr int HID = 64;  // hidden width
 constexpr int K2 = 80;   // hidden + constant + zero pad
@@ -172,15 +182,16 @@ __host__ __device__ constexpr Smem plan(bool train) {
         o += al128(b);
         return r;
     };
-    s.x = take(TM * K1 * 2);
-    s.h1 = take(TM * K2 * 2);
-    s.h2 = take(TM * K2 * 2);
+    const uint32_t sub = (uint32_t)subtiles(train);
+    s.x = take(sub * XS);
+    s.h1 = take(sub * HS);
+    s.h2 = take(sub * HS);
     s.w1 = take(HID * K1 * 2);
     s.w2 = take(HID * K2 * 2);
     s.w3 = take(NO * K2 * 2);
-    s.w3t = take(HID * NO * 2);
-    s.w2t = take(HID * HID * 2);
     if (train) {
+        s.w3t = take(HID * NO * 2);
+        s.w2t = take(HID * HID * 2);
         s.dO = take(TM * NO * 2);    // [cell][16]   A of dh2
         s.dz2 = take(TM * HID * 2);  // [cell][64]   A of dh1
         s.aw = take(128 * KW * 2);   // [dz2^T; dz1^T] [128][cells]
@@ -190,7 +201,7 @@ __host__ __device__ constexpr Smem plan(bool train) {
     }
     s.bar = take(8);
     s.tslot = take(4);
-    s.loss = take(TM * 8);
+    s.loss = take(sub * TM * 8);
     s.total = o;
     return s;
 }
@@ -201,24 +212,34 @@ constexpr uint32_t T_G2 = 160, T_G1 = 224;           // backward deltas
 constexpr uint32_t T_WA = 288, T_WB = 384;           // [dW2 | dW1] (96), dW3^T (16)
 constexpr uint32_t TMEM_TRAIN = 512, TMEM_INFER = 256;
 
-struct SweepArgs {
+}  // namespace mlp
+
+struct MlpSweepArgs {
     const float* in;
     const float* target;  // training only
     float* out;           // inference only
     int64_t n_outer, n_inner;
     int n_line;
+    // drift: table column j = (c / sel_div) % sel_mod
     int64_t sel_div;
     int sel_mod;
     const int32_t* shift;
     const float* W;      // [6][sel_mod] Lagrange weights
     const float* alpha;  // [sel_mod] fractional shifts
+    // kick: field E[o / e_div], shift (E dt) / dv
+    const double* E;
+    int64_t e_div;
+    double dt, dv;
     const __nv_bfloat16* net;
     float* grad;      // training: [GRAD_ELEMS]
     double* loss;     // training: sum of r^2
     float inv_scale;  // training: residual scale
-    int64_t tiles;    // n_outer * n_line * ceil(n_inner / TM)
+    int64_t cells;    // n_outer * n_line * n_inner
     int* status;
 };
+
+namespace mlp {
+using SweepArgs = MlpSweepArgs;
 
 // copy a row-major [R][K] bf16 matrix from global into the K-major layout
 __device__ void load_matrix(unsigned char* sm, uint32_t dst, const __nv_bfloat16* src, int R, int K) {
@@ -228,18 +249,24 @@ __device__ void load_matrix(unsigned char* sm, uint32_t dst, const __nv_bfloat16
     }
 }
 
-template <bool TRAIN>
-__global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ SweepArgs a) {
+template <bool TRAIN, bool KICK>
+__global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __grid_constant__ SweepArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     constexpr Smem S = plan(TRAIN);
+    constexpr int SUB = subtiles(TRAIN);
+    constexpr int NT = TM * SUB;
+    constexpr uint32_t TD3 = TRAIN ? T_D3 : T_D1;  // inference: layer 3 reuses layer 1's columns
     const int t = threadIdx.x;
+    const int u = t / TM;        // this thread's tile of the CTA
+    const int tl = t % TM;       // its cell (row) within the tile
+    const uint32_t ux = (uint32_t)u * XS, uh = (uint32_t)u * HS;
     const uint32_t base = smem_u32(sm);
     const uint32_t bar = base + S.bar;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + S.tslot);
     const uint32_t ncols = TRAIN ? TMEM_TRAIN : TMEM_INFER;
 
     // zero every operand buffer once: padding rows / columns stay zero
-    for (uint32_t i = t * 16; i < S.bar; i += TM * 16) *reinterpret_cast<uint4*>(sm + i) = make_uint4(0, 0, 0, 0);
+    for (uint32_t i = t * 16; i < S.bar; i += NT * 16) *reinterpret_cast<uint4*>(sm + i) = make_uint4(0, 0, 0, 0);
     __syncthreads();
     load_matrix(sm, S.w1, a.net + OFF_W1, HID, K1);
     load_matrix(sm, S.w2, a.net + OFF_W2, HID, K2);
@@ -249,9 +276,9 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
         load_matrix(sm, S.w2t, a.net + OFF_W2T, HID, HID);
     }
     // constant-one columns of the layer inputs (bias columns)
-    st_bf16(sm, S.x + kmaj(t, 7, K1), 1.0f);
-    st_bf16(sm, S.h1 + kmaj(t, HID, K2), 1.0f);
-    st_bf16(sm, S.h2 + kmaj(t, HID, K2), 1.0f);
+    st_bf16(sm, S.x + ux + kmaj(tl, 7, K1), 1.0f);
+    st_bf16(sm, S.h1 + uh + kmaj(tl, HID, K2), 1.0f);
+    st_bf16(sm, S.h2 + uh + kmaj(tl, HID, K2), 1.0f);
     if (TRAIN) {
         // the transposed copies hold the constant rows: h1'^T row 64 and h2'^T row 64
         st_bf16(sm, S.bw + kmaj(HID, t, KW), 1.0f);
@@ -272,7 +299,8 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
     __syncthreads();
     fence_after();
     const uint32_t tm = *tslot;
-    const uint32_t lane_base = tm + ((uint32_t)(t & ~31) << 16);  // this warp's 32 lanes
+    // this warp's 32 lanes, in this tile's 128 columns
+    const uint32_t lane_base = tm + ((uint32_t)(tl & ~31) << 16) + (uint32_t)u * 128u;
     uint32_t phase = 0;
     bool ok = true;
     double loss_acc = 0.0;
@@ -295,30 +323,43 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
         return all;
     };
 
-    const int64_t cblocks = (a.n_inner + TM - 1) / TM;
-    for (int64_t tile = blockIdx.x; tile < a.tiles && ok; tile += gridDim.x) {
-        const int64_t cb = tile % cblocks;
-        const int64_t ol = tile / cblocks;
-        const int l = (int)(ol % a.n_line);
-        const int64_t o = ol / a.n_line;
-        const int64_t c = cb * TM + t;
-        const bool act = c < a.n_inner;
-        const int n = a.n_line;
-        // stencil of this cell: f_k = in[o, (l - s - (k - 2)) mod n, c]
+    const int64_t tiles = (a.cells + TM - 1) / TM;
+    const int n = a.n_line;
+    for (int64_t tile0 = (int64_t)blockIdx.x * SUB; tile0 < tiles && ok; tile0 += (int64_t)gridDim.x * SUB) {
+        const int64_t cell = (tile0 + u) * TM + tl;  // = (o * n + l) * n_inner + c
+        const bool act = cell < a.cells;
+        const int64_t c = act ? cell % a.n_inner : 0;
+        const int l = act ? (int)((cell / a.n_inner) % n) : 0;
+        const int64_t o = act ? cell / (a.n_inner * n) : 0;
+        // stencil of this cell: f_k = in[o, l - s - (k - 2), c], taken mod n
+        // (drift) or zero outside [0, n) (kick)
         float f[6], w[6];
         float al = 0.0f;
         if (act) {
-            const int j = (int)((c / a.sel_div) % a.sel_mod);
-            const int s = a.shift[j];
-            al = a.alpha[j];
-            int r = (int)(((int64_t)l - s + 2) % n);
-            if (r < 0) r += n;
             const float* col = a.in + (o * n) * a.n_inner + c;
+            if constexpr (KICK) {
+                const double e = a.E[o / a.e_div];
+                int s = kick_weights<double, float>(e, a.dt, a.dv, -1, w);
+                s = max(-(1 << 28), min(1 << 28, s));
+                const double d = e * a.dt / a.dv;
+                al = (float)(d - floor(d));
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                f[k] = col[(int64_t)r * a.n_inner];
-                w[k] = a.W[k * a.sel_mod + j];
-                r = r == 0 ? n - 1 : r - 1;
+                for (int k = 0; k < 6; ++k) {
+                    const int64_t r = (int64_t)l - s + 2 - k;
+                    f[k] = (r >= 0 && r < n) ? col[r * a.n_inner] : 0.0f;
+                }
+            } else {
+                const int j = (int)((c / a.sel_div) % a.sel_mod);
+                const int s = a.shift[j];
+                al = a.alpha[j];
+                int r = (int)(((int64_t)l - s + 2) % n);
+                if (r < 0) r += n;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    f[k] = col[(int64_t)r * a.n_inner];
+                    w[k] = a.W[k * a.sel_mod + j];
+                    r = r == 0 ? n - 1 : r - 1;
+                }
             }
         } else {
 #pragma unroll
@@ -329,8 +370,8 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
         for (int k = 0; k < 6; ++k) sc = fmaxf(sc, fabsf(f[k]));
         const float inv = sc > 0.0f ? 1.0f / sc : 0.0f;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) st_bf16(sm, S.x + kmaj(t, k, K1), f[k] * inv);
-        st_bf16(sm, S.x + kmaj(t, 6, K1), act ? al - 0.5f : 0.0f);
+        for (int k = 0; k < 6; ++k) st_bf16(sm, S.x + ux + kmaj(tl, k, K1), f[k] * inv);
+        st_bf16(sm, S.x + ux + kmaj(tl, 6, K1), act ? al - 0.5f : 0.0f);
         if (TRAIN) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) st_bf16(sm, S.bw + kmaj(K2 + k, t, KW), f[k] * inv);
@@ -338,7 +379,11 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
             st_bf16(sm, S.bw + kmaj(K2 + 7, t, KW), act ? 1.0f : 0.0f);
         }
         // layer 1
-        if (!(ok = run([&] { gemm(tm + T_D1, base + S.x, base + S.w1, K1, HID, false); }))) break;
+        if (!(ok = run([&] {
+                  for (int v = 0; v < SUB; ++v)
+                      gemm(tm + v * 128 + T_D1, base + S.x + v * XS, base + S.w1, K1, HID, false);
+              })))
+            break;
         uint32_t m1[2] = {0u, 0u}, m2[2] = {0u, 0u};  // relu masks of z1, z2
 #pragma unroll
         for (int q = 0; q < HID / 16; ++q) {
@@ -351,12 +396,16 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
                 const bool pos = v[i] > 0.0f;
                 if (pos) m1[h >> 5] |= 1u << (h & 31);
                 const float y = act && pos ? v[i] : 0.0f;
-                st_bf16(sm, S.h1 + kmaj(t, h, K2), y);
+                st_bf16(sm, S.h1 + uh + kmaj(tl, h, K2), y);
                 if (TRAIN) st_bf16(sm, S.bw + kmaj(h, t, KW), y);
             }
         }
         // layer 2
-        if (!(ok = run([&] { gemm(tm + T_D2, base + S.h1, base + S.w2, K2, HID, false); }))) break;
+        if (!(ok = run([&] {
+                  for (int v = 0; v < SUB; ++v)
+                      gemm(tm + v * 128 + T_D2, base + S.h1 + v * HS, base + S.w2, K2, HID, false);
+              })))
+            break;
 #pragma unroll
         for (int q = 0; q < HID / 16; ++q) {
             float v[16];
@@ -368,15 +417,19 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
                 const bool pos = v[i] > 0.0f;
                 if (pos) m2[h >> 5] |= 1u << (h & 31);
                 const float y = act && pos ? v[i] : 0.0f;
-                st_bf16(sm, S.h2 + kmaj(t, h, K2), y);
+                st_bf16(sm, S.h2 + uh + kmaj(tl, h, K2), y);
                 if (TRAIN) st_bf16(sm, S.h2t + kmaj(h, t, KW), y);
             }
         }
         if (TRAIN) st_bf16(sm, S.h2t + kmaj(HID, t, KW), act ? 1.0f : 0.0f);
         // layer 3
-        if (!(ok = run([&] { gemm(tm + T_D3, base + S.h2, base + S.w3, K2, NO, false); }))) break;
+        if (!(ok = run([&] {
+                  for (int v = 0; v < SUB; ++v)
+                      gemm(tm + v * 128 + TD3, base + S.h2 + v * HS, base + S.w3, K2, NO, false);
+              })))
+            break;
         float ov[16];
-        tmem_ld16(lane_base + T_D3, ov);
+        tmem_ld16(lane_base + TD3, ov);
         tmem_wait_ld();
         float mean = 0.0f;
 #pragma unroll
@@ -386,11 +439,11 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
 #pragma unroll
         for (int k = 0; k < 6; ++k) y = fmaf(w[k] + (ov[k] - mean), f[k], y);
         if (!TRAIN) {
-            if (act) a.out[(o * n + l) * a.n_inner + c] = y;
+            if (act) a.out[cell] = y;
             continue;
         }
         // ---- training: residual, deltas, weight gradients ----
-        const float tg = act ? a.target[(o * n + l) * a.n_inner + c] : 0.0f;
+        const float tg = act ? a.target[cell] : 0.0f;
         const float r = act ? (y - tg) * a.inv_scale : 0.0f;
         loss_acc += (double)r * r;
         const float gy = 2.0f * r * a.inv_scale;  // dL/dy
@@ -481,7 +534,7 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
         __syncthreads();
         if (t == 0) {
             double sum = 0.0;
-            for (int i = 0; i < TM; ++i) sum += red[i];
+            for (int i = 0; i < NT; ++i) sum += red[i];
             atomicAdd(a.loss, sum);
         }
     }
@@ -498,39 +551,23 @@ __global__ void __launch_bounds__(TM, 1) k_mlp_sweep(const __grid_constant__ Swe
 
 size_t mlp_smem_bytes(bool train) { return mlp::plan(train).total; }
 
-int run_mlp_sweep(bool train, const float* in, const float* target, float* out, int64_t n_outer, int64_t n_line,
-                  int64_t n_inner, int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W,
-                  const float* alpha, const void* net, float* grad, double* loss, double inv_scale, int* status,
-                  cudaStream_t st) {
-    mlp::SweepArgs a{};
-    a.in = in;
-    a.target = target;
-    a.out = out;
-    a.n_outer = n_outer;
-    a.n_inner = n_inner;
-    a.n_line = (int)n_line;
-    a.sel_div = sel_div;
-    a.sel_mod = (int)sel_mod;
-    a.shift = shift;
-    a.W = W;
-    a.alpha = alpha;
-    a.net = static_cast<const __nv_bfloat16*>(net);
-    a.grad = grad;
-    a.loss = loss;
-    a.inv_scale = (float)inv_scale;
-    a.tiles = n_outer * n_line * ((n_inner + mlp::TM - 1) / mlp::TM);
-    a.status = status;
+int run_mlp_sweep(bool train, bool kick, const MlpSweepArgs& args, cudaStream_t st) {
+    MlpSweepArgs a = args;
+    a.cells = a.n_outer * a.n_line * a.n_inner;
+    const int64_t tiles = (a.cells + mlp::TM - 1) / mlp::TM;
     // inference asks for at least 100 KB so that no more than two CTAs (2 x 256
     // tensor-memory columns) share an SM
     const size_t smem = train ? mlp_smem_bytes(true) : std::max<size_t>(mlp_smem_bytes(false), 100 * 1024);
-    auto kern = train ? mlp::k_mlp_sweep<true> : mlp::k_mlp_sweep<false>;
+    auto kern = train ? (kick ? mlp::k_mlp_sweep<true, true> : mlp::k_mlp_sweep<true, false>)
+                      : (kick ? mlp::k_mlp_sweep<false, true> : mlp::k_mlp_sweep<false, false>);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return set_cuda_error("cudaFuncSetAttribute(k_mlp_sweep)");
     // training holds all 512 tensor-memory columns: one CTA per SM;
     // inference holds 256: two CTAs per SM
     const int64_t per_sm = train ? 1 : 2;
-    const int64_t grid = std::min<int64_t>(a.tiles, (int64_t)sm_count() * per_sm);
-    kern<<<(unsigned)std::max<int64_t>(grid, 1), mlp::TM, smem, st>>>(a);
+    const int64_t sub = mlp::subtiles(train);
+    const int64_t grid = std::min<int64_t>((tiles + sub - 1) / sub, (int64_t)sm_count() * per_sm);
+    kern<<<(unsigned)std::max<int64_t>(grid, 1), mlp::TM * mlp::subtiles(train), smem, st>>>(a);
     return check_launch("k_mlp_sweep");
 }
 
@@ -543,35 +580,107 @@ using namespace vp;
 
 extern "C" {
 
-static int mlp_check(const float* in, const void* net, int64_t n_outer, int64_t n_line, int64_t n_inner,
-                     int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha,
-                     const int32_t* status, const char* who) {
-    if (!in || !net || !shift || !W || !alpha || !status) return set_error(VP_ERR_ARG, who);
-    if (n_outer <= 0 || n_line <= 0 || n_inner <= 0 || sel_div <= 0 || sel_mod <= 0 || n_line >= (1 << 30))
+static int mlp_sizes(int64_t n_outer, int64_t n_line, int64_t n_inner) {
+    if (n_outer <= 0 || n_line <= 0 || n_inner <= 0 || n_line >= (1 << 30) || n_outer * n_line * n_inner < 0)
         return set_error(VP_ERR_ARG, "vp_mlp: bad size");
     return VP_OK;
+}
+
+static MlpSweepArgs drift_args(const float* f_in, int64_t n_outer, int64_t n_line, int64_t n_inner, int64_t sel_div,
+                               int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha,
+                               const void* net, int32_t* status) {
+    MlpSweepArgs a{};
+    a.in = f_in;
+    a.n_outer = n_outer;
+    a.n_line = (int)n_line;
+    a.n_inner = n_inner;
+    a.sel_div = sel_div;
+    a.sel_mod = (int)sel_mod;
+    a.shift = shift;
+    a.W = W;
+    a.alpha = alpha;
+    a.e_div = 1;
+    a.dv = 1.0;
+    a.net = static_cast<const __nv_bfloat16*>(net);
+    a.inv_scale = 1.0f;
+    a.status = reinterpret_cast<int*>(status);
+    return a;
+}
+
+static MlpSweepArgs kick_args(const float* f_in, int64_t n_outer, int64_t n_line, int64_t n_inner, const double* E,
+                              int64_t e_div, double dt, double dv, const void* net, int32_t* status) {
+    MlpSweepArgs a{};
+    a.in = f_in;
+    a.n_outer = n_outer;
+    a.n_line = (int)n_line;
+    a.n_inner = n_inner;
+    a.sel_div = 1;
+    a.sel_mod = 1;
+    a.E = E;
+    a.e_div = e_div;
+    a.dt = dt;
+    a.dv = dv;
+    a.net = static_cast<const __nv_bfloat16*>(net);
+    a.inv_scale = 1.0f;
+    a.status = reinterpret_cast<int*>(status);
+    return a;
 }
 
 int vp_mlp_drift(const float* f_in, float* f_out, int64_t n_outer, int64_t n_line, int64_t n_inner, int64_t sel_div,
                  int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha, const void* net,
                  int32_t* status, void* stream) {
-    int rc = mlp_check(f_in, net, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha, status,
-                       "vp_mlp_drift: null pointer");
-    if (rc) return rc;
+    if (!f_in || !net || !shift || !W || !alpha || !status) return set_error(VP_ERR_ARG, "vp_mlp_drift: null pointer");
     if (!f_out || f_out == f_in) return set_error(VP_ERR_ARG, "vp_mlp_drift: f_out null or aliasing f_in");
-    return run_mlp_sweep(false, f_in, nullptr, f_out, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha,
-                         net, nullptr, nullptr, 1.0, reinterpret_cast<int*>(status), static_cast<cudaStream_t>(stream));
+    if (sel_div <= 0 || sel_mod <= 0) return set_error(VP_ERR_ARG, "vp_mlp_drift: bad table size");
+    int rc = mlp_sizes(n_outer, n_line, n_inner);
+    if (rc) return rc;
+    MlpSweepArgs a = drift_args(f_in, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha, net, status);
+    a.out = f_out;
+    return run_mlp_sweep(false, false, a, static_cast<cudaStream_t>(stream));
 }
 
 int vp_mlp_train(const float* f_in, const float* target, int64_t n_outer, int64_t n_line, int64_t n_inner,
                  int64_t sel_div, int64_t sel_mod, const int32_t* shift, const float* W, const float* alpha,
                  const void* net, double inv_scale, float* grad, double* loss, int32_t* status, void* stream) {
-    int rc = mlp_check(f_in, net, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha, status,
-                       "vp_mlp_train: null pointer");
-    if (rc) return rc;
+    if (!f_in || !net || !shift || !W || !alpha || !status) return set_error(VP_ERR_ARG, "vp_mlp_train: null pointer");
     if (!target || !grad || !loss) return set_error(VP_ERR_ARG, "vp_mlp_train: null target, grad or loss");
-    return run_mlp_sweep(true, f_in, target, nullptr, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha,
-                         net, grad, loss, inv_scale, reinterpret_cast<int*>(status), static_cast<cudaStream_t>(stream));
+    if (sel_div <= 0 || sel_mod <= 0) return set_error(VP_ERR_ARG, "vp_mlp_train: bad table size");
+    int rc = mlp_sizes(n_outer, n_line, n_inner);
+    if (rc) return rc;
+    MlpSweepArgs a = drift_args(f_in, n_outer, n_line, n_inner, sel_div, sel_mod, shift, W, alpha, net, status);
+    a.target = target;
+    a.grad = grad;
+    a.loss = loss;
+    a.inv_scale = (float)inv_scale;
+    return run_mlp_sweep(true, false, a, static_cast<cudaStream_t>(stream));
+}
+
+int vp_mlp_kick(const float* f_in, float* f_out, int64_t n_outer, int64_t n_line, int64_t n_inner, const double* E,
+                int64_t e_div, double dt, double dv, const void* net, int32_t* status, void* stream) {
+    if (!f_in || !E || !net || !status) return set_error(VP_ERR_ARG, "vp_mlp_kick: null pointer");
+    if (!f_out || f_out == f_in) return set_error(VP_ERR_ARG, "vp_mlp_kick: f_out null or aliasing f_in");
+    if (e_div <= 0 || n_outer % e_div || dv == 0.0) return set_error(VP_ERR_ARG, "vp_mlp_kick: bad e_div or dv");
+    int rc = mlp_sizes(n_outer, n_line, n_inner);
+    if (rc) return rc;
+    MlpSweepArgs a = kick_args(f_in, n_outer, n_line, n_inner, E, e_div, dt, dv, net, status);
+    a.out = f_out;
+    return run_mlp_sweep(false, true, a, static_cast<cudaStream_t>(stream));
+}
+
+int vp_mlp_train_kick(const float* f_in, const float* target, int64_t n_outer, int64_t n_line, int64_t n_inner,
+                      const double* E, int64_t e_div, double dt, double dv, const void* net, double inv_scale,
+                      float* grad, double* loss, int32_t* status, void* stream) {
+    if (!f_in || !E || !net || !status) return set_error(VP_ERR_ARG, "vp_mlp_train_kick: null pointer");
+    if (!target || !grad || !loss) return set_error(VP_ERR_ARG, "vp_mlp_train_kick: null target, grad or loss");
+    if (e_div <= 0 || n_outer % e_div || dv == 0.0) return set_error(VP_ERR_ARG, "vp_mlp_train_kick: bad e_div or dv");
+    int rc = mlp_sizes(n_outer, n_line, n_inner);
+    if (rc) return rc;
+    MlpSweepArgs a = kick_args(f_in, n_outer, n_line, n_inner, E, e_div, dt, dv, net, status);
+    a.target = target;
+    a.grad = grad;
+    a.loss = loss;
+    a.inv_scale = (float)inv_scale;
+    return run_mlp_sweep(true, true, a, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

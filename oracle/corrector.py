@@ -61,14 +61,44 @@ def stencil(f: np.ndarray, shift: np.ndarray, axis: int, vel_axis: int):
     return np.stack(F), jj
 
 
-def forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3):
-    """Corrected drift of f (float32) and the intermediates of every cell."""
+def kick_cells(f: np.ndarray, E: np.ndarray, dt: float, dv: float, axis: int):
+    """Per-cell stencil F [cells][6], plain weights w [cells][6] (float32) and
+    fraction alpha [cells] of the exact kick along axis (vp_kick, window < 0):
+    row o of the [outer][line][inner] view moves by d = (E_o dt)/dv (float64),
+    s = floor(d), f_k = f[o, l - s - (k - 2), c] (zero outside the line)."""
+    f = np.asarray(f, np.float32)
+    shape = f.shape
+    n_outer = int(np.prod(shape[:axis]))
+    n, n_inner = shape[axis], int(np.prod(shape[axis + 1:]))
+    Eo = np.repeat(np.asarray(E, np.float64).reshape(-1), n_outer // np.asarray(E).size)
+    d = (Eo * dt) / dv
+    s = np.floor(d)
+    al = d - s
+    from oracle.core import lagrange5_weights
+
+    w6 = np.asarray(lagrange5_weights(al)).astype(np.float32)  # [6][outer]
+    g = f.reshape(n_outer, n, n_inner)
+    F = np.zeros((6, n_outer, n, n_inner), np.float32)
+    for k in range(6):
+        src = np.arange(n)[None, :] - s.astype(np.int64)[:, None] + 2 - k  # [outer][line]
+        ok = (src >= 0) & (src < n)
+        F[k] = np.where(ok[:, :, None], np.take_along_axis(g, np.clip(src, 0, n - 1)[:, :, None], axis=1), 0)
+    cells = n_outer * n * n_inner
+    w = np.broadcast_to(w6.T[:, None, None, :], (n_outer, n, n_inner, 6)).reshape(cells, 6)
+    alc = np.broadcast_to(al.astype(np.float32)[:, None, None], (n_outer, n, n_inner)).reshape(cells)
+    return F.reshape(6, cells).T, w, alc
+
+
+def drift_cells(f: np.ndarray, shift, W, alpha, axis: int, vel_axis: int):
+    """Per-cell stencil, table weights and fraction of the periodic drift."""
     f = np.asarray(f, np.float32)
     F, jj = stencil(f, shift, axis, vel_axis)
-    F = F.reshape(6, -1).T  # [cells][6]
     j = jj.reshape(-1)
-    w = np.asarray(W, np.float32)[:, j].T  # [cells][6]
-    al = np.asarray(alpha, np.float32)[j]
+    return F.reshape(6, -1).T, np.asarray(W, np.float32)[:, j].T, np.asarray(alpha, np.float32)[j]
+
+
+def forward_cells(F, w, al, W1, W2, W3):
+    """The corrected sweep of cells with stencils F, weights w, fractions al."""
     s = np.abs(F).max(axis=1)
     inv = np.where(s > 0, np.float32(1.0) / np.where(s > 0, s, 1).astype(np.float32), np.float32(0.0))
     inv = inv.astype(np.float32)
@@ -93,13 +123,13 @@ def forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3):
         a = (w[:, k] + (o[:, k] - mean)).astype(np.float32)
         y = (a.astype(np.float64) * F[:, k].astype(np.float64) + y.astype(np.float64)).astype(np.float32)
     cache = dict(F=F, x=x, z1=z1, h1=h1, z2=z2, h2=h2, o=o, W1b=W1b, W2b=W2b, W3b=W3b)
-    return y.reshape(f.shape), cache
+    return y, cache
 
 
-def train_grad(f, target, shift, W, alpha, axis, vel_axis, W1, W2, W3, inv_scale):
+def train_cells(F, w, al, target, W1, W2, W3, inv_scale):
     """(sum r^2, dW1, dW2, dW3) of r = (y - target) * inv_scale."""
-    y, c = forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3)
-    r = ((y.reshape(-1) - np.asarray(target, np.float32).reshape(-1)) * np.float32(inv_scale)).astype(np.float32)
+    y, c = forward_cells(F, w, al, W1, W2, W3)
+    r = ((y - np.asarray(target, np.float32).reshape(-1)) * np.float32(inv_scale)).astype(np.float32)
     loss = float(np.sum(r.astype(np.float64) ** 2))
     gy = (np.float32(2.0) * r * np.float32(inv_scale)).astype(np.float32)
     g = gy[:, None] * c["F"]
@@ -115,3 +145,14 @@ def train_grad(f, target, shift, W, alpha, axis, vel_axis, W1, W2, W3, inv_scale
     dW2 = dz2.T.astype(np.float64) @ c["h1"].astype(np.float64)
     dW3 = do.T.astype(np.float64) @ c["h2"].astype(np.float64)
     return loss, dW1, dW2, dW3
+
+
+def forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3):
+    """Corrected drift of f (float32) and the intermediates of every cell."""
+    y, cache = forward_cells(*drift_cells(f, shift, W, alpha, axis, vel_axis), W1, W2, W3)
+    return y.reshape(np.shape(f)), cache
+
+
+def train_grad(f, target, shift, W, alpha, axis, vel_axis, W1, W2, W3, inv_scale):
+    """(sum r^2, dW1, dW2, dW3) of the corrected drift against target."""
+    return train_cells(*drift_cells(f, shift, W, alpha, axis, vel_axis), target, W1, W2, W3, inv_scale)

@@ -1,8 +1,8 @@
-"""Learned drift correction on tensor cores (vp_mlp_drift / vp_mlp_train)
-against the CPU oracle of the same network (oracle/corrector.py): the
-forward pass, the loss and the weight gradients; training lowers the loss on
-coarse / refined pairs; with a zero output layer the corrected drift is the
-plain drift."""
+"""Learned interpolation correction on tensor cores (vp_mlp_drift /
+vp_mlp_kick and their training passes) against the CPU oracle of the same
+network (oracle/corrector.py): the forward pass, the loss and the weight
+gradients, for drifts and kicks; with a zero output layer the corrected sweep
+is the plain one; training lowers the loss on coarse / refined pairs."""
 import math
 
 import numpy as np
@@ -58,6 +58,59 @@ def test_forward_matches_oracle(vp, axis):
     assert err < 1e-2, err
 
 
+@pytest.mark.parametrize("axis", [2, 3])
+def test_kick_forward_matches_oracle(vp, axis):
+    C, net, st, f = _setup(vp, seed=2)
+    g = torch.Generator().manual_seed(7)
+    E = (torch.randn(SHAPE[:2], generator=g, dtype=torch.float64) * 3.0).cuda()
+    dv = st.dvx if axis == 2 else st.dvy
+    y = net.kick(f, E, axis, 0.4, dv)
+    torch.cuda.synchronize()
+    net.check()
+    plain = vp.ops.kick(f, E, 0.4, dv, axis, window=-1)
+    F, w, al = OC.kick_cells(f.cpu().numpy(), E.cpu().numpy(), 0.4, dv, axis)
+    yo, _ = OC.forward_cells(F, w, al, *_oracle_args(net))
+    corr_gpu = (y - plain).cpu().numpy().reshape(-1)
+    corr_or = yo - plain.cpu().numpy().reshape(-1)
+    assert np.abs(corr_or).max() > 1e-3 * f.abs().max().item()
+    err = np.linalg.norm(corr_gpu - corr_or) / np.linalg.norm(corr_or)
+    assert err < 1e-2, err
+
+
+def test_kick_zero_output_layer_is_plain_kick(vp):
+    C, net, st, f = _setup(vp, out_scale=0.0)
+    E = torch.linspace(-4, 4, SHAPE[0] * SHAPE[1], dtype=torch.float64).reshape(SHAPE[:2]).cuda()
+    for axis, dv in ((2, st.dvx), (3, st.dvy)):
+        y = net.kick(f, E, axis, 0.4, dv)
+        plain = vp.ops.kick(f, E, 0.4, dv, axis, window=-1)
+        torch.cuda.synchronize()
+        assert (y - plain).abs().max().item() <= 2e-6 * f.abs().max().item()
+    net.check()
+
+
+@pytest.mark.parametrize("axis", [2, 3])
+def test_kick_gradients_match_oracle(vp, axis):
+    C, net, st, f = _setup(vp, seed=4)
+    g = torch.Generator().manual_seed(8)
+    E = (torch.randn(SHAPE[:2], generator=g, dtype=torch.float64) * 2.0).cuda()
+    dv = st.dvx if axis == 2 else st.dvy
+    target = vp.ops.kick(f, E, 0.4, dv, axis, window=-1) * 0.99
+    inv_scale = 1.0 / f.abs().max().item()
+    net.zero_grad()
+    net.accumulate_kick(f, target, E, axis, 0.4, dv, inv_scale)
+    torch.cuda.synchronize()
+    net.check()
+    F, w, al = OC.kick_cells(f.cpu().numpy(), E.cpu().numpy(), 0.4, dv, axis)
+    loss, dW1, dW2, dW3 = OC.train_cells(F, w, al, target.cpu().numpy(), *_oracle_args(net), inv_scale)
+    assert abs(net.loss.item() - loss) <= 1e-3 * loss
+    gr = net.grad.cpu().numpy()
+    n1, n2 = C.HID * C.K1, C.HID * C.K2
+    for got, ref in ((gr[:n1].reshape(C.HID, C.K1), dW1), (gr[n1:n1 + n2].reshape(C.HID, C.K2), dW2),
+                     (gr[n1 + n2:].reshape(C.NO, C.K2), dW3)):
+        err = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30)
+        assert err < 2e-2, err
+
+
 def test_zero_output_layer_is_plain_drift(vp):
     C, net, st, f = _setup(vp, out_scale=0.0)
     y = net.drift(f, st.tx, _alpha(C, st, 0), 0, 2)
@@ -92,32 +145,43 @@ def test_gradients_match_oracle(vp, axis):
 
 
 def test_training_lowers_loss(vp):
-    """Forty Adam steps on coarse / 2x-refined pairs lower the pair loss."""
+    """Sixty Adam steps on the kick pairs of a 2x-refined run restricted to a
+    16^4 grid lower the pair loss."""
     C = vp.corrector
     Nx = Nv = 16
     L_ = 4 * math.pi
-    src = C.PairSource(Nx, Nx, Nv, Nv, L_, L_, 6.0, 6.0, 0.2)
+    src = C.PairSource(Nx, Nx, Nv, Nv, L_, L_, 6.0, 6.0, 0.1)
     net = C.Corrector("cuda", seed=3)
-    f = vp.workloads.initial_2d("landau", 2 * Nx, 2 * Nx, 2 * Nv - 1, 2 * Nv - 1, L_, L_, 6.0, 6.0, 0.1, 0.5)
-    for _ in range(5):
-        f = src.fine.step(f)
-    (fx, gx), (fy, gy) = src.pairs(f)
-    inv = 1.0 / fx.abs().max().item()
-    cells = fx.numel()
-    losses = []
-    for _ in range(40):
-        net.zero_grad()
-        net.accumulate(fx, gx, src.coarse.tx, src.alpha_x, 0, 2, inv)
-        net.accumulate(fy, gy, src.coarse.ty, src.alpha_y, 1, 3, inv)
-        losses.append(net.loss.item() / (2 * cells))
-        net.adam(2 * cells, lr=3e-3)
-    net.check()
-    assert losses[-1] < 0.7 * losses[0], (losses[0], losses[-1])
+    ic = dict(kind="landau", eps=0.1, k=0.5, v0=0.0)
+    pairs = C.collect_kick_pairs(src, [ic], (20, 40, 60), L_, 6.0)
+    assert len(pairs) == 6
+    losses = C.train_kicks(net, pairs, src.coarse, iters=60, batch=6, lr=1e-3)
+    assert losses[-1] < 0.8 * losses[0], (losses[0], losses[-1])
+
+
+def test_learned_step_with_zero_nets_is_plain_step(vp):
+    """With zero output layers the learned stepper is the plain step (up to
+    FP32 summation order: separate kicks instead of the fused one)."""
+    C = vp.corrector
+    n = 16
+    L_ = 4 * math.pi
+    ls = C.LearnedStepper2D(C.Corrector("cuda"), n, n, n, n, L_, L_, 6.0, 6.0, 0.1, drift_net=C.Corrector("cuda"))
+    st = vp.Stepper2D(n, n, n, n, L_, L_, 6.0, 6.0, 0.1, dtype=torch.float32, window=-1, precise_tables=True)
+    f = vp.workloads.initial_2d("landau", n, n, n, n, L_, L_, 6.0, 6.0, 0.05, 0.5)
+    h = torch.zeros((12, 2), dtype=torch.float64, device="cuda")
+    ls.run(f.clone(), 12, history=h, graph=True, chunk=4)
+    hp = torch.zeros((12, 8), dtype=torch.float64, device="cuda")
+    st.run(f.clone(), 12, history=hp, graph=False)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(h[:, :2].cpu().numpy(), hp[:, :2].cpu().numpy(), rtol=1e-5)
 
 
 def test_learned_step_runs(vp):
+    """An untrained network: the step runs (graph-captured) and stays finite;
+    the corrected kicks need not conserve mass exactly, so the mass drift is
+    reported, not bounded here."""
     C = vp.corrector
-    net = C.Corrector("cuda", seed=0)
+    net = C.Corrector("cuda", seed=0, out_scale=1e-4)
     n = 16
     ls = C.LearnedStepper2D(net, n, n, n, n, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1)
     f = vp.workloads.initial_2d("landau", n, n, n, n, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.05, 0.5)
@@ -127,4 +191,4 @@ def test_learned_step_runs(vp):
     net.check()
     hh = h.cpu().numpy()
     assert np.isfinite(hh).all() and (hh[:, 0] > 0).all()
-    assert abs(hh[-1, 1] / hh[0, 1] - 1) < 1e-3
+    assert abs(hh[-1, 1] / hh[0, 1] - 1) < 5e-2
