@@ -373,8 +373,8 @@ int vp_mlp_train(const float* f_in, const float* target, int64_t n_outer, int64_
                  double* loss, int32_t* status, void* stream);
 /* The same correction applied to the kick of vp_kick (window < 0): row o of
  * [n_outer][n_line][n_inner] moves by E[o / e_div] * dt / dv cells, zero
- * outside the line; the shift, the fraction alpha and the plain weights are
- * those of vp_kick. */
+ * outside the line; the shift, the fraction alpha and the plain weights
+ * follow vp_kick's formulas, evaluated in FP32. */
 int vp_mlp_kick(const float* f_in, float* f_out, int64_t n_outer, int64_t n_line, int64_t n_inner,
                 const double* E, int64_t e_div, double dt, double dv, const void* net, int32_t* status,
                 void* stream);

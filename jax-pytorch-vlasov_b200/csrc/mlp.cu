@@ -3,7 +3,7 @@
 // A per-cell network proposes a correction dw to the 6 Lagrange weights of
 // a sweep: a periodic drift (x / y, shift and weights from the drift table)
 // or a Dirichlet kick (vx / vy, shift and weights from the plane's field E,
-// the arithmetic of the plain kick):
+// the formulas of the plain kick evaluated in FP32):
 //   x  = [f_k / s (k < 6), alpha - 1/2, 1, 0 x 8]          s = max_k |f_k|
 //   h1 = relu(W1 x)            W1: [64][16]  (column 7 = bias)
 //   h2 = relu(W2 [h1, 1, 0])   W2: [64][80]  (column 64 = bias)
@@ -15,9 +15,10 @@
 //
 // Each tile is 128 consecutive cells of the flattened
 // [n_outer][n_line][n_inner] array (the MMA M), thread <-> cell <->
-// accumulator lane; an inference CTA of 256 threads runs two tiles per MMA
-// round trip (tensor-memory columns 0-127 and 128-255), a training CTA of
-// 128 threads one. Every operand lives in shared
+// accumulator lane, one tile per CTA of 128 threads at a time. Inference
+// CTAs hold 128 tensor-memory columns and ~48 KB of shared memory, so four
+// share an SM and overlap one another's MMA waits; training CTAs hold all 512
+// columns (the weight gradients live there). Every operand lives in shared
 // memory in the canonical K-major layout without swizzle (8 x 16-byte core
 // matrices, K chunks 128 bytes apart, 8-row groups (K/8)*128 bytes apart).
 // A single thread issues the MMAs; completion is signalled through one
@@ -47,9 +48,9 @@ namespace vp {
 namespace mlp {
 
 constexpr int TM = 128;  // cells per tile = MMA M
-// tiles per CTA: inference keeps two tiles (256 threads) in each MMA round
-// trip, training one (its tensor memory holds the weight gradients)
-__host__ __device__ constexpr int subtiles(bool train) { return train ? 1 : 2; }
+// tiles per CTA and MMA round trip (one: independent CTAs interleave their
+// MMA waits with each other's epilogues)
+__host__ __device__ constexpr int subtiles(bool) { return 1; }
 constexpr int XS = TM * 16 * 2;  // bytes of one tile's layer-1 input [TM][16]
 constexpr int HS = TM * 80 * 2;  // bytes of one tile's hidden layer [TM][80]
 constexpr int K1 = 16;   // layer-1 input width
@@ -163,6 +164,25 @@ __device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float
     *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
 }
 
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a in the low half
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// 8 consecutive K elements of one row (one 16-byte row of a core matrix)
+__device__ __forceinline__ void st8_bf16(unsigned char* base, uint32_t off, const float* v) {
+    *reinterpret_cast<uint4*>(base + off) =
+        make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+}
+
+// the stencil, plain weights and fraction of one cell
+struct CellData {
+    float f[6], w[6];
+    float al;
+    int64_t cell;
+    bool act;
+};
+
 // ---------------------------------------------------------------------------
 // shared-memory plan (bytes)
 // ---------------------------------------------------------------------------
@@ -185,7 +205,9 @@ __host__ __device__ constexpr Smem plan(bool train) {
     const uint32_t sub = (uint32_t)subtiles(train);
     s.x = take(sub * XS);
     s.h1 = take(sub * HS);
-    s.h2 = take(sub * HS);
+    // inference: layer 2's output overwrites layer 1's (no longer read once
+    // the layer-2 MMA has completed); training keeps both for the gradients
+    s.h2 = train ? take(sub * HS) : s.h1;
     s.w1 = take(HID * K1 * 2);
     s.w2 = take(HID * K2 * 2);
     s.w3 = take(NO * K2 * 2);
@@ -210,7 +232,7 @@ __host__ __device__ constexpr Smem plan(bool train) {
 constexpr uint32_t T_D1 = 0, T_D2 = 64, T_D3 = 128;  // forward (D3: 16 used of 32)
 constexpr uint32_t T_G2 = 160, T_G1 = 224;           // backward deltas
 constexpr uint32_t T_WA = 288, T_WB = 384;           // [dW2 | dW1] (96), dW3^T (16)
-constexpr uint32_t TMEM_TRAIN = 512, TMEM_INFER = 256;
+constexpr uint32_t TMEM_TRAIN = 512, TMEM_INFER = 128;
 
 }  // namespace mlp
 
@@ -306,8 +328,9 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
     double loss_acc = 0.0;
     bool wacc = false;  // weight-gradient accumulators hold data
 
-    // one MMA group issued by thread 0, completion awaited by all threads
-    auto run = [&](auto&& issue) -> bool {
+    // one MMA group issued by thread 0, completion awaited by all threads;
+    // `work` runs on every thread while the tensor cores compute
+    auto run_with = [&](auto&& issue, auto&& work) -> bool {
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -316,89 +339,112 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
             issue();
             commit(bar);
         }
+        work();
         const bool done = mbar_wait(bar, phase & 1u);
         phase++;
         const bool all = __syncthreads_and(done) != 0;  // every thread takes the same exit
         fence_after();
         return all;
     };
+    auto run = [&](auto&& issue) -> bool { return run_with(issue, [] {}); };
 
     const int64_t tiles = (a.cells + TM - 1) / TM;
     const int n = a.n_line;
-    for (int64_t tile0 = (int64_t)blockIdx.x * SUB; tile0 < tiles && ok; tile0 += (int64_t)gridDim.x * SUB) {
-        const int64_t cell = (tile0 + u) * TM + tl;  // = (o * n + l) * n_inner + c
-        const bool act = cell < a.cells;
-        const int64_t c = act ? cell % a.n_inner : 0;
-        const int l = act ? (int)((cell / a.n_inner) % n) : 0;
-        const int64_t o = act ? cell / (a.n_inner * n) : 0;
-        // stencil of this cell: f_k = in[o, l - s - (k - 2), c], taken mod n
-        // (drift) or zero outside [0, n) (kick)
-        float f[6], w[6];
-        float al = 0.0f;
-        if (act) {
+    // stencil of a cell: f_k = in[o, l - s - (k - 2), c], taken mod n (drift)
+    // or zero outside [0, n) (kick)
+    auto gather = [&](int64_t tile0) {
+        CellData d;
+        d.cell = (tile0 + u) * TM + tl;  // = (o * n + l) * n_inner + c
+        d.act = tile0 < tiles && d.cell < a.cells;
+        d.al = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) d.f[k] = d.w[k] = 0.0f;
+        if (d.act) {
+            const int64_t c = d.cell % a.n_inner;
+            const int l = (int)((d.cell / a.n_inner) % n);
+            const int64_t o = d.cell / (a.n_inner * n);
             const float* col = a.in + (o * n) * a.n_inner + c;
             if constexpr (KICK) {
-                const double e = a.E[o / a.e_div];
-                int s = kick_weights<double, float>(e, a.dt, a.dv, -1, w);
+                // shift and weights in FP32 (the network corrects them anyway;
+                // FP64 divisions per cell would dominate the kernel)
+                const float e = (float)a.E[o / a.e_div];
+                int s = kick_weights<float, float>(e, a.dt, a.dv, -1, d.w);
                 s = max(-(1 << 28), min(1 << 28, s));
-                const double d = e * a.dt / a.dv;
-                al = (float)(d - floor(d));
+                const float dd = __fdiv_rn(__fmul_rn(e, (float)a.dt), (float)a.dv);
+                d.al = __fsub_rn(dd, floorf(dd));
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
                     const int64_t r = (int64_t)l - s + 2 - k;
-                    f[k] = (r >= 0 && r < n) ? col[r * a.n_inner] : 0.0f;
+                    d.f[k] = (r >= 0 && r < n) ? col[r * a.n_inner] : 0.0f;
                 }
             } else {
                 const int j = (int)((c / a.sel_div) % a.sel_mod);
                 const int s = a.shift[j];
-                al = a.alpha[j];
+                d.al = a.alpha[j];
                 int r = (int)(((int64_t)l - s + 2) % n);
                 if (r < 0) r += n;
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
-                    f[k] = col[(int64_t)r * a.n_inner];
-                    w[k] = a.W[k * a.sel_mod + j];
+                    d.f[k] = col[(int64_t)r * a.n_inner];
+                    d.w[k] = a.W[k * a.sel_mod + j];
                     r = r == 0 ? n - 1 : r - 1;
                 }
             }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) f[k] = w[k] = 0.0f;
         }
+        return d;
+    };
+
+    const int64_t step = (int64_t)gridDim.x * SUB;
+    CellData nxt = gather((int64_t)blockIdx.x * SUB);
+    for (int64_t tile0 = (int64_t)blockIdx.x * SUB; tile0 < tiles && ok; tile0 += step) {
+        const CellData cur = nxt;
+        const bool act = cur.act;
+        const int64_t cell = cur.cell;
+        const float* f = cur.f;
+        const float* w = cur.w;
         float sc = 0.0f;
 #pragma unroll
         for (int k = 0; k < 6; ++k) sc = fmaxf(sc, fabsf(f[k]));
         const float inv = sc > 0.0f ? 1.0f / sc : 0.0f;
+        {
+            float xv[8];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) st_bf16(sm, S.x + ux + kmaj(tl, k, K1), f[k] * inv);
-        st_bf16(sm, S.x + ux + kmaj(tl, 6, K1), act ? al - 0.5f : 0.0f);
+            for (int k = 0; k < 6; ++k) xv[k] = f[k] * inv;
+            xv[6] = act ? cur.al - 0.5f : 0.0f;
+            xv[7] = 1.0f;
+            st8_bf16(sm, S.x + ux + kmaj(tl, 0, K1), xv);
+        }
         if (TRAIN) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) st_bf16(sm, S.bw + kmaj(K2 + k, t, KW), f[k] * inv);
-            st_bf16(sm, S.bw + kmaj(K2 + 6, t, KW), act ? al - 0.5f : 0.0f);
+            st_bf16(sm, S.bw + kmaj(K2 + 6, t, KW), act ? cur.al - 0.5f : 0.0f);
             st_bf16(sm, S.bw + kmaj(K2 + 7, t, KW), act ? 1.0f : 0.0f);
         }
         // layer 1
-        if (!(ok = run([&] {
-                  for (int v = 0; v < SUB; ++v)
-                      gemm(tm + v * 128 + T_D1, base + S.x + v * XS, base + S.w1, K1, HID, false);
-              })))
+        if (!(ok = run_with(
+                  [&] {
+                      for (int v = 0; v < SUB; ++v)
+                          gemm(tm + v * 128 + T_D1, base + S.x + v * XS, base + S.w1, K1, HID, false);
+                  },
+                  [&] { nxt = gather(tile0 + step); })))
             break;
         uint32_t m1[2] = {0u, 0u}, m2[2] = {0u, 0u};  // relu masks of z1, z2
 #pragma unroll
-        for (int q = 0; q < HID / 16; ++q) {
-            float v[16];
-            tmem_ld16(lane_base + T_D1 + q * 16, v);
+        for (int q = 0; q < HID / 16; q += 2) {  // two loads in flight per wait
+            float v[32];
+            tmem_ld16(lane_base + T_D1 + q * 16, *reinterpret_cast<float(*)[16]>(v));
+            tmem_ld16(lane_base + T_D1 + q * 16 + 16, *reinterpret_cast<float(*)[16]>(v + 16));
             tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
+            for (int i = 0; i < 32; ++i) {
                 const int h = q * 16 + i;
                 const bool pos = v[i] > 0.0f;
-                if (pos) m1[h >> 5] |= 1u << (h & 31);
-                const float y = act && pos ? v[i] : 0.0f;
-                st_bf16(sm, S.h1 + uh + kmaj(tl, h, K2), y);
-                if (TRAIN) st_bf16(sm, S.bw + kmaj(h, t, KW), y);
+                if (TRAIN && pos) m1[h >> 5] |= 1u << (h & 31);
+                v[i] = act && pos ? v[i] : 0.0f;
+                if (TRAIN) st_bf16(sm, S.bw + kmaj(h, t, KW), v[i]);
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) st8_bf16(sm, S.h1 + uh + kmaj(tl, q * 16 + 8 * i, K2), v + 8 * i);
         }
         // layer 2
         if (!(ok = run([&] {
@@ -407,19 +453,21 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
               })))
             break;
 #pragma unroll
-        for (int q = 0; q < HID / 16; ++q) {
-            float v[16];
-            tmem_ld16(lane_base + T_D2 + q * 16, v);
+        for (int q = 0; q < HID / 16; q += 2) {  // two loads in flight per wait
+            float v[32];
+            tmem_ld16(lane_base + T_D2 + q * 16, *reinterpret_cast<float(*)[16]>(v));
+            tmem_ld16(lane_base + T_D2 + q * 16 + 16, *reinterpret_cast<float(*)[16]>(v + 16));
             tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
+            for (int i = 0; i < 32; ++i) {
                 const int h = q * 16 + i;
                 const bool pos = v[i] > 0.0f;
-                if (pos) m2[h >> 5] |= 1u << (h & 31);
-                const float y = act && pos ? v[i] : 0.0f;
-                st_bf16(sm, S.h2 + uh + kmaj(tl, h, K2), y);
-                if (TRAIN) st_bf16(sm, S.h2t + kmaj(h, t, KW), y);
+                if (TRAIN && pos) m2[h >> 5] |= 1u << (h & 31);
+                v[i] = act && pos ? v[i] : 0.0f;
+                if (TRAIN) st_bf16(sm, S.h2t + kmaj(h, t, KW), v[i]);
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) st8_bf16(sm, S.h2 + uh + kmaj(tl, q * 16 + 8 * i, K2), v + 8 * i);
         }
         if (TRAIN) st_bf16(sm, S.h2t + kmaj(HID, t, KW), act ? 1.0f : 0.0f);
         // layer 3
@@ -454,11 +502,15 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
             gm += g6[k];
         }
         gm *= (1.0f / 6.0f);
+        {
+            float dv8[8];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float d = act ? g6[k] - gm : 0.0f;
-            st_bf16(sm, S.dO + kmaj(t, k, NO), d);
-            st_bf16(sm, S.doT + kmaj(k, t, KW), d);
+            for (int k = 0; k < 6; ++k) {
+                dv8[k] = act ? g6[k] - gm : 0.0f;
+                st_bf16(sm, S.doT + kmaj(k, t, KW), dv8[k]);
+            }
+            dv8[6] = dv8[7] = 0.0f;
+            st8_bf16(sm, S.dO + kmaj(t, 0, NO), dv8);
         }
         // dh2 = do W3 (B = W3^T [64][16])
         if (!(ok = run([&] { gemm(tm + T_G2, base + S.dO, base + S.w3t, NO, HID, false); }))) break;
@@ -467,13 +519,15 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
             float v[16];
             tmem_ld16(lane_base + T_G2 + q * 16, v);
             tmem_wait_ld();
+            float dz[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int h = q * 16 + i;
-                const float d = (m2[h >> 5] >> (h & 31)) & 1u ? v[i] : 0.0f;
-                st_bf16(sm, S.dz2 + kmaj(t, h, HID), act ? d : 0.0f);
-                st_bf16(sm, S.aw + kmaj(h, t, KW), act ? d : 0.0f);
+                dz[i] = act && ((m2[h >> 5] >> (h & 31)) & 1u) ? v[i] : 0.0f;
+                st_bf16(sm, S.aw + kmaj(h, t, KW), dz[i]);
             }
+            st8_bf16(sm, S.dz2 + kmaj(t, q * 16, HID), dz);
+            st8_bf16(sm, S.dz2 + kmaj(t, q * 16 + 8, HID), dz + 8);
         }
         // dh1 = dz2 W2 (B = W2^T [64][64])
         if (!(ok = run([&] { gemm(tm + T_G1, base + S.dz2, base + S.w2t, HID, HID, false); }))) break;
@@ -555,16 +609,16 @@ int run_mlp_sweep(bool train, bool kick, const MlpSweepArgs& args, cudaStream_t 
     MlpSweepArgs a = args;
     a.cells = a.n_outer * a.n_line * a.n_inner;
     const int64_t tiles = (a.cells + mlp::TM - 1) / mlp::TM;
-    // inference asks for at least 100 KB so that no more than two CTAs (2 x 256
+    // inference asks for at least 48 KB so that no more than four CTAs (4 x 128
     // tensor-memory columns) share an SM
-    const size_t smem = train ? mlp_smem_bytes(true) : std::max<size_t>(mlp_smem_bytes(false), 100 * 1024);
+    const size_t smem = train ? mlp_smem_bytes(true) : std::max<size_t>(mlp_smem_bytes(false), 48 * 1024);
     auto kern = train ? (kick ? mlp::k_mlp_sweep<true, true> : mlp::k_mlp_sweep<true, false>)
                       : (kick ? mlp::k_mlp_sweep<false, true> : mlp::k_mlp_sweep<false, false>);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return set_cuda_error("cudaFuncSetAttribute(k_mlp_sweep)");
     // training holds all 512 tensor-memory columns: one CTA per SM;
-    // inference holds 256: two CTAs per SM
-    const int64_t per_sm = train ? 1 : 2;
+    // inference holds 128: four CTAs per SM
+    const int64_t per_sm = train ? 1 : 4;
     const int64_t sub = mlp::subtiles(train);
     const int64_t grid = std::min<int64_t>((tiles + sub - 1) / sub, (int64_t)sm_count() * per_sm);
     kern<<<(unsigned)std::max<int64_t>(grid, 1), mlp::TM * mlp::subtiles(train), smem, st>>>(a);

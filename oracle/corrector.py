@@ -64,16 +64,16 @@ def stencil(f: np.ndarray, shift: np.ndarray, axis: int, vel_axis: int):
 def kick_cells(f: np.ndarray, E: np.ndarray, dt: float, dv: float, axis: int):
     """Per-cell stencil F [cells][6], plain weights w [cells][6] (float32) and
     fraction alpha [cells] of the exact kick along axis (vp_kick, window < 0):
-    row o of the [outer][line][inner] view moves by d = (E_o dt)/dv (float64),
+    row o of the [outer][line][inner] view moves by d = (E_o dt)/dv (float32),
     s = floor(d), f_k = f[o, l - s - (k - 2), c] (zero outside the line)."""
     f = np.asarray(f, np.float32)
     shape = f.shape
     n_outer = int(np.prod(shape[:axis]))
     n, n_inner = shape[axis], int(np.prod(shape[axis + 1:]))
-    Eo = np.repeat(np.asarray(E, np.float64).reshape(-1), n_outer // np.asarray(E).size)
-    d = (Eo * dt) / dv
+    Eo = np.repeat(np.asarray(E, np.float64).reshape(-1).astype(np.float32), n_outer // np.asarray(E).size)
+    d = (Eo * np.float32(dt)) / np.float32(dv)  # float32, as the corrected kick evaluates it
     s = np.floor(d)
-    al = d - s
+    al = (d - s).astype(np.float32)
     from oracle.core import lagrange5_weights
 
     w6 = np.asarray(lagrange5_weights(al)).astype(np.float32)  # [6][outer]
