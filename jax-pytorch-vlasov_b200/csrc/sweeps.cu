@@ -37,13 +37,24 @@ constexpr int kBlock = 256;  // threads per block of the sweep kernels
 // One work item of a strided sweep: a segment of output rows of one tile of
 // blockDim.x * VEC columns of one outer row. All threads of the block call it
 // with the same item (the moment epilogue synchronises the block).
-template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ>
+// KU: rows per chunk of the sliding window (KU loads in flight per thread).
+// The 2-byte storage type uses 16 with the 6-row window so that a thread
+// keeps as many bytes in flight as the 4-byte one (the 7-row window's
+// per-element weights leave no registers for it); the moment epilogue's
+// reduce-scatter wants 8.
+template <typename TS, int NT, bool RHO>
+__host__ __device__ constexpr int chunk_rows() {
+    return (sizeof(TS) == 2 && NT == 6 && !RHO) ? 16 : kU;
+}
+
+template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ, int KU = kU>
 __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t item, unsigned char* smem_raw) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
     constexpr int NW = NT - 1;  // window rows carried from chunk to chunk
     constexpr int WV = NT == 6 ? 1 : VEC;  // distinct weight vectors per thread
     static_assert(NT == 6 || (NT == 7 && !KICK), "7-row windows are for drifts");
+    static_assert(!RHO || KU == 8, "the moment epilogue reduces 8 rows per chunk");
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -154,16 +165,16 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
         }
 
         // rows of the chunk whose first output row is lc (U loads in flight)
-        V nx[kU];
+        V nx[KU];
         auto load_chunk = [&](int lc) {
-            // whole lines of a multiple of kU rows end on the rows they began with
-            const bool last = WRAPREUSE && a.nseg == 1 && (n % kU) == 0 && (lc + kU >= l_end);
+            // whole lines of a multiple of KU rows end on the rows they began with
+            const bool last = WRAPREUSE && a.nseg == 1 && (n % KU) == 0 && (lc + KU >= l_end);
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < KU; ++u) {
                 if constexpr (!KICK) {
                     const int rr = wrap_up(rnext + u, n);
-                    if (WRAPREUSE && last && u >= kU - NW)
-                        nx[u] = first[WRAPREUSE ? u - (kU - NW) : 0];
+                    if (WRAPREUSE && last && u >= KU - NW)
+                        nx[u] = first[WRAPREUSE ? u - (KU - NW) : 0];
                     else
                         nx[u] = active ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
                 } else {
@@ -171,14 +182,16 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
                     nx[u] = (active && rr >= 0 && rr < n) ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
                 }
             }
-            rnext = KICK ? rnext + kU : wrap_up(rnext + kU, n);
+            rnext = KICK ? rnext + KU : wrap_up(rnext + KU, n);
         };
         load_chunk(l0);
 
-        for (int l = l0; l < l_end; l += kU) {
-            V res[kU];
+        for (int l = l0; l < l_end; l += KU) {
+            double rs[RHO ? KU : 1];
+            // each output row is stored (and summed) as soon as it is formed
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < KU; ++u) {
+                V res;
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
                     auto g = [&](int j) -> C { return j < NW ? win[j].v[e] : nx[j - NW].v[e]; };
@@ -188,29 +201,23 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
 #pragma unroll
                     for (int j = NT - 2; j >= 0; --j) acc = fma(wt[we][j], g(u + j), acc);
                     if constexpr (EQ) acc += bias[e];
-                    res[u].v[e] = acc;
+                    res.v[e] = acc;
                 }
-            }
-#pragma unroll
-            for (int u = 0; u < kU; ++u)
-                if (active && l + u < l_end) stv<TS, VEC>(dst + (int64_t)(l + u) * ni, res[u]);
-
-            double rs[RHO ? kU : 1];
-            if constexpr (RHO) {
-#pragma unroll
-                for (int u = 0; u < kU; ++u) {
+                const bool row_ok = active && l + u < l_end;
+                if (row_ok) stv<TS, VEC>(dst + (int64_t)(l + u) * ni, res);
+                if constexpr (RHO) {
                     double acc = 0.0;
-                    if (active && l + u < l_end) {
+                    if (row_ok) {
 #pragma unroll
-                        for (int e = 0; e < VEC; ++e) acc += (double)as_stored<TS>(res[u].v[e]);
+                        for (int e = 0; e < VEC; ++e) acc += (double)as_stored<TS>(res.v[e]);
                     }
                     rs[u] = acc;
                 }
             }
 #pragma unroll
-            for (int j = 0; j < NW; ++j) win[j] = nx[kU - NW + j];
+            for (int j = 0; j < NW; ++j) win[j] = nx[KU - NW + j];
             // next chunk's loads go out before the moment epilogue
-            if (l + kU < l_end) load_chunk(l + kU);
+            if (l + KU < l_end) load_chunk(l + KU);
 
             if constexpr (RHO) {
                 // reduce-scatter of the 8 row sums over the 32 lanes (fixed
@@ -258,7 +265,7 @@ template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, boo
 __global__ void __launch_bounds__(kBlock, 2) k_strided(const __grid_constant__ StridedArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     for (int64_t item = blockIdx.x; item < a.items; item += gridDim.x)
-        strided_item<TS, VEC, NT, KICK, RHO, WRAPREUSE, EQ>(a, item, smem_raw);
+        strided_item<TS, VEC, NT, KICK, RHO, WRAPREUSE, EQ, chunk_rows<TS, NT, RHO>()>(a, item, smem_raw);
 }
 
 // The same sweep over the items of many runs: run r owns the global items
@@ -273,7 +280,7 @@ __global__ void __launch_bounds__(kBlock, 2)
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         while (r + 1 < n_runs && start[r + 1] <= g) ++r;
         const StridedArgs a = runs[r];
-        strided_item<TS, VEC, NT, false, RHO, WRAPREUSE, false>(a, g - start[r], smem_raw);
+        strided_item<TS, VEC, NT, false, RHO, WRAPREUSE, false, chunk_rows<TS, NT, RHO>()>(a, g - start[r], smem_raw);
     }
 }
 
@@ -348,7 +355,8 @@ template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool EQ>
 static int launch_strided_t(StridedArgs a, int sms, cudaStream_t st) {
     // whole periodic lines reuse their first rows for the wrap (not with the
     // moment epilogue, whose prefetched chunk needs the registers)
-    const bool full = (a.nseg == 1) && (a.n_line % kU == 0) && (a.n_line >= kU) && !RHO;
+    constexpr int KU = chunk_rows<TS, NT, RHO>();
+    const bool full = (a.nseg == 1) && (a.n_line % KU == 0) && (a.n_line >= KU) && !RHO;
     const size_t smem = RHO ? (size_t)(kBlock / 32) * a.seg * sizeof(double) : 0;
     auto kern = (!KICK && full) ? k_strided<TS, VEC, NT, KICK, RHO, true, EQ>
                                 : k_strided<TS, VEC, NT, KICK, RHO, false, EQ>;
