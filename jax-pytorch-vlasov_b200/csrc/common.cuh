@@ -90,6 +90,65 @@ __device__ __forceinline__ void stv(TS* __restrict__ p, const Vec<TS, VEC>& r) {
     }
 }
 
+// A chunk row as it is held between its load and its use: the packed
+// storage bits for 4 x bf16 (2 registers; unpacked where the stencil reads
+// them, so the loads of a whole chunk stay in flight together), the compute
+// vector itself for every other case.
+template <typename TS, int VEC>
+struct Raw {
+    static constexpr bool packed = sizeof(TS) == 2 && VEC == 4;
+    using type = Vec<TS, VEC>;
+};
+template <>
+struct Raw<__nv_bfloat16, 4> {
+    static constexpr bool packed = true;
+    using type = uint2;
+};
+
+template <typename TS, int VEC>
+__device__ __forceinline__ typename Raw<TS, VEC>::type ldraw(const TS* __restrict__ p) {
+    if constexpr (Raw<TS, VEC>::packed) {
+        return __ldg(reinterpret_cast<const uint2*>(p));
+    } else {
+        return ldv<TS, VEC>(p);
+    }
+}
+
+template <typename TS, int VEC>
+__device__ __forceinline__ typename Raw<TS, VEC>::type raw_zero() {
+    if constexpr (Raw<TS, VEC>::packed) {
+        return make_uint2(0u, 0u);
+    } else {
+        Vec<TS, VEC> z;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) z.v[e] = compute_t<TS>(0);
+        return z;
+    }
+}
+
+// element e (a compile-time index after unrolling) of a held row
+template <typename TS, int VEC>
+__device__ __forceinline__ compute_t<TS> raw_get(const typename Raw<TS, VEC>::type& r, int e) {
+    if constexpr (Raw<TS, VEC>::packed) {
+        const uint32_t w = (e < 2) ? r.x : r.y;
+        return __uint_as_float((e & 1) ? (w & 0xFFFF0000u) : (w << 16));  // bf16 -> f32 is exact
+    } else {
+        return r.v[e];
+    }
+}
+
+template <typename TS, int VEC>
+__device__ __forceinline__ Vec<TS, VEC> raw_vec(const typename Raw<TS, VEC>::type& r) {
+    if constexpr (Raw<TS, VEC>::packed) {
+        Vec<TS, VEC> v;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) v.v[e] = raw_get<TS, VEC>(r, e);
+        return v;
+    } else {
+        return r;
+    }
+}
+
 // The value a stored element reads back as (rounding of the storage type).
 template <typename TS> __device__ __forceinline__ compute_t<TS> as_stored(compute_t<TS> v) {
     return to_c(from_c<TS>(v));

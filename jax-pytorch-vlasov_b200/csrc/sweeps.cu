@@ -38,13 +38,12 @@ constexpr int kBlock = 256;  // threads per block of the sweep kernels
 // blockDim.x * VEC columns of one outer row. All threads of the block call it
 // with the same item (the moment epilogue synchronises the block).
 // KU: rows per chunk of the sliding window (KU loads in flight per thread).
-// The 2-byte storage type uses 16 with the 6-row window so that a thread
-// keeps as many bytes in flight as the 4-byte one (the 7-row window's
-// per-element weights leave no registers for it); the moment epilogue's
-// reduce-scatter wants 8.
+// The 2-byte storage type uses 16 so that a thread keeps as many bytes in
+// flight as the 4-byte one (its held rows stay packed, 2 registers per 4
+// values); the moment epilogue's reduce-scatter wants 8.
 template <typename TS, int NT, bool RHO>
 __host__ __device__ constexpr int chunk_rows() {
-    return (sizeof(TS) == 2 && NT == 6 && !RHO) ? 16 : kU;
+    return (sizeof(TS) == 2 && !RHO) ? 16 : kU;
 }
 
 template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ, int KU = kU>
@@ -134,18 +133,20 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
         const TS* src = in + (o * n) * ni + col;
         TS* dst = out + (o * n) * ni + col;
 
-        V zero;
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) zero.v[e] = C(0);
+        using R = typename Raw<TS, VEC>::type;  // a held row (packed for 4 x bf16)
+        const R rzero = raw_zero<TS, VEC>();
 
         V win[NW];
+        R first[WRAPREUSE ? NW : 1];
         int rnext;
         if constexpr (!KICK) {
             int64_t r64 = ((int64_t)l0 - s_hi - 3) % n;
             int r = (int)(r64 < 0 ? r64 + n : r64);
 #pragma unroll
             for (int j = 0; j < NW; ++j) {
-                win[j] = active ? ldv<TS, VEC>(src + (int64_t)r * ni) : zero;
+                const R w = active ? ldraw<TS, VEC>(src + (int64_t)r * ni) : rzero;
+                win[j] = raw_vec<TS, VEC>(w);
+                if constexpr (WRAPREUSE) first[j] = w;
                 r = wrap_up(r + 1, n);
             }
             rnext = r;
@@ -154,18 +155,14 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
 #pragma unroll
             for (int j = 0; j < NW; ++j) {
                 const int rr = r + j;
-                win[j] = (active && rr >= 0 && rr < n) ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
+                win[j] = raw_vec<TS, VEC>((active && rr >= 0 && rr < n) ? ldraw<TS, VEC>(src + (int64_t)rr * ni)
+                                                                          : rzero);
             }
             rnext = r + NW;
         }
-        V first[WRAPREUSE ? NW : 1];
-        if constexpr (WRAPREUSE) {
-#pragma unroll
-            for (int j = 0; j < NW; ++j) first[j] = win[j];
-        }
 
-        // rows of the chunk whose first output row is lc (U loads in flight)
-        V nx[KU];
+        // rows of the chunk whose first output row is lc (KU loads in flight)
+        R nx[KU];
         auto load_chunk = [&](int lc) {
             // whole lines of a multiple of KU rows end on the rows they began with
             const bool last = WRAPREUSE && a.nseg == 1 && (n % KU) == 0 && (lc + KU >= l_end);
@@ -176,10 +173,10 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
                     if (WRAPREUSE && last && u >= KU - NW)
                         nx[u] = first[WRAPREUSE ? u - (KU - NW) : 0];
                     else
-                        nx[u] = active ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
+                        nx[u] = active ? ldraw<TS, VEC>(src + (int64_t)rr * ni) : rzero;
                 } else {
                     const int rr = rnext + u;
-                    nx[u] = (active && rr >= 0 && rr < n) ? ldv<TS, VEC>(src + (int64_t)rr * ni) : zero;
+                    nx[u] = (active && rr >= 0 && rr < n) ? ldraw<TS, VEC>(src + (int64_t)rr * ni) : rzero;
                 }
             }
             rnext = KICK ? rnext + KU : wrap_up(rnext + KU, n);
@@ -194,7 +191,7 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
                 V res;
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
-                    auto g = [&](int j) -> C { return j < NW ? win[j].v[e] : nx[j - NW].v[e]; };
+                    auto g = [&](int j) -> C { return j < NW ? win[j].v[e] : raw_get<TS, VEC>(nx[j - NW], e); };
                     const int we = NT == 6 ? 0 : e;
                     // ascending stencil tap k = descending window row j
                     C acc = wt[we][NT - 1] * g(u + NT - 1);
@@ -215,7 +212,7 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
                 }
             }
 #pragma unroll
-            for (int j = 0; j < NW; ++j) win[j] = nx[KU - NW + j];
+            for (int j = 0; j < NW; ++j) win[j] = raw_vec<TS, VEC>(nx[KU - NW + j]);
             // next chunk's loads go out before the moment epilogue
             if (l + KU < l_end) load_chunk(l + KU);
 
