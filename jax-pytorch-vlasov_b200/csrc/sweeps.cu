@@ -40,10 +40,10 @@ constexpr int kBlock = 256;  // threads per block of the sweep kernels
 // KU: rows per chunk of the sliding window (KU loads in flight per thread).
 // The 2-byte storage type uses 16 so that a thread keeps as many bytes in
 // flight as the 4-byte one (its held rows stay packed, 2 registers per 4
-// values); the moment epilogue's reduce-scatter wants 8.
+// values); the moment epilogue reduces 8 rows at a time.
 template <typename TS, int NT, bool RHO>
 __host__ __device__ constexpr int chunk_rows() {
-    return (sizeof(TS) == 2 && !RHO) ? 16 : kU;
+    return sizeof(TS) == 2 ? 16 : kU;
 }
 
 template <typename TS, int VEC, int NT, bool KICK, bool RHO, bool WRAPREUSE, bool EQ, int KU = kU>
@@ -53,7 +53,7 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
     constexpr int NW = NT - 1;  // window rows carried from chunk to chunk
     constexpr int WV = NT == 6 ? 1 : VEC;  // distinct weight vectors per thread
     static_assert(NT == 6 || (NT == 7 && !KICK), "7-row windows are for drifts");
-    static_assert(!RHO || KU == 8, "the moment epilogue reduces 8 rows per chunk");
+    static_assert(!RHO || KU % 8 == 0, "the moment epilogue reduces 8 rows at a time");
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -183,8 +183,38 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
         };
         load_chunk(l0);
 
+        // reduce-scatter of 8 row sums over the 32 lanes (fixed order): lane
+        // ends with row ((lane>>4)&1)*4 + ((lane>>3)&1)*2 + ((lane>>2)&1) of
+        // the 8 rows from l + row0, written to the warp's row partials
+        auto reduce8 = [&](const double (&r8)[8], int l, int row0) {
+            const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+            double t4[4], t2[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double send = h16 ? r8[i] : r8[i + 4];
+                const double keep = h16 ? r8[i + 4] : r8[i];
+                t4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const double send = h8 ? t4[i] : t4[i + 2];
+                const double keep = h8 ? t4[i + 2] : t4[i];
+                t2[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+            }
+            double t1;
+            {
+                const double send = h4 ? t2[0] : t2[1];
+                const double keep = h4 ? t2[1] : t2[0];
+                t1 = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+            }
+            t1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+            t1 += __shfl_xor_sync(0xffffffffu, t1, 1);
+            const int row = row0 + (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
+            if ((lane & 3) == 0 && l + row < l_end) wpart[warp * a.seg + (l - l0) + row] = t1;
+        };
+
         for (int l = l0; l < l_end; l += KU) {
-            double rs[RHO ? KU : 1];
+            double rs[RHO ? 8 : 1];
             // each output row is stored (and summed) as soon as it is formed
 #pragma unroll
             for (int u = 0; u < KU; ++u) {
@@ -208,7 +238,10 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
 #pragma unroll
                         for (int e = 0; e < VEC; ++e) acc += (double)as_stored<TS>(res.v[e]);
                     }
-                    rs[u] = acc;
+                    rs[u & 7] = acc;
+                    // every completed group of 8 rows but the chunk's last is
+                    // reduced at once (the last waits for the next loads)
+                    if ((u & 7) == 7 && u + 1 < KU) reduce8(rs, l, u - 7);
                 }
             }
 #pragma unroll
@@ -216,34 +249,7 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
             // next chunk's loads go out before the moment epilogue
             if (l + KU < l_end) load_chunk(l + KU);
 
-            if constexpr (RHO) {
-                // reduce-scatter of the 8 row sums over the 32 lanes (fixed
-                // order): lane ends with row ((lane>>4)&1)*4 + ((lane>>3)&1)*2 + ((lane>>2)&1)
-                const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
-                double t4[4], t2[2];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const double send = h16 ? rs[i] : rs[i + 4];
-                    const double keep = h16 ? rs[i + 4] : rs[i];
-                    t4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-                }
-#pragma unroll
-                for (int i = 0; i < 2; ++i) {
-                    const double send = h8 ? t4[i] : t4[i + 2];
-                    const double keep = h8 ? t4[i + 2] : t4[i];
-                    t2[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-                }
-                double t1;
-                {
-                    const double send = h4 ? t2[0] : t2[1];
-                    const double keep = h4 ? t2[1] : t2[0];
-                    t1 = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-                }
-                t1 += __shfl_xor_sync(0xffffffffu, t1, 2);
-                t1 += __shfl_xor_sync(0xffffffffu, t1, 1);
-                const int row = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
-                if ((lane & 3) == 0 && l + row < l_end) wpart[warp * a.seg + (l - l0) + row] = t1;
-            }
+            if constexpr (RHO) reduce8(rs, l, KU - 8);
         }
 
         if constexpr (RHO) {
@@ -579,14 +585,15 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         TS* dst = out + p * (int64_t)nvx * nvy + li * VEC;
         double m_pre = 0.0, m_post = 0.0, m_l2 = 0.0, m_sum = 0.0;
 
-        auto load_row = [&](int rr) -> V {
-            V v = (active && rr >= 0 && rr < nvx) ? ldv<TS, VEC>(src + (int64_t)rr * nvy) : zero;
+        using R = typename Raw<TS, VEC>::type;  // a held row (packed for 4 x bf16)
+        auto load_row = [&](int rr) -> R {
+            R v = (active && rr >= 0 && rr < nvx) ? ldraw<TS, VEC>(src + (int64_t)rr * nvy) : raw_zero<TS, VEC>();
             if constexpr (DIAG) {
                 if (active && rr >= 0 && rr < nvx) {
                     const double vx2 = a.vx[rr] * a.vx[rr];
 #pragma unroll
                     for (int e = 0; e < VEC; ++e) {
-                        double fv = (double)v.v[e];
+                        double fv = (double)raw_get<TS, VEC>(v, e);
                         if constexpr (EQ) fv += a.eqA[rr] * Be[e];
                         m_pre += fv * (vx2 + vy2[e]);
                     }
@@ -598,11 +605,11 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         V win[5];
         const int r0 = -sx - 3;
 #pragma unroll
-        for (int j = 0; j < 5; ++j) win[j] = load_row(r0 + j);
+        for (int j = 0; j < 5; ++j) win[j] = raw_vec<TS, VEC>(load_row(r0 + j));
         int rnext = r0 + 5;
 
         for (int l = 0; l < nvx; l += kU) {
-            V nx[kU];
+            R nx[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) nx[u] = load_row(rnext + u);
             rnext += kU;
@@ -615,7 +622,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                 if constexpr (EQ) dA = (l + u < nvx) ? dA_row(l + u) : 0.0;
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
-                    auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : nx[j - 5].v[e]; };
+                    auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : raw_get<TS, VEC>(nx[j - 5], e); };
                     C acc = wx[0] * g(u + 5);
                     acc = fma(wx[1], g(u + 4), acc);
                     acc = fma(wx[2], g(u + 3), acc);
@@ -699,7 +706,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
             }
             __syncwarp();
 #pragma unroll
-            for (int j = 0; j < 5; ++j) win[j] = nx[kU - 5 + j];
+            for (int j = 0; j < 5; ++j) win[j] = raw_vec<TS, VEC>(nx[kU - 5 + j]);
         }
         if constexpr (DIAG) {
             for (int off = team >> 1; off > 0; off >>= 1) {
