@@ -497,12 +497,21 @@ __device__ __forceinline__ void vy_taps(const C (&t)[12], const C (&wy)[6], C (&
     }
 }
 
+// Rows of a plane per chunk of the fused kick: 4 for 4 doubles per lane (the
+// same 128 bytes in flight per thread as 8 rows of 4 floats, in half the
+// registers), else 8.
+template <typename TS, int VEC>
+__host__ __device__ constexpr int kick2d_rows() {
+    return (sizeof(TS) == 8 && VEC == 4) ? 4 : kU;
+}
+
 // Planes [base, base + teams per block) of a fused kick: one team of lanes
 // per plane. All threads of the block call it with the same base.
 template <typename TS, int VEC, bool DIAG, bool EQ>
 __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t base, unsigned char* smem_raw) {
     using C = compute_t<TS>;
     using V = Vec<TS, VEC>;
+    constexpr int KK = kick2d_rows<TS, VEC>();
     const TS* __restrict__ in = static_cast<const TS*>(a.in);
     TS* __restrict__ out = static_cast<TS*>(a.out);
     const int team = a.team;
@@ -511,7 +520,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
     const int li = threadIdx.x % team;
     const bool lane_ok = li < a.groups;
     const int nvx = a.nvx, nvy = a.nvy, groups = a.groups;
-    C* rowbuf = reinterpret_cast<C*>(smem_raw) + (size_t)tid_team * kU * nvy;
+    C* rowbuf = reinterpret_cast<C*>(smem_raw) + (size_t)tid_team * KK * nvy;
 
     double vy2[VEC];
     if constexpr (DIAG) {
@@ -608,15 +617,15 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         for (int j = 0; j < 5; ++j) win[j] = raw_vec<TS, VEC>(load_row(r0 + j));
         int rnext = r0 + 5;
 
-        for (int l = 0; l < nvx; l += kU) {
-            R nx[kU];
+        for (int l = 0; l < nvx; l += KK) {
+            R nx[KK];
 #pragma unroll
-            for (int u = 0; u < kU; ++u) nx[u] = load_row(rnext + u);
-            rnext += kU;
-            // vx kick of rows l..l+kU-1 into the team's row buffer (rounded to
+            for (int u = 0; u < KK; ++u) nx[u] = load_row(rnext + u);
+            rnext += KK;
+            // vx kick of rows l..l+KK-1 into the team's row buffer (rounded to
             // the storage type, as the reference stores f between the kicks)
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < KK; ++u) {
                 C rv[VEC];
                 double dA = 0.0;
                 if constexpr (EQ) dA = (l + u < nvx) ? dA_row(l + u) : 0.0;
@@ -644,7 +653,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
             __syncwarp();
             // vy kick of the buffered rows
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < KK; ++u) {
                 V rres;
                 if constexpr (VEC == 4) {
                     C t[12];
@@ -706,7 +715,11 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
             }
             __syncwarp();
 #pragma unroll
-            for (int j = 0; j < 5; ++j) win[j] = raw_vec<TS, VEC>(nx[kU - 5 + j]);
+            for (int j = 0; j < 5; ++j) {  // the last 5 rows of [win; nx] (KK may be < 5)
+                const int idx = j + KK;
+                if (idx < 5) win[j] = win[idx];
+                else win[j] = raw_vec<TS, VEC>(nx[idx - 5]);
+            }
         }
         if constexpr (DIAG) {
             for (int off = team >> 1; off > 0; off >>= 1) {
@@ -757,7 +770,7 @@ __global__ void __launch_bounds__(kBlock, 2)
 template <typename TS, int VEC, bool DIAG, bool EQ>
 static int launch_kick2d_t(Kick2dArgs a, cudaStream_t st) {
     const int teams = kBlock / a.team;
-    const size_t smem = (size_t)teams * kU * a.nvy * sizeof(compute_t<TS>);
+    const size_t smem = (size_t)teams * kick2d_rows<TS, VEC>() * a.nvy * sizeof(compute_t<TS>);
     auto kern = k_kick2d<TS, VEC, DIAG, EQ>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -971,7 +984,8 @@ int64_t kick2d_batch_finish(Kick2dArgs* a, int dtype, int vec, int block, int64_
     const int teams = block / team;
     *items = (a->n_planes + teams - 1) / teams;
     const int64_t csz = dtype == VP_F64 ? 8 : 4;
-    return (int64_t)teams * kU * a->nvy * csz;
+    const int rows = (dtype == VP_F64 && vec == 4) ? kick2d_rows<double, 4>() : kU;
+    return (int64_t)teams * rows * a->nvy * csz;
 }
 
 template <typename TS, int VEC>

@@ -117,6 +117,30 @@ def test_kick2d(vp, dtype, shape, window):
     np.testing.assert_allclose(m[..., 0], np.einsum("xyab,ab->xy", fin, v2), rtol=1e-12)
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
+@pytest.mark.parametrize("shape", [(4, 4, 32, 128), (2, 2, 30, 128), (3, 2, 13, 128), (2, 3, 9, 64)])
+def test_kick2d_without_moments(vp, dtype, shape):
+    """The step's form of the fused kick (no moment epilogue), including the
+    4-row chunks of 4 doubles per lane and plane rows that end mid-chunk."""
+    ref_dt = torch.float64 if dtype == torch.float64 else torch.float32
+    T = NP[ref_dt]
+    g = O.make_grid2d(*shape, 2 * math.pi, 3.0, 4.0, 5.0, dtype=T)
+    f = seeded(5, shape, ref_dt)
+    if dtype == torch.bfloat16:
+        f = to_dev(f, dtype).float().cpu().numpy()
+    rng = np.random.default_rng(11)
+    Ex = rng.uniform(-2.5, 2.5, shape[:2]) * g.dvx / 0.1
+    Ey = rng.uniform(-2.5, 2.5, shape[:2]) * g.dvy / 0.1
+    mid = O.kick_static(f, Ex.astype(T) if ref_dt == torch.float32 else Ex, 0.1, g.dvx, 2, window=-1)
+    if dtype == torch.bfloat16:
+        mid = to_dev(mid, dtype).float().cpu().numpy()
+    want = O.kick_static(mid, Ey.astype(T) if ref_dt == torch.float32 else Ey, 0.1, g.dvy, 3, window=-1)
+    got = vp.ops.kick2d(to_dev(f, dtype), torch.from_numpy(Ex).cuda(), torch.from_numpy(Ey).cuda(), 0.1, g.dvx,
+                        g.dvy, window=-1)
+    tol = {torch.float64: 1e-14, torch.float32: 1e-5, torch.bfloat16: 2e-2}[dtype]
+    assert relerr(got, want) < tol
+
+
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 @pytest.mark.parametrize("axis", [0, 1, 2, 3])
 @pytest.mark.parametrize("shape", [(8, 6, 10, 12), (7, 9, 5, 6)])
