@@ -120,6 +120,17 @@ int vp_advect_gather(const void* f_in, void* f_out, int dtype, int64_t n_outer, 
                      int64_t n_inner, const void* vel, int64_t vs_outer, int64_t vs_line,
                      int64_t vs_inner, double dt, double dx, int periodic, void* stream);
 
+/* ---- interpolation helpers ---------------------------------------------- */
+
+/* The 6-point Lagrange sum of lagrange5_interp_sum (vlasov2D2V.py:238-260;
+ * vlasov1D1V.py, same function): out[i] = sum_k w_k(alpha[i]) vals[6 i + k]
+ * with the closed-form weights of the nodes -2..3, each product rounded and
+ * the terms summed left to right. dtype VP_F32 or VP_F64. */
+int vp_lagrange_interp(const void* alpha, const void* vals, void* out, int dtype, int64_t n, void* stream);
+/* The product-form weights of get_lagrange5_weights (vlasov2D2V.py:210-235):
+ * weights[6 i + j] = prod_{m != j} (alpha[i] - x_m) / (x_j - x_m). */
+int vp_lagrange_weights(const void* alpha, void* weights, int dtype, int64_t n, void* stream);
+
 /* ---- moments and field ------------------------------------------------- */
 
 /* Velocity moment. Replaces compute_rho (vlasov2D2V.py:416-431):

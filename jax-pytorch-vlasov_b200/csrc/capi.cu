@@ -237,6 +237,18 @@ int vp_rho(const void* f, int dtype, int64_t n_points, int64_t n_v, double dvx, 
     return run_rho(dtype, f, n_points, n_v, dvx, dvy, rho, out_dtype, S(stream));
 }
 
+int vp_lagrange_interp(const void* alpha, const void* vals, void* out, int dtype, int64_t n, void* stream) {
+    VP_CHECK(n >= 0, "vp_lagrange_interp: negative size");
+    VP_CHECK(n == 0 || (alpha && vals && out), "vp_lagrange_interp: null pointer");
+    return run_lagrange(dtype, alpha, vals, out, n, 0, S(stream));
+}
+
+int vp_lagrange_weights(const void* alpha, void* weights, int dtype, int64_t n, void* stream) {
+    VP_CHECK(n >= 0, "vp_lagrange_weights: negative size");
+    VP_CHECK(n == 0 || (alpha && weights), "vp_lagrange_weights: null pointer");
+    return run_lagrange(dtype, alpha, nullptr, weights, n, 1, S(stream));
+}
+
 size_t vp_poisson2d_workspace_bytes(int64_t nx, int64_t ny) { return poisson2d_ws_bytes(nx, ny); }
 
 int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,

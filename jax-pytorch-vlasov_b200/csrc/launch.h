@@ -149,6 +149,7 @@ int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n,
                int64_t vso, int64_t vsl, int64_t vsc, double dt, double dx, int periodic, cudaStream_t st);
 int run_rho(int dtype, const void* f, int64_t n_points, int64_t n_v, double dvx, double dvy, void* rho,
             int out_dtype, cudaStream_t st);
+int run_lagrange(int dtype, const void* alpha, const void* vals, void* out, int64_t n, int mode, cudaStream_t st);
 
 // batched step (sweeps.cu)
 int strided_batch_args(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner,

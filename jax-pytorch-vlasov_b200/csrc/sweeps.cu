@@ -1230,3 +1230,59 @@ int run_rho(int dtype, const void* f, int64_t n_points, int64_t n_v, double dvx,
 }
 
 }  // namespace vp
+
+// ---------------------------------------------------------------------------
+// Lagrange helpers of the interpolation API: the 6-point sum with the
+// closed-form weights (lagrange5_interp_sum, vlasov2D2V.py:238-260: each
+// product rounded, summed left to right) and the product-form weights
+// (get_lagrange5_weights, :210-235: w_j = prod_{m != j} (a - x_m)/(x_j - x_m)
+// over the nodes x = -2..3, in that order), every operation rounded on its
+// own so the results equal the reference's eager evaluation bit for bit.
+// ---------------------------------------------------------------------------
+namespace vp {
+
+template <typename T>
+__global__ void k_lagrange(const T* __restrict__ alpha, const T* __restrict__ vals, T* __restrict__ out, int64_t n,
+                           int mode) {
+    using R = Rn<T>;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T a = alpha[i];
+    if (mode == 0) {
+        T w[6];
+        lagrange6<T>(a, w);
+        T acc = R::mul(w[0], vals[6 * i]);
+#pragma unroll
+        for (int k = 1; k < 6; ++k) acc = R::add(acc, R::mul(w[k], vals[6 * i + k]));
+        out[i] = acc;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const T xj = T(j - 2);
+            T w = T(1);
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                if (m == j) continue;
+                const T xm = T(m - 2);
+                w = R::div(R::mul(w, R::sub(a, xm)), R::sub(xj, xm));
+            }
+            out[6 * i + j] = w;
+        }
+    }
+}
+
+int run_lagrange(int dtype, const void* alpha, const void* vals, void* out, int64_t n, int mode, cudaStream_t st) {
+    if (n == 0) return VP_OK;
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (dtype == VP_F64)
+        k_lagrange<double><<<grid, 256, 0, st>>>(static_cast<const double*>(alpha), static_cast<const double*>(vals),
+                                                 static_cast<double*>(out), n, mode);
+    else if (dtype == VP_F32)
+        k_lagrange<float><<<grid, 256, 0, st>>>(static_cast<const float*>(alpha), static_cast<const float*>(vals),
+                                                static_cast<float*>(out), n, mode);
+    else
+        return set_error(VP_ERR_DTYPE, "vp_lagrange: float32 or float64 only");
+    return check_launch("k_lagrange");
+}
+
+}  // namespace vp

@@ -15,7 +15,8 @@ from . import _lib as L
 from . import ops
 from .engine import Stepper1D
 from .vlasov2d2v import (STENCIL_OFFSETS, _blocks_to_shift, _check_offsets, check_v_window,  # noqa: F401
-                         lagrange5_weights, precompute_x_drift, static_stencil_offsets)
+                         get_lagrange5_weights, lagrange5_interp_sum, lagrange5_weights, precompute_x_drift,
+                         static_stencil_offsets)
 
 
 def _default_device():

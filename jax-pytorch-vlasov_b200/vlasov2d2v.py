@@ -123,6 +123,42 @@ def lagrange5_weights(alpha):
     return out.to(alpha.device) if torch.is_tensor(alpha) else out
 
 
+def _lagrange_dtype(*ts):
+    dt = torch.result_type(*ts) if len(ts) > 1 else ts[0].dtype
+    if dt not in (torch.float32, torch.float64):
+        raise TypeError(f"Lagrange helpers take float32 or float64 tensors, not {dt}")
+    return dt
+
+
+def lagrange5_interp_sum(alpha, gather_vals):
+    """The 6-point interpolation sum (lagrange5_interp_sum,
+    vlasov2D2V.py:238-260): sum_k w_k(alpha) * gather_vals[..., k] with the
+    closed-form weights, computed on the device by vp_lagrange_interp with
+    the reference's rounding (bit-identical to its eager evaluation)."""
+    L.require_cuda(alpha, gather_vals)
+    if gather_vals.shape[-1] != 6:
+        raise ValueError("gather_vals must have 6 values in its last dimension")
+    dt = _lagrange_dtype(alpha, gather_vals)
+    shape = torch.broadcast_shapes(alpha.shape, gather_vals.shape[:-1])
+    a = alpha.to(dt).expand(shape).contiguous()
+    v = gather_vals.to(dt).expand(*shape, 6).contiguous()
+    out = torch.empty(shape, dtype=dt, device=a.device)
+    L.call("vp_lagrange_interp", L.ptr(a), L.ptr(v), L.ptr(out), L.dtype_code(dt), a.numel(), L.stream_of(a))
+    return out
+
+
+def get_lagrange5_weights(alpha):
+    """Product-form Lagrange weights of the nodes -2..3
+    (get_lagrange5_weights, vlasov2D2V.py:210-235), shape (*alpha.shape, 6),
+    computed on the device by vp_lagrange_weights."""
+    L.require_cuda(alpha)
+    dt = _lagrange_dtype(alpha)
+    a = alpha.contiguous()
+    out = torch.empty((*a.shape, 6), dtype=dt, device=a.device)
+    L.call("vp_lagrange_weights", L.ptr(a), L.ptr(out), L.dtype_code(dt), a.numel(), L.stream_of(a))
+    return out
+
+
 def static_stencil_offsets(stencil_offsets) -> Tuple[int, ...]:
     """vlasov2D2V.py:644-667."""
     if isinstance(stencil_offsets, torch.Tensor):
