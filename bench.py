@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--dtype", choices=["float32", "bfloat16", "float64"], default=None)
     ap.add_argument("--size", type=int, default=None, help="override N of a 2D2V workload (N^4 grid)")
     ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
     ap.add_argument("--train-ics", type=int, default=125, help="learned workload: training initial conditions")
@@ -461,14 +461,12 @@ def run_e2e(a, f_dev, dev, dtype, world, dist, torch, vp):
     cells = math.prod(a.grid)
     gdt = torch.float64 if dtype == torch.float64 else torch.float32
     h_in = f_dev.cpu().pin_memory()
-    h_out = torch.empty_like(h_in).pin_memory()
-    d_in = torch.empty_like(f_dev)
     if a.kind == "1d":
         m = importlib.import_module("jax-pytorch-vlasov_b200.vlasov1d1v")
         g = m.Grid.create(*a.grid, a.L, a.vmax, device=dev, dtype=gdt)
-        h_rho = torch.empty(a.grid[0], dtype=gdt).pin_memory()
+        h_rho0 = torch.empty(a.grid[0], dtype=gdt)
 
-        def call():
+        def call(d_in):
             return m.vlasov_step_gather_free(d_in, a.dt, g.v, g.inv_kx, g.inv_kx_sq, g.x_indices, g.v_indices,
                                              g.x_batch_offsets, g.v_batch_offsets, g.stencil_offsets, g.dx, g.dv,
                                              g.V_max, True, 1)
@@ -476,36 +474,62 @@ def run_e2e(a, f_dev, dev, dtype, world, dist, torch, vp):
     else:
         m = importlib.import_module("jax-pytorch-vlasov_b200.vlasov2d2v")
         g = m.Grid.create(*a.grid, a.L, a.L, a.vmax, a.vmax, device=dev, dtype=gdt)
-        h_rho = torch.empty(a.grid[:2], dtype=gdt).pin_memory()
+        h_rho0 = torch.empty(a.grid[:2], dtype=gdt)
         f0 = torch.zeros(a.grid[2:], dtype=gdt, device=dev)
 
-        def call():
+        def call(d_in):
             return m.vlasov_step_gather_free(d_in, f0, a.dt, g.x, g.y, g.vx, g.vy, g.kx, g.ky, g.inv_ksq,
                                              g.x_indices, g.y_indices, g.vx_indices, g.vy_indices,
                                              g.stencil_offsets, g.dx, g.dy, g.dvx, g.dvy, g.Nx, g.Ny, True, 1)
         path = "vlasov2d2v.vlasov_step_gather_free with pinned host f in/out"
 
-    def e2e_step():
-        d_in.copy_(h_in, non_blocking=True)
-        fo, rho, _ = call()
-        h_out.copy_(fo, non_blocking=True)
-        h_rho.copy_(rho, non_blocking=True)
+    # Consecutive steps overlap: step i+1's input copies in on one stream
+    # while step i computes and step i-1's result copies out on another
+    # (PCIe carries both directions at once). Inputs rotate through three
+    # device buffers, results through two pinned host buffers.
+    comp = torch.cuda.current_stream(dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    d_in = [torch.empty_like(f_dev) for _ in range(3)]
+    h_out = [torch.empty_like(h_in).pin_memory() for _ in range(2)]
+    h_rho = [torch.empty_like(h_rho0).pin_memory() for _ in range(2)]
+    read_done = [None] * 3
 
-    e2e_step()
+    def e2e_step(i):
+        j = i % 3
+        if read_done[j] is not None:
+            s_in.wait_event(read_done[j])
+        with torch.cuda.stream(s_in):
+            d_in[j].copy_(h_in, non_blocking=True)
+        loaded = torch.cuda.Event()
+        loaded.record(s_in)
+        comp.wait_event(loaded)
+        fo, rho, _ = call(d_in[j])
+        done = torch.cuda.Event()
+        done.record(comp)
+        read_done[j] = done
+        s_out.wait_event(done)
+        with torch.cuda.stream(s_out):
+            h_out[i % 2].copy_(fo, non_blocking=True)
+            h_rho[i % 2].copy_(rho, non_blocking=True)
+        fo.record_stream(s_out)
+        rho.record_stream(s_out)
+
+    for i in range(3):
+        e2e_step(i)
     torch.cuda.synchronize(dev)
     dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(a.e2e_steps):
-        e2e_step()
-    e1.record()
+    e0.record(s_in)
+    for i in range(a.e2e_steps):
+        e2e_step(i)
+    e1.record(s_out)
     torch.cuda.synchronize(dev)
     ems = dist.max_over_ranks(e0.elapsed_time(e1))
     return {"value": world * cells * a.e2e_steps / (ems / 1e3), "unit": "cell-updates/s",
             "h2d_bytes_per_step": h_in.numel() * h_in.element_size(),
-            "d2h_bytes_per_step": h_out.numel() * h_out.element_size() + h_rho.numel() * h_rho.element_size(),
-            "steps": a.e2e_steps, "path": path}
+            "d2h_bytes_per_step": h_out[0].numel() * h_out[0].element_size() + h_rho[0].numel() * h_rho[0].element_size(),
+            "steps": a.e2e_steps, "path": path + ", steps pipelined over copy-in / compute / copy-out streams"}
 
 
 # ---------------------------------------------------------------------------
@@ -657,31 +681,65 @@ def run_batch(a):
         # end to end through the public API: every step copies every run's f
         # from pinned host memory, steps the batch, and copies f and the
         # diagnostics back
+        # The stepper advances its runs in place in one arena, so steps
+        # overlap through staging buffers: step i+1's input copies in on one
+        # stream while step i computes (staging -> arena, step, arena ->
+        # staging) and step i-1's result copies out on another.
         arena = st._arenas[0]
         h_in = arena.cpu().pin_memory()
-        h_out = torch.empty_like(h_in).pin_memory()
-        h_diag = torch.empty((n, L.DIAG_COUNT), dtype=torch.float64).pin_memory()
+        h_out = [torch.empty_like(h_in).pin_memory() for _ in range(2)]
+        h_diag = [torch.empty((n, L.DIAG_COUNT), dtype=torch.float64).pin_memory() for _ in range(2)]
+        stage_in = [torch.empty_like(arena) for _ in range(2)]
+        stage_out = [torch.empty_like(arena) for _ in range(2)]
+        diag_out = [torch.empty((n, L.DIAG_COUNT), dtype=torch.float64, device=dev) for _ in range(2)]
+        comp = torch.cuda.current_stream(dev)
+        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        consumed = [None, None]  # compute event that last read stage_in[k]
+        shipped = [None, None]   # copy-out event that last read stage_out[k]
 
-        def e2e_step():
-            arena.copy_(h_in, non_blocking=True)
+        def e2e_step(i):
+            k = i % 2
+            if consumed[k] is not None:
+                s_in.wait_event(consumed[k])
+            with torch.cuda.stream(s_in):
+                stage_in[k].copy_(h_in, non_blocking=True)
+            loaded = torch.cuda.Event()
+            loaded.record(s_in)
+            comp.wait_event(loaded)
+            arena.copy_(stage_in[k], non_blocking=True)
             st.step(0)
-            h_out.copy_(arena, non_blocking=True)
-            h_diag.copy_(st.stage[0], non_blocking=True)
+            if shipped[k] is not None:
+                comp.wait_event(shipped[k])
+            stage_out[k].copy_(arena, non_blocking=True)
+            diag_out[k].copy_(st.stage[0], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(comp)
+            consumed[k] = done
+            s_out.wait_event(done)
+            with torch.cuda.stream(s_out):
+                h_out[k].copy_(stage_out[k], non_blocking=True)
+                h_diag[k].copy_(diag_out[k], non_blocking=True)
+            out = torch.cuda.Event()
+            out.record(s_out)
+            shipped[k] = out
 
-        e2e_step()
+        for i in range(3):
+            e2e_step(i)
         torch.cuda.synchronize(dev)
         dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(a.e2e_steps):
-            e2e_step()
-        e1.record()
+        e0.record(s_in)
+        for i in range(a.e2e_steps):
+            e2e_step(i)
+        e1.record(s_out)
         torch.cuda.synchronize(dev)
         e_ms = dist.max_over_ranks(e0.elapsed_time(e1))
         e2e = {"value": world * cells * a.e2e_steps / (e_ms / 1e3), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": int(arena.numel()), "d2h_bytes_per_step": int(arena.numel() + h_diag.numel() * 8),
-               "steps": a.e2e_steps, "path": "BatchStepper2D.step with every run's f copied from/to pinned host memory"}
+               "h2d_bytes_per_step": int(arena.numel()), "d2h_bytes_per_step": int(arena.numel() + n * L.DIAG_COUNT * 8),
+               "steps": a.e2e_steps,
+               "path": "BatchStepper2D.step with every run's f copied from/to pinned host memory, steps pipelined "
+                       "over copy-in / compute / copy-out streams through device staging buffers"}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -220,7 +220,7 @@ def _fused(f, dt, table, grid_inv_kx, grid_inv_kx_sq, grid_dx, grid_dv, physics_
     st.physics_mode = bool(physics_mode)
     out = st.step(f, torch.empty_like(f))
     cdt = _out_dtype(f)
-    return out, st.rho.to(cdt), st.phi.to(cdt)
+    return out, st.rho.to(cdt, copy=True), st.phi.to(cdt, copy=True)
 
 
 def vlasov_step_gather_free(f, dt, grid_v, grid_inv_kx, grid_inv_kx_sq, x_indices, v_indices, x_batch_offsets,
@@ -320,8 +320,8 @@ class Vlasov:
                                               g.V_max, self.physics_mode)
             else:
                 f = self.stepper.run(f, n, history=hist[done: done + n])
-                rho = self.stepper.rho.to(_out_dtype(f)).clone()
-                phi = self.stepper.phi.to(_out_dtype(f)).clone()
+                rho = self.stepper.rho.to(_out_dtype(f), copy=True)
+                phi = self.stepper.phi.to(_out_dtype(f), copy=True)
             done += n
             state = SimulationState(Field(rho, phi), Variables(f, state.variables.f0), state.t + n * self.dt,
                                     state.step + n)

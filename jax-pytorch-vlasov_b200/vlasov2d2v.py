@@ -368,7 +368,7 @@ def _fused_step(f, dt, tables, spectral, grid_dx, grid_dy, grid_dvx, grid_dvy, p
     plan.physics_mode = bool(physics_mode)
     out = plan.step(f, torch.empty_like(f))
     cdt = _out_dtype(f)
-    return out, plan.drho.to(cdt), plan.phi.to(cdt)
+    return out, plan.drho.to(cdt, copy=True), plan.phi.to(cdt, copy=True)
 
 
 def _spectral(grid_kx, grid_ky, grid_inv_ksq, device):
@@ -522,8 +522,8 @@ class Vlasov:
                 rho_out, phi_out = drho, phi
             else:
                 f = st.run(f, n, history=hist[done: done + n], graph=self.graph and n >= 4)
-                rho_out = st.drho.to(_out_dtype(f)).clone()
-                phi_out = st.phi.to(_out_dtype(f)).clone()
+                rho_out = st.drho.to(_out_dtype(f), copy=True)
+                phi_out = st.phi.to(_out_dtype(f), copy=True)
             done += n
             state = SimulationState(Field(rho_out, phi_out), Variables(f, state.variables.f0),
                                     state.t + n * self.dt, state.step + n)

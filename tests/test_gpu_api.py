@@ -207,3 +207,29 @@ def test_vlasov_driver_1d(v1, tmp_path):
                                              g.V_max, True)
     assert torch.equal(f, state.variables.fn)
     assert sorted(os.listdir(tmp_path)) == ["field_000000.npz", "field_000010.npz", "field_000020.npz"]
+
+
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_fused_step_returns_fresh_fields(v1, v2, dt):
+    """rho and phi returned by one fused step stay as they were after the
+    next call (the reference computes new tensors each call)."""
+    g = v2.Grid.create(**STEP, dtype=TD[dt])
+    f = seeded(3, (g.Nx, g.Ny, g.Nvx, g.Nvy), dt)
+    f0 = torch.zeros((g.Nvx, g.Nvy), dtype=TD[dt], device="cuda")
+    args = (0.1, g.x, g.y, g.vx, g.vy, g.kx, g.ky, g.inv_ksq, g.x_indices, g.y_indices, g.vx_indices,
+            g.vy_indices, g.stencil_offsets, g.dx, g.dy, g.dvx, g.dvy, g.Nx, g.Ny, True)
+    f1, rho1, phi1 = v2.vlasov_step_gather_free(f, f0, *args)
+    keep = rho1.clone(), phi1.clone()
+    f2, rho2, phi2 = v2.vlasov_step_gather_free(f1, f0, *args)
+    assert rho1.data_ptr() != rho2.data_ptr() and phi1.data_ptr() != phi2.data_ptr()
+    assert torch.equal(rho1, keep[0]) and torch.equal(phi1, keep[1])
+    assert not torch.equal(rho1, rho2)
+    g1 = v1.Grid.create(24, 20, 4.0 * math.pi, 5.0, dtype=TD[dt])
+    fl = seeded(4, (24, 20), dt)
+    a1 = (0.1, g1.v, g1.inv_kx, g1.inv_kx_sq, g1.x_indices, g1.v_indices, g1.x_batch_offsets, g1.v_batch_offsets,
+          g1.stencil_offsets, g1.dx, g1.dv, g1.V_max, True)
+    s1, r1, p1 = v1.vlasov_step_gather_free(fl, *a1)
+    keep = r1.clone(), p1.clone()
+    s2, r2, p2 = v1.vlasov_step_gather_free(s1, *a1)
+    assert r1.data_ptr() != r2.data_ptr() and p1.data_ptr() != p2.data_ptr()
+    assert torch.equal(r1, keep[0]) and torch.equal(p1, keep[1])
