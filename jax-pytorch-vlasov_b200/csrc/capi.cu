@@ -1,6 +1,7 @@
 // C ABI of the Vlasov-Poisson library: argument checks, workspace layout and
 // the launch sequence of one Strang step. Declarations and the reference
 // functions each entry point replaces: include/vlasov_b200.h.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -102,7 +103,11 @@ size_t step2d_layout(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, char* bas
         return p;
     };
     Step2dWs t;
-    t.part = reinterpret_cast<double*>(take(drift_rho_part_bytes(nx, ny, nvx * nvy)));
+    // density partials: per 128-column tile of the y sweep, or per
+    // 32-column group of the fused (x, y) pass
+    const size_t part_sweep = drift_rho_part_bytes(nx, ny, nvx * nvy);
+    const size_t part_plane = al((size_t)nx * ny * (size_t)plane_part_tiles(nvx, nvy) * sizeof(double));
+    t.part = reinterpret_cast<double*>(take(std::max(part_sweep, part_plane)));
     t.rho = reinterpret_cast<double*>(take((size_t)nx * ny * sizeof(double)));
     t.ex = reinterpret_cast<double*>(take((size_t)nx * ny * sizeof(double)));
     t.ey = reinterpret_cast<double*>(take((size_t)nx * ny * sizeof(double)));
@@ -324,15 +329,35 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         return set_error(VP_ERR_UNSUPPORTED, "vp_step2d: the equilibrium split needs the fused kick (nvy <= 128)");
     const EqSplit eqs{d->eq_vx, d->eq_vy, nvx, nvy};
     const EqSplit* EQ = eq_on ? &eqs : EQ_NONE;
-    const int n_sweeps = phys ? (fused ? 5 : 6) : 4;
+    // The position drifts in pairs through the (x, y) plane when the layout
+    // allows (one pass over f each, intermediate on chip, bit-identical);
+    // otherwise one sweep per axis. The fused passes are timed under the x
+    // phases, the y phases then stay empty.
+    const bool planar = !eq_on && plane_fits(d->dtype, nx, ny, nvx, nvy, d->f_in) &&
+                        plane_fits(d->dtype, nx, ny, nvx, nvy, d->f_out) &&
+                        plane_fits(d->dtype, nx, ny, nvx, nvy, d->f_tmp);
+    const int n_sweeps = (phys ? (fused ? 3 : 4) : 2) + (planar ? 0 : 2);
     int i = 0;
     auto dst_of = [&](int k) -> void* { return ((n_sweeps - 1 - k) % 2 == 0) ? d->f_out : d->f_tmp; };
     const void* src = d->f_in;
     int rc;
     Marks mk{d->events, st};
+    void* dst;
+    if (planar) {
+        // x then y drift (dt/2 each), with the density when needed
+        if ((rc = mk.begin(VP_PHASE_DRIFT_X1))) return rc;
+        dst = dst_of(i++);
+        int tiles = 0;
+        rc = run_plane(d->dtype, true, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y,
+                       want_rho ? w.part : nullptr, &tiles, st);
+        if (!rc && want_rho) rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, 0.0, w.rho, st);
+        if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
+        if ((rc = mk.begin(VP_PHASE_DRIFT_Y1)) || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
+        src = dst;
+    } else {
     // x drift (dt/2)
     if ((rc = mk.begin(VP_PHASE_DRIFT_X1))) return rc;
-    void* dst = dst_of(i++);
+    dst = dst_of(i++);
     rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_spread_x, d->shift_x, d->W_x, nullptr, 0, 1,
                      0.0, 1.0, -1, nullptr, nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
@@ -352,6 +377,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     }
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
     src = dst;
+    }
     Pois2dWsView pv{};
     double* moments = nullptr;
     if ((rc = mk.begin(VP_PHASE_FIELD))) return rc;
@@ -392,6 +418,15 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         if ((rc = mk.end(VP_PHASE_FIELD)) || (rc = mk.begin(VP_PHASE_KICK)) || (rc = mk.end(VP_PHASE_KICK)))
             return rc;
     }
+    if (planar) {
+        // y then x drift (dt/2 each)
+        if ((rc = mk.begin(VP_PHASE_DRIFT_Y2)) || (rc = mk.end(VP_PHASE_DRIFT_Y2))) return rc;
+        if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
+        dst = dst_of(i++);
+        rc = run_plane(d->dtype, false, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y, nullptr,
+                       nullptr, st);
+        if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
+    } else {
     // y drift (dt/2)
     if ((rc = mk.begin(VP_PHASE_DRIFT_Y2))) return rc;
     dst = dst_of(i++);
@@ -405,6 +440,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     rc = run_strided(d->dtype, src, dst, 1, nx, ny * nvx * nvy, false, nvy, nvx, d->shift_spread_x, d->shift_x, d->W_x, nullptr, 0, 1,
                      0.0, 1.0, -1, nullptr, nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
+    }
     if (want_diag) {
         const double dV = d->dx * d->dy * d->dvx * d->dvy;
         if (!phys) {

@@ -236,4 +236,33 @@ __device__ __forceinline__ int wrap_up(int r, int n) {
     return r;
 }
 
+// ---------------------------------------------------------------------------
+// shared-memory addresses, the global timer, mbarrier waits with a limit
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait for the mbarrier phase with the given parity; false after ~1 s
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    const uint64_t t0 = now_ns();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (now_ns() - t0 > 1000000000ull) return false;
+    }
+}
+
 }  // namespace vp

@@ -75,10 +75,6 @@ constexpr int GRAD_ELEMS = G_W3 + NO * K2;
 // ---------------------------------------------------------------------------
 // tcgen05 / mbarrier primitives (inline PTX)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
 // byte offset of element (r, k) of a [R][K] K-major bf16 matrix
 __device__ __forceinline__ uint32_t kmaj(int r, int k, int K) {
     return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
@@ -121,28 +117,6 @@ __device__ __forceinline__ void commit(uint32_t mbar) {
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ uint64_t now_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// wait for the mbarrier phase with the given parity; false after ~1 s
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    const uint64_t t0 = now_ns();
-    while (true) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(mbar), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if (now_ns() - t0 > 1000000000ull) return false;
-    }
-}
 
 // 16 consecutive FP32 columns of this thread's accumulator lane
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {

@@ -1,0 +1,556 @@
+// Two drifts in the (x, y) plane of f[x][y][vx][vy] in one pass over HBM.
+//
+// The position half-steps of the Strang step come in pairs: x then y before
+// the field solve (the y drift also yields the charge density), y then x
+// after the kick. As two sweeps, each pair writes and re-reads a full
+// intermediate copy of f; this kernel keeps the intermediate on chip.
+//
+//  * A CTA owns a group of 32 consecutive columns of the (vx, vy) plane
+//    (lane <-> column; the group sits inside one vx, so it shares one x
+//    shift) over all y, 8 y rows per thread, and walks x.
+//  * Each x row of the group (ny rows of 32 contiguous floats, 128 B) comes
+//    in as one TMA box into a ring of DEPTH shared-memory slabs, completion
+//    on one mbarrier per slab (waits are bounded); output rows leave the
+//    same way, staged in shared memory and written by TMA stores.
+//  * The x drift is a 6-row sliding window in registers. The y drift (shift
+//    per vy, i.e. per lane) reads 13 consecutive rows of a whole row plane
+//    in shared memory: the slab itself (y first) or a double-buffered plane
+//    of x-drifted rows (x first). Slabs and planes carry 16 halo rows after
+//    row ny (copies of rows 0..15), so the periodic window never wraps.
+//  * The row loop is unrolled by DEPTH = 6 = the window length, so ring
+//    slots, buffer parities and window registers are fixed per unrolled
+//    step; pairs of y rows go through the paired FP32 FMA of sm_100.
+//  * Every element goes through the same FMA chain as in the single-axis
+//    sweep (k_strided: round(w5 g5), then fma down to tap 0) and the
+//    intermediate is kept in FP32 as that sweep stores it, so f is
+//    bit-identical to the two-sweep path.
+//  * x first runs its y drift one row behind the x drift (the plane of row
+//    k is complete at the barrier of step k), so every row costs one
+//    barrier. It can also sum each output row over its 32 columns in FP64
+//    (from the staged output, one step later still: four threads per y row,
+//    8 columns each, then two shuffles) into per-group partials of the
+//    charge density, [nx][groups][ny], reduced in a fixed order by
+//    k_rho_finalize.
+// A wait that runs out (1 s) makes the CTA wait for its stores, fill its
+// whole share of the output (and its density partials) with NaN, wait
+// (bounded) for its loads in flight and leave, so a failure shows in the
+// results.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace vp {
+namespace plane {
+
+constexpr int CG = 32;                   // columns per group (= lanes)
+constexpr int YT = 8;                    // y rows per thread
+constexpr int MAXW = 16;                 // warps per CTA
+constexpr int YMAX = MAXW * YT;          // ny <= 128
+constexpr int YMIN = 16;                 // ny >= 16: the halo copies 16 real rows
+constexpr int DEPTH = 6;                 // slabs in flight = unroll of the row loop
+constexpr int HALO = 16;                 // rows after row ny: copies of rows 0..15
+constexpr int BUF = (YMAX + HALO) * CG;  // floats per slab or plane
+constexpr int STG = YMAX * CG;           // floats per output staging buffer
+
+struct Args {
+    float* out;
+    int nx, ny, nvx, nvy;
+    int64_t m;          // columns per (x, y) point: nvx * nvy
+    int n_cg;           // column groups: m / CG
+    const int* shift_x;
+    const float* W_x;   // [6][nvx] tap weights
+    const int* shift_y;
+    const float* W_y;   // [6][nvy]
+    double* part;       // [nx][n_cg][ny] FP64 row sums (x first with the density)
+};
+
+// The rows a CTA loads. Work comes in segments (one group, output rows
+// xa .. xa+n-1), each loading the rows xa - s - 3 + q, q = 0 .. n + 4, of
+// its group (s: the group's x shift). CTA b of G first takes whole lines of
+// the groups b, b + G, b + 2G, ... (neighbouring groups then stream the same
+// x rows at the same time, so HBM sees long runs of each (x, y) point's
+// columns), then an even share of the rows of the n_cg % G groups left.
+struct Seq {
+    int w, full, b, G;  // whole-line rounds: done, total; this CTA; CTAs
+    int64_t t, t1;      // share of the remaining lines' rows
+    int cg, xa, n, q, r0;
+    __device__ __forceinline__ void init(const Args& a, int b_, int G_) {
+        b = b_;
+        G = G_;
+        full = a.n_cg / G;
+        w = 0;
+        const int64_t rest = (int64_t)(a.n_cg - full * G) * a.nx;
+        t = rest * b / G;
+        t1 = rest * (b + 1) / G;
+        if (valid()) start(a);
+    }
+    __device__ __forceinline__ void start(const Args& a) {
+        if (w < full) {
+            cg = w * G + b;
+            xa = 0;
+            n = a.nx;
+        } else {
+            cg = full * G + (int)(t / a.nx);
+            xa = (int)(t % a.nx);
+            const int64_t left = t1 - t;
+            n = (int)(left < (int64_t)(a.nx - xa) ? left : (int64_t)(a.nx - xa));
+        }
+        const int jx = (int)(((int64_t)cg * CG / a.nvy) % a.nvx);
+        r0 = xa - __ldg(a.shift_x + jx) - 3;
+        q = 0;
+    }
+    __device__ __forceinline__ bool valid() const { return w < full || t < t1; }
+    __device__ __forceinline__ int row(int nx) const {
+        const int r = (r0 + q) % nx;
+        return r < 0 ? r + nx : r;
+    }
+    __device__ __forceinline__ void next(const Args& a) {
+        if (++q == n + 5) {
+            if (w < full)
+                ++w;
+            else
+                t += n;
+            if (valid()) start(a);
+        }
+    }
+};
+
+// producer state in shared memory (only thread 0 touches it)
+struct Producer {
+    Seq seq;
+    long long issued;
+};
+
+template <int P> struct Step { static constexpr int value = P; };
+
+__device__ __forceinline__ void bar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void expect_bytes(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// box at (column c0, row r0) of the [nx*ny][m] view of f into dst
+__device__ __forceinline__ void tma_load(const CUtensorMap* tm, uint32_t dst, uint32_t bar, int c0, int r0) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(r0), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store(const CUtensorMap* tm, uint32_t src, int c0, int r0) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(tm)),
+                 "r"(c0), "r"(r0), "r"(src)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// the bulk stores issued so far have read their shared memory / are done
+__device__ __forceinline__ void stores_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void stores_done() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// mbarrier phase wait that sleeps between polls; false after ~1 s
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = now_ns();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity), "r"(20000u)
+            : "memory");
+        if (ok) return true;
+        if (now_ns() - t0 > 1000000000ull) return false;
+    }
+}
+
+// 6-tap drift of a pair of rows: round(w5 t5), then fma down to tap 0
+__device__ __forceinline__ float2 taps(const float2 (&w)[6], float2 t0, float2 t1, float2 t2, float2 t3, float2 t4,
+                                       float2 t5) {
+    float2 acc = __fmul2_rn(w[5], t5);
+    acc = __ffma2_rn(w[4], t4, acc);
+    acc = __ffma2_rn(w[3], t3, acc);
+    acc = __ffma2_rn(w[2], t2, acc);
+    acc = __ffma2_rn(w[1], t1, acc);
+    return __ffma2_rn(w[0], t0, acc);
+}
+
+// y drift of the thread's 8 rows from 13 consecutive rows of a buffer
+// (g: row y0 - s - 3 of the lane's column, halo included)
+__device__ __forceinline__ void y_drift(const float* g, const float2 (&wy)[6], float2 (&o)[YT / 2]) {
+    float r[YT + 5];
+#pragma unroll
+    for (int k = 0; k < YT + 5; ++k) r[k] = g[k * CG];
+#pragma unroll
+    for (int p = 0; p < YT / 2; ++p) {
+        const int i = 2 * p;
+        o[p] = taps(wy, make_float2(r[i], r[i + 1]), make_float2(r[i + 1], r[i + 2]), make_float2(r[i + 2], r[i + 3]),
+                    make_float2(r[i + 3], r[i + 4]), make_float2(r[i + 4], r[i + 5]), make_float2(r[i + 5], r[i + 6]));
+    }
+}
+
+// FULL: ny is a multiple of 8, every thread row is a real row
+template <bool XFIRST, bool RHO, bool FULL>
+__global__ void __launch_bounds__(MAXW * 32, 1)
+    k_plane(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap thalo,
+            const __grid_constant__ CUtensorMap tout, const __grid_constant__ Args a) {
+    static_assert(!RHO || XFIRST, "the density comes with the x-first order");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][BUF]
+    float* stage = slabs + DEPTH * BUF;             // [2][STG]
+    float* planes = stage + 2 * STG;                // [2][BUF] (x first)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(planes + (XFIRST ? 2 * BUF : 0));
+    Producer* prod = reinterpret_cast<Producer*>(bars + DEPTH);
+    const int nx = a.nx, ny = a.ny;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int y0 = warp * YT;
+    Seq cons;
+    cons.init(a, blockIdx.x, gridDim.x);
+    if (!cons.valid()) return;
+    const uint32_t slab0 = smem_u32(slabs), stage0 = smem_u32(stage), bar0 = smem_u32(bars);
+    const uint32_t in_bytes = (uint32_t)((ny + (XFIRST ? 0 : HALO)) * CG * 4);
+    // the producer's current row into slab d
+    auto issue = [&](int d, const Seq& s) {
+        const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
+        const int r = s.row(nx) * ny;
+        expect_bytes(bar, in_bytes);
+        tma_load(&tin, dst, bar, s.cg * CG, r);
+        if constexpr (!XFIRST) tma_load(&thalo, dst + (uint32_t)(ny * CG * 4), bar, s.cg * CG, r);
+    };
+    if (tid == 0) {
+        for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        Seq p = cons;
+        long long n = 0;
+        for (; n < DEPTH && p.valid(); ++n) {
+            issue((int)n, p);
+            p.next(a);
+        }
+        prod->seq = p;
+        prod->issued = n;
+    }
+    __syncthreads();
+
+    float2 win[YT / 2][6];
+#pragma unroll
+    for (int p = 0; p < YT / 2; ++p)
+#pragma unroll
+        for (int s = 0; s < 6; ++s) win[p][s] = make_float2(0.f, 0.f);
+    float2 wx[6], wy[6];
+    int yoff = 0;           // float offset of row y0 - sy - 3 (mod ny), column lane
+    uint32_t parity = 0;    // of the current pass over the ring
+    long long L = 0;        // loads consumed
+    bool pend = false;      // x first: a row waiting for its y drift
+    int pend_x = 0, pend_cg = 0;
+    bool failed = false;
+    int last = 0;
+
+    // x first: y drift of the pending row from plane PL into stage PL
+    auto y_pending = [&](auto pl) {
+        constexpr int PL = decltype(pl)::value;
+        float2 o[YT / 2];
+        y_drift(planes + PL * BUF + yoff, wy, o);
+        float* st = stage + PL * STG;
+#pragma unroll
+        for (int p = 0; p < YT / 2; ++p) {
+            const int y = y0 + 2 * p;
+            if (FULL || y < ny) st[y * CG + lane] = o[p].x;
+            if (FULL || y + 1 < ny) st[(y + 1) * CG + lane] = o[p].y;
+        }
+    };
+    // x first: density partials of row rx of group rcg from its complete
+    // stage SP (thread: y row tid / 4, columns 8 (tid % 4) .. + 7)
+    const int rrow = tid >> 2, rq = tid & 3;
+    auto rho_row = [&](auto sp, bool on, int rx, int rcg) {
+        constexpr int SP = decltype(sp)::value;
+        const float4* src = reinterpret_cast<const float4*>(stage + SP * STG + rrow * CG) + 2 * rq;
+        // odd rows read their second chunk first: neighbouring rows then
+        // never hit the same banks
+        const int odd = rrow & 1;
+        const float4 u = src[odd], v = src[1 - odd];
+        const double s = (((double)u.x + (double)u.y) + ((double)u.z + (double)u.w)) +
+                         (((double)v.x + (double)v.y) + ((double)v.z + (double)v.w));
+        double t = s + __shfl_xor_sync(0xffffffffu, s, 1);
+        t += __shfl_xor_sync(0xffffffffu, t, 2);
+        if (on && rq == 0 && rrow < ny) a.part[((int64_t)rx * a.n_cg + rcg) * ny + rrow] = t;
+    };
+    bool rho_on = false;    // x first: a stored row waiting for its density
+    int rho_x = 0, rho_cg = 0;
+
+    // the weights and y window of the consumer's current group
+    auto tables = [&]() {
+        const int jx = (int)(((int64_t)cons.cg * CG / a.nvy) % a.nvx);
+        const int jy = (int)(((int64_t)cons.cg * CG) % a.nvy) + lane;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
+            wx[j] = make_float2(u, u);
+            wy[j] = make_float2(v, v);
+        }
+        int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
+        if (r < 0) r += ny;
+        yoff = r * CG + lane;
+    };
+    tables();
+
+    auto body = [&](auto step) -> bool {
+        constexpr int P = decltype(step)::value;
+        if constexpr (XFIRST) {
+            // both unconditional (their buffers are free when nothing is
+            // pending); only the writes that leave the CTA are predicated
+            if constexpr (RHO) rho_row(Step<P & 1>{}, rho_on, rho_x, rho_cg);
+            y_pending(Step<(P + 1) & 1>{});
+        }
+        const bool ok = wait_phase(bar0 + 8 * P, parity);
+        const bool emit = cons.q >= 5;
+        const float* sl = slabs + P * BUF;
+        float2 nv[YT / 2];
+        if constexpr (XFIRST) {
+            // x drift: window slots hold loads L-5 .. L-1, the new row is L
+#pragma unroll
+            for (int p = 0; p < YT / 2; ++p)
+                nv[p] = make_float2(sl[(y0 + 2 * p) * CG + lane], sl[(y0 + 2 * p + 1) * CG + lane]);
+            {  // unconditional: a plane written without output is never read
+                float* pl = planes + (P & 1) * BUF;
+#pragma unroll
+                for (int p = 0; p < YT / 2; ++p) {
+                    const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                          win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                    const int y = y0 + 2 * p;
+                    if (FULL || y < ny) pl[y * CG + lane] = o.x;
+                    if (FULL || y + 1 < ny) pl[(y + 1) * CG + lane] = o.y;
+                    if (y0 < HALO) {  // warp-uniform: the rows copied after row ny
+                        pl[(ny + y) * CG + lane] = o.x;
+                        pl[(ny + y + 1) * CG + lane] = o.y;
+                    }
+                }
+            }
+        } else {
+            // y drift of the new row from its slab, then the x drift
+            y_drift(sl + yoff, wy, nv);
+            {  // unconditional: a stage written without output is never stored
+                float* st = stage + (P & 1) * STG;
+#pragma unroll
+                for (int p = 0; p < YT / 2; ++p) {
+                    const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                          win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                    const int y = y0 + 2 * p;
+                    if (FULL || y < ny) st[y * CG + lane] = o.x;
+                    if (FULL || y + 1 < ny) st[(y + 1) * CG + lane] = o.y;
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < YT / 2; ++p) win[p][P] = nv[p];
+        // staged rows become visible to the TMA store; the previous store
+        // has read its stage before that buffer is written again
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (tid == 0) stores_read();
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            return false;
+        }
+        if (P == DEPTH - 1) parity ^= 1u;
+        ++L;
+        if (tid == 0) {
+            if constexpr (XFIRST) {
+                if (pend) tma_store(&tout, stage0 + (uint32_t)(((P + 1) & 1) * STG * 4), pend_cg * CG, pend_x * ny);
+            } else {
+                if (emit)
+                    tma_store(&tout, stage0 + (uint32_t)((P & 1) * STG * 4), cons.cg * CG,
+                              (cons.xa + cons.q - 5) * ny);
+            }
+            Seq& p = prod->seq;
+            if (p.valid()) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue(P, p);
+                p.next(a);
+                prod->issued += 1;
+            }
+        }
+        if constexpr (XFIRST) {
+            rho_on = pend;
+            rho_x = pend_x;
+            rho_cg = pend_cg;
+            pend = emit;
+            pend_x = cons.xa + cons.q - 5;
+            pend_cg = cons.cg;
+        }
+        cons.next(a);
+        last = P;
+        // a new group: its tables after the pending row of the last one
+        // went through (x first: one step into the group, before any
+        // output row; y first: before its first row)
+        if (cons.valid() && cons.q == (XFIRST ? 1 : 0)) tables();
+        return cons.valid();
+    };
+
+    while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
+           body(Step<5>{})) {
+    }
+
+    if constexpr (XFIRST) {
+        if (!failed) {
+            // the rows still in the pipeline: the density of the row stored
+            // at the last step, then the last row (its plane is complete)
+            if (RHO) {
+                if (last & 1)
+                    rho_row(Step<0>{}, rho_on, rho_x, rho_cg);
+                else
+                    rho_row(Step<1>{}, rho_on, rho_x, rho_cg);
+            }
+            if (pend) {
+                if (last & 1)
+                    y_pending(Step<1>{});
+                else
+                    y_pending(Step<0>{});
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (tid == 0) stores_read();
+                __syncthreads();
+                if (tid == 0) tma_store(&tout, stage0 + (uint32_t)((last & 1) * STG * 4), pend_cg * CG, pend_x * ny);
+                if (RHO) {
+                    if (last & 1)
+                        rho_row(Step<1>{}, true, pend_x, pend_cg);
+                    else
+                        rho_row(Step<0>{}, true, pend_x, pend_cg);
+                }
+            }
+        }
+    }
+    if (tid == 0) stores_done();
+    if (failed) {
+        // no store lands after this point: the whole share reads NaN, then
+        // the loads in flight land
+        __syncthreads();
+        Seq z;
+        z.init(a, blockIdx.x, gridDim.x);
+        while (z.valid()) {
+            if (z.q >= 5) {
+                const int x = z.xa + z.q - 5;
+                for (int i = 0; i < YT && y0 + i < ny; ++i) {
+                    a.out[((int64_t)x * ny + y0 + i) * a.m + (int64_t)z.cg * CG + lane] = NAN;
+                    if (RHO && lane == 0) a.part[((int64_t)x * a.n_cg + z.cg) * ny + y0 + i] = (double)NAN;
+                }
+            }
+            z.next(a);
+        }
+        if (tid == 0)
+            for (long long k = L; k < prod->issued; ++k)
+                wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+    }
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once
+static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// [nx*ny][m] FP32 view of f with a {CG, rows} box
+static bool make_map(CUtensorMap* tm, const void* base, int64_t m, int64_t rows_total, int box_rows) {
+    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)rows_total};
+    const cuuint64_t strides[1] = {(cuuint64_t)(m * sizeof(float))};
+    const cuuint32_t box[2] = {(cuuint32_t)CG, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encoder()(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static constexpr size_t smem_bytes(bool xfirst) {
+    return (size_t)(DEPTH * BUF + 2 * STG + (xfirst ? 2 * BUF : 0)) * 4 + DEPTH * 8 + sizeof(Producer);
+}
+
+template <bool XFIRST, bool RHO, bool FULL>
+static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUtensorMap& tout, const Args& a,
+                    cudaStream_t st) {
+    auto kern = k_plane<XFIRST, RHO, FULL>;
+    constexpr size_t smem = smem_bytes(XFIRST);
+    const int block = 32 * ((a.ny + YT - 1) / YT);
+    static int raised[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(VP_ERR_CUDA, "run_plane: device index out of range");
+    if (!raised[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return set_cuda_error("cudaFuncSetAttribute(k_plane)");
+        raised[dev] = 1;
+    }
+    const int occ = occupancy(kern, block, smem);
+    const int64_t total = (int64_t)a.n_cg * a.nx;
+    const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
+    kern<<<(unsigned)grid, block, smem, st>>>(tin, thalo, tout, a);
+    return check_launch("k_plane");
+}
+
+}  // namespace plane
+
+bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* f) {
+    using namespace plane;
+    if (dtype != VP_F32) return false;
+    if (ny < YMIN || ny > YMAX || nvy % CG != 0 || nvx < 1 || nx < 1) return false;
+    if ((int64_t)nx * ny >= (1ll << 31) || nvx * nvy >= (1ll << 31)) return false;
+    if (reinterpret_cast<uintptr_t>(f) % 16 != 0) return false;
+    return encoder() != nullptr;
+}
+
+int64_t plane_part_tiles(int64_t nvx, int64_t nvy) { return nvx * nvy / plane::CG; }
+
+int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
+              const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
+              cudaStream_t st) {
+    using namespace plane;
+    if (!plane_fits(dtype, nx, ny, nvx, nvy, in) || !plane_fits(dtype, nx, ny, nvx, nvy, out))
+        return set_error(VP_ERR_UNSUPPORTED, "run_plane: layout not fused");
+    Args a{};
+    a.out = static_cast<float*>(out);
+    a.nx = (int)nx;
+    a.ny = (int)ny;
+    a.nvx = (int)nvx;
+    a.nvy = (int)nvy;
+    a.m = nvx * nvy;
+    a.n_cg = (int)(a.m / CG);
+    a.shift_x = shift_x;
+    a.W_x = static_cast<const float*>(W_x);
+    a.shift_y = shift_y;
+    a.W_y = static_cast<const float*>(W_y);
+    a.part = part;
+    if (tiles) *tiles = a.n_cg;
+    CUtensorMap tin, thalo, tout;
+    if (!make_map(&tin, in, a.m, nx * ny, (int)ny) || !make_map(&thalo, in, a.m, nx * ny, HALO) ||
+        !make_map(&tout, out, a.m, nx * ny, (int)ny))
+        return set_error(VP_ERR_CUDA, "run_plane: cuTensorMapEncodeTiled failed");
+    const bool full = ny % YT == 0;
+    if (xfirst) {
+        if (part)
+            return full ? launch_t<true, true, true>(tin, thalo, tout, a, st)
+                        : launch_t<true, true, false>(tin, thalo, tout, a, st);
+        return full ? launch_t<true, false, true>(tin, thalo, tout, a, st)
+                    : launch_t<true, false, false>(tin, thalo, tout, a, st);
+    }
+    return full ? launch_t<false, false, true>(tin, thalo, tout, a, st)
+                : launch_t<false, false, false>(tin, thalo, tout, a, st);
+}
+
+}  // namespace vp

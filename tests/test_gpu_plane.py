@@ -1,0 +1,55 @@
+"""The fused (x, y) drift passes of the 2D2V step against the single-axis
+sweeps: f bit for bit, the charge density to FP64 summation order."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+# (Nx, Ny, Nvx, Nvy): Ny not a multiple of 8, Ny = 1, Nx below the stencil
+# width, groups of 32 columns inside wider vy rows, the 128-row maximum
+SHAPES = [(16, 16, 32, 32), (8, 6, 16, 64), (12, 100, 4, 32), (5, 3, 2, 32), (33, 128, 8, 64), (7, 1, 3, 32),
+          (64, 128, 16, 128)]
+
+
+def seeded(shape, seed):
+    g = np.random.default_rng(seed)
+    return torch.from_numpy(1.0 + 0.25 * g.standard_normal(shape)).float().cuda()
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("dt", [0.1, 1.3])
+def test_plane_pairs_equal_sweeps(vp, shape, dt):
+    Nx, Ny, Nvx, Nvy = shape
+    st = vp.Stepper2D(Nx, Ny, Nvx, Nvy, 4 * math.pi, 3.0, 6.0, 5.0, dt, dtype=torch.float32, physics_mode=False)
+    f = seeded(shape, 7)
+    got = st.step(f)
+    a = vp.ops.drift(f, st.tx, 0, 2)
+    b = vp.ops.drift(a, st.ty, 1, 3)
+    c = vp.ops.drift(b, st.ty, 1, 3)
+    want = vp.ops.drift(c, st.tx, 0, 2)
+    assert torch.equal(got, want)
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 32, 32), (12, 100, 4, 32), (64, 128, 16, 128)])
+def test_plane_density(vp, shape):
+    Nx, Ny, Nvx, Nvy = shape
+    st = vp.Stepper2D(Nx, Ny, Nvx, Nvy, 4 * math.pi, 3.0, 6.0, 5.0, 0.4, dtype=torch.float32, physics_mode=True)
+    f = seeded(shape, 11)
+    st.step(f)
+    a = vp.ops.drift(f, st.tx, 0, 2)
+    _, rho = vp.ops.drift_rho(a, st.ty, 1, 3, st.dvx * st.dvy)
+    np.testing.assert_allclose(st.drho.cpu().numpy(), rho.cpu().numpy() - 1.0, rtol=0, atol=1e-12)
+
+
+def test_plane_graph_replay(vp):
+    """Captured steps (the TMA descriptors live in the kernel parameters)
+    replay to the eager result."""
+    shape = (32, 64, 8, 64)
+    st = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.2, dtype=torch.float32)
+    f = seeded(shape, 3)
+    fa = st.run(f.clone(), 12, graph=False)
+    fb = st.run(f.clone(), 12, graph=True, graph_chunk=4)
+    assert torch.equal(fa, fb)
