@@ -30,7 +30,7 @@
 //    (from the staged output, one step later still: four threads per y row,
 //    8 columns each, then two shuffles) into per-group partials of the
 //    charge density, [nx][groups][ny], reduced in a fixed order by
-//    k_rho_finalize.
+//    k_rho_finalize_wide.
 // A wait that runs out (1 s) makes the CTA wait for its stores, fill its
 // whole share of the output (and its density partials) with NaN, wait
 // (bounded) for its loads in flight and leave, so a failure shows in the

@@ -445,9 +445,48 @@ int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n
     return launch_strided<false, false, false>(dtype, a, vec, nt, sms, st);
 }
 
+// The same sum for many tiles (the fused plane pass writes one partial per
+// 32 columns): block (32 lines, 8 slices); slice s adds the tiles
+// t = s (mod 8) with four running sums (t = s, s+8, s+16, s+24 mod 32),
+// then the 8 slices are added in order. Fixed order, so deterministic.
+__global__ void __launch_bounds__(256) k_rho_finalize_wide(const double* __restrict__ part, int n_line, int tiles,
+                                                           double scale, double offset, double* __restrict__ rho) {
+    __shared__ double sl[8][33];
+    const int l = blockIdx.x * 32 + threadIdx.x;
+    const int64_t o = blockIdx.y;
+    const int sidx = threadIdx.y;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (l < n_line) {
+        const double* p = part + (o * tiles) * (int64_t)n_line + l;
+        int t = sidx;
+        for (; t + 24 < tiles; t += 32) {
+            a0 += p[(int64_t)t * n_line];
+            a1 += p[(int64_t)(t + 8) * n_line];
+            a2 += p[(int64_t)(t + 16) * n_line];
+            a3 += p[(int64_t)(t + 24) * n_line];
+        }
+        if (t < tiles) a0 += p[(int64_t)t * n_line];
+        if (t + 8 < tiles) a1 += p[(int64_t)(t + 8) * n_line];
+        if (t + 16 < tiles) a2 += p[(int64_t)(t + 16) * n_line];
+    }
+    sl[sidx][threadIdx.x] = (a0 + a1) + (a2 + a3);
+    __syncthreads();
+    if (sidx == 0 && l < n_line) {
+        double acc = sl[0][threadIdx.x];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) acc += sl[k][threadIdx.x];
+        rho[o * n_line + l] = acc * scale + offset;
+    }
+}
+
 int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int tiles, double scale, double offset,
                      double* rho,
                      cudaStream_t st) {
+    if (tiles > 32 && n_outer <= 65535) {
+        const dim3 grid((unsigned)((n_line + 31) / 32), (unsigned)n_outer);
+        k_rho_finalize_wide<<<grid, dim3(32, 8), 0, st>>>(part, (int)n_line, tiles, scale, offset, rho);
+        return check_launch("k_rho_finalize_wide");
+    }
     const int64_t total = n_outer * n_line;
     k_rho_finalize<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, n_outer, (int)n_line, tiles, scale, offset,
                                                                       rho);
