@@ -256,10 +256,22 @@ typedef struct vp_step2d_desc {
     const double* eq_vx;
     const double* eq_vy;
     double eq_moment;
+    /* nonzero: the position drifts run as one sweep per axis even where the
+     * fused (x, y) plane passes apply; f is the same either way, the
+     * density then also has the single-axis sweeps' summation order. */
+    int32_t sweeps_only;
 } vp_step2d_desc;
 
 int vp_step2d(const vp_step2d_desc* desc, void* stream);
 size_t vp_step2d_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy);
+/* How vp_step2d runs this descriptor, without GPU work: returns the number
+ * of passes over f (each reads and writes f once; < 0 on a bad descriptor)
+ * and sets *plane_fused (may be NULL) to 1 when the position drifts go in
+ * pairs through the fused (x, y) plane passes (FP32 storage, 16 <= ny <=
+ * 128, nvy a multiple of 32, 16-byte aligned buffers, no equilibrium
+ * split). No counterpart in the reference, whose drifts are separate tensor
+ * operations; it tells a caller how much HBM traffic one step moves. */
+int vp_step2d_passes(const vp_step2d_desc* desc, int32_t* plane_fused);
 
 /* One Strang step of the 1D1V system, the schedule of
  * vlasov_step_gather_free_impl (vlasov1D1V.py:668-701): x(dt/2) fused with

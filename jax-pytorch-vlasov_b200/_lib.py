@@ -55,6 +55,7 @@ class Step2dDesc(ctypes.Structure):
         ("drho", P), ("phi", P), ("ex", P), ("ey", P), ("diag", P),
         ("workspace", P), ("workspace_bytes", SZ), ("events", P),
         ("eq_vx", P), ("eq_vy", P), ("eq_moment", D),
+        ("sweeps_only", I32),
     ]
 
 
@@ -112,6 +113,7 @@ SIGNATURES = {
     "vp_poisson1d": (ctypes.c_int, [P, I64, P, P, D, P, P, P, P, P, SZ, P]),
     "vp_poisson1d_workspace_bytes": (SZ, [I64]),
     "vp_step2d": (ctypes.c_int, [ctypes.POINTER(Step2dDesc), P]),
+    "vp_step2d_passes": (ctypes.c_int, [ctypes.POINTER(Step2dDesc), P]),
     "vp_batch2d_table_bytes": (SZ, [I32]),
     "vp_batch2d_plan": (ctypes.c_int, [I32, I32, I32, ctypes.POINTER(BatchRun), I32, ctypes.POINTER(BatchTiles), P,
                                        SZ]),

@@ -299,6 +299,24 @@ size_t vp_step2d_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nv
     return step2d_layout(nx, ny, nvx, nvy, nullptr, nullptr);
 }
 
+// the position drifts go through the fused (x, y) plane passes
+static bool step2d_planar(const vp_step2d_desc* d) {
+    const bool eq_on = d->eq_vx || d->eq_vy;
+    return !eq_on && !d->sweeps_only && plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_in) &&
+           plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_out) &&
+           plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_tmp);
+}
+
+int vp_step2d_passes(const vp_step2d_desc* d, int32_t* plane_fused) {
+    VP_CHECK(d, "vp_step2d_passes: null descriptor");
+    if (!dtype_ok(d->dtype)) return set_error(VP_ERR_DTYPE, "vp_step2d_passes: unknown dtype");
+    const bool phys = d->physics_mode != 0;
+    const bool fused = kick2d_fits(d->dtype, d->nvy, d->f_in, d->f_out, d->f_tmp);
+    const bool planar = step2d_planar(d);
+    if (plane_fused) *plane_fused = planar ? 1 : 0;
+    return (phys ? (fused ? 1 : 2) : 0) + (planar ? 2 : 4);
+}
+
 int vp_step2d(const vp_step2d_desc* d, void* stream) {
     VP_CHECK(d, "vp_step2d: null descriptor");
     if (!dtype_ok(d->dtype)) return set_error(VP_ERR_DTYPE, "vp_step2d: unknown dtype");
@@ -333,9 +351,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     // allows (one pass over f each, intermediate on chip, bit-identical);
     // otherwise one sweep per axis. The fused passes are timed under the x
     // phases, the y phases then stay empty.
-    const bool planar = !eq_on && plane_fits(d->dtype, nx, ny, nvx, nvy, d->f_in) &&
-                        plane_fits(d->dtype, nx, ny, nvx, nvy, d->f_out) &&
-                        plane_fits(d->dtype, nx, ny, nvx, nvy, d->f_tmp);
+    const bool planar = step2d_planar(d);
     const int n_sweeps = (phys ? (fused ? 3 : 4) : 2) + (planar ? 0 : 2);
     int i = 0;
     auto dst_of = [&](int k) -> void* { return ((n_sweeps - 1 - k) % 2 == 0) ? d->f_out : d->f_tmp; };

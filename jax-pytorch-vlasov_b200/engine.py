@@ -160,9 +160,12 @@ class Stepper2D(_Stepper):
 
     def __init__(self, Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt, dtype=torch.float32, device="cuda",
                  physics_mode=True, window=-1, diagnostics=1, vx=None, vy=None, equilibrium=None,
-                 precise_tables=False):
+                 precise_tables=False, fuse_drifts=True):
         self._init_common(dtype, device, physics_mode, window, diagnostics)
         self.shape = (int(Nx), int(Ny), int(Nvx), int(Nvy))
+        # False: one sweep per axis even where the fused (x, y) plane passes
+        # apply (same f; the density keeps the single-axis summation order)
+        self.fuse_drifts = bool(fuse_drifts)
         self.Lx, self.Ly = float(Lx), float(Ly)
         self.dx, self.dy = self.Lx / Nx, self.Ly / Ny
         grid_dt = torch.float64 if (dtype == torch.float64 or precise_tables) else torch.float32
@@ -190,6 +193,18 @@ class Stepper2D(_Stepper):
         # split storage f = A(vx) B(vy) + g: the state buffers hold g
         self._set_equilibrium(equilibrium, (self.dvx, self.dvy))
 
+    def passes(self, f_in: torch.Tensor, f_out: torch.Tensor) -> tuple[int, bool]:
+        """How step(f_in, f_out) runs: (passes over f, whether the position
+        drifts go in pairs through the fused (x, y) plane passes)."""
+        self._check(f_in)
+        self._check(f_out)
+        d = self._desc(f_in, f_out, None)
+        flag = ctypes.c_int32(0)
+        n = L.load().vp_step2d_passes(ctypes.byref(d), ctypes.byref(flag))
+        if n < 0:
+            raise L.VlasovError("vp_step2d_passes: " + L.load().vp_last_error().decode(errors="replace"))
+        return int(n), bool(flag.value)
+
     def _desc(self, f_in, f_out, diag) -> L.Step2dDesc:
         d = L.Step2dDesc()
         d.dtype = L.dtype_code(self.dtype)
@@ -211,6 +226,7 @@ class Stepper2D(_Stepper):
         if self.eq is not None:
             d.eq_vx, d.eq_vy = self.eq[0].data_ptr(), self.eq[1].data_ptr()
             d.eq_moment = self.eq_moment
+        d.sweeps_only = 0 if getattr(self, "fuse_drifts", True) else 1
         return d
 
 

@@ -53,3 +53,32 @@ def test_plane_graph_replay(vp):
     fa = st.run(f.clone(), 12, graph=False)
     fb = st.run(f.clone(), 12, graph=True, graph_chunk=4)
     assert torch.equal(fa, fb)
+
+
+@pytest.mark.parametrize("dtype,physics,want", [(torch.float32, True, (3, True)), (torch.float32, False, (2, True)),
+                                                (torch.float64, True, (5, False)), (torch.bfloat16, True, (5, False))])
+def test_step_passes(vp, dtype, physics, want):
+    """vp_step2d_passes: passes over f and whether the drifts are fused."""
+    shape = (16, 16, 32, 32)
+    st = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1, dtype=dtype, physics_mode=physics)
+    f = st.empty_f()
+    assert st.passes(f, st.empty_f()) == want
+    # ny above 128, or fusion turned off, keeps the single-axis sweeps
+    wide = vp.Stepper2D(4, 136, 2, 32, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1, dtype=torch.float32)
+    assert wide.passes(wide.empty_f(), wide.empty_f()) == (3 + 2, False)
+    off = vp.Stepper2D(*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.1, dtype=dtype, physics_mode=physics,
+                       fuse_drifts=False)
+    assert off.passes(f, off.empty_f()) == (want[0] + (2 if want[1] else 0), False)
+
+
+def test_fused_and_sweeps_only_steps(vp):
+    """Fused and single-axis drifts give the same f and density to FP64
+    summation order over a physics step."""
+    shape = (16, 32, 8, 64)
+    args = (*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.3)
+    a = vp.Stepper2D(*args, dtype=torch.float32)
+    b = vp.Stepper2D(*args, dtype=torch.float32, fuse_drifts=False)
+    f = seeded(shape, 5)
+    fa, fb = a.step(f), b.step(f)
+    np.testing.assert_allclose(a.drho.cpu().numpy(), b.drho.cpu().numpy(), rtol=0, atol=1e-13)
+    np.testing.assert_allclose(fa.cpu().numpy(), fb.cpu().numpy(), rtol=0, atol=1e-6)
