@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweeps-only", action="store_true",
+                    help="2D2V: one sweep per axis even where the fused (x, y) plane passes apply")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for cpu_baseline")
     ap.add_argument("--train-ics", type=int, default=125, help="learned workload: training initial conditions")
     ap.add_argument("--train-iters", type=int, default=1500, help="learned workload: Adam steps")
@@ -311,7 +313,7 @@ def run_ours(a):
         n_sweeps = 3
     else:
         st = vp.Stepper2D(*a.grid, a.L, a.L, a.vmax, a.vmax, a.dt, dtype=dtype, device=dev, window=1,
-                          diagnostics=a.diagnostics)
+                          diagnostics=a.diagnostics, fuse_drifts=not a.sweeps_only)
     f = _initial_f(a, dev, dtype, rank, torch)
     b = st.empty_f()
     planar = False

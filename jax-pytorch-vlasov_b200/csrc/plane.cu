@@ -54,8 +54,10 @@ constexpr int YMAX = MAXW * YT;          // ny <= 128
 constexpr int YMIN = 16;                 // ny >= 16: the halo copies 16 real rows
 constexpr int DEPTH = 6;                 // slabs in flight = unroll of the row loop
 constexpr int HALO = 16;                 // rows after row ny: copies of rows 0..15
-constexpr int BUF = (YMAX + HALO) * CG;  // floats per slab or plane
-constexpr int STG = YMAX * CG;           // floats per output staging buffer
+// floats per slab or plane, and per output staging buffer, of a kernel
+// built for at most ym rows (64 or 128: two CTAs or one per SM)
+__host__ __device__ constexpr int buf_floats(int ym) { return (ym + HALO) * CG; }
+__host__ __device__ constexpr int stage_floats(int ym) { return ym * CG; }
 
 struct Args {
     float* out;
@@ -198,12 +200,15 @@ __device__ __forceinline__ void y_drift(const float* g, const float2 (&wy)[6], f
     }
 }
 
-// FULL: ny is a multiple of 8, every thread row is a real row
-template <bool XFIRST, bool RHO, bool FULL>
-__global__ void __launch_bounds__(MAXW * 32, 1)
+// FULL: ny is a multiple of 8, every thread row is a real row.
+// YM: the most rows the buffers hold (ny <= YM); 64 halves the shared memory
+// so that two CTAs share an SM.
+template <bool XFIRST, bool RHO, bool FULL, int YM>
+__global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     k_plane(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap thalo,
             const __grid_constant__ CUtensorMap tout, const __grid_constant__ Args a) {
     static_assert(!RHO || XFIRST, "the density comes with the x-first order");
+    constexpr int BUF = buf_floats(YM), STG = stage_floats(YM);
     extern __shared__ __align__(1024) unsigned char smem[];
     float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][BUF]
     float* stage = slabs + DEPTH * BUF;             // [2][STG]
@@ -478,15 +483,16 @@ static bool make_map(CUtensorMap* tm, const void* base, int64_t m, int64_t rows_
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-static constexpr size_t smem_bytes(bool xfirst) {
-    return (size_t)(DEPTH * BUF + 2 * STG + (xfirst ? 2 * BUF : 0)) * 4 + DEPTH * 8 + sizeof(Producer);
+static constexpr size_t smem_bytes(bool xfirst, int ym) {
+    return (size_t)(DEPTH * buf_floats(ym) + 2 * stage_floats(ym) + (xfirst ? 2 * buf_floats(ym) : 0)) * 4 +
+           DEPTH * 8 + sizeof(Producer);
 }
 
-template <bool XFIRST, bool RHO, bool FULL>
+template <bool XFIRST, bool RHO, bool FULL, int YM>
 static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUtensorMap& tout, const Args& a,
                     cudaStream_t st) {
-    auto kern = k_plane<XFIRST, RHO, FULL>;
-    constexpr size_t smem = smem_bytes(XFIRST);
+    auto kern = k_plane<XFIRST, RHO, FULL, YM>;
+    constexpr size_t smem = smem_bytes(XFIRST, YM);
     const int block = 32 * ((a.ny + YT - 1) / YT);
     static int raised[64] = {0};
     int dev = 0;
@@ -542,15 +548,19 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
         !make_map(&tout, out, a.m, nx * ny, (int)ny))
         return set_error(VP_ERR_CUDA, "run_plane: cuTensorMapEncodeTiled failed");
     const bool full = ny % YT == 0;
-    if (xfirst) {
-        if (part)
-            return full ? launch_t<true, true, true>(tin, thalo, tout, a, st)
-                        : launch_t<true, true, false>(tin, thalo, tout, a, st);
-        return full ? launch_t<true, false, true>(tin, thalo, tout, a, st)
-                    : launch_t<true, false, false>(tin, thalo, tout, a, st);
-    }
-    return full ? launch_t<false, false, true>(tin, thalo, tout, a, st)
-                : launch_t<false, false, false>(tin, thalo, tout, a, st);
+    auto go = [&](auto ym) {
+        constexpr int YM = decltype(ym)::value;
+        if (xfirst) {
+            if (part)
+                return full ? launch_t<true, true, true, YM>(tin, thalo, tout, a, st)
+                            : launch_t<true, true, false, YM>(tin, thalo, tout, a, st);
+            return full ? launch_t<true, false, true, YM>(tin, thalo, tout, a, st)
+                        : launch_t<true, false, false, YM>(tin, thalo, tout, a, st);
+        }
+        return full ? launch_t<false, false, true, YM>(tin, thalo, tout, a, st)
+                    : launch_t<false, false, false, YM>(tin, thalo, tout, a, st);
+    };
+    return ny <= YMAX / 2 ? go(Step<YMAX / 2>{}) : go(Step<YMAX>{});
 }
 
 }  // namespace vp
