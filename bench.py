@@ -279,8 +279,9 @@ def _initial_f(a, dev, dtype, rank, torch):
         nx, nv = a.grid
         x = torch.linspace(0, a.L, nx + 1, dtype=gdt, device=dev)[:-1]
         v = torch.linspace(-a.vmax, a.vmax, nv, dtype=gdt, device=dev)
-        f = (1.0 + eps * torch.cos(a.icp[1] * x))[:, None] * torch.exp(-0.5 * v * v)[None, :] / math.sqrt(2 * math.pi)
-        return f.to(dtype).contiguous()
+        ops = importlib.import_module("jax-pytorch-vlasov_b200.ops")
+        return ops.init_product(1.0 + eps * torch.cos(a.icp[1] * x), torch.exp(-0.5 * v * v) / math.sqrt(2 * math.pi),
+                                dtype)
     n, _, nv, _ = a.grid
     x = torch.linspace(0, a.L, n + 1, dtype=gdt, device=dev)[:-1]
     v = torch.linspace(-a.vmax, a.vmax, nv, dtype=gdt, device=dev)
@@ -291,7 +292,8 @@ def _initial_f(a, dev, dtype, rank, torch):
         fv = M(v)[:, None] * M(v)[None, :]
     else:
         fv = (0.5 * (M(v - a.icp[2]) + M(v + a.icp[2])))[:, None] * M(v)[None, :]
-    return (sp.float()[:, :, None, None] * fv.float()[None, None]).to(dtype).contiguous()
+    # one FP64 product per element, rounded once (the library's IC kernel)
+    return importlib.import_module("jax-pytorch-vlasov_b200.ops").init_product(sp, fv, dtype)
 
 
 def run_ours(a):

@@ -120,6 +120,18 @@ int vp_advect_gather(const void* f_in, void* f_out, int dtype, int64_t n_outer, 
                      int64_t n_inner, const void* vel, int64_t vs_outer, int64_t vs_line,
                      int64_t vs_inner, double dt, double dx, int periodic, void* stream);
 
+/* ---- initial conditions ---------------------------------------------------- */
+
+/* f[p][v] = space[p] * vel[v] for p < n_points, v < n_v (f row-major,
+ * space and vel FP64 on the device), the product rounded once to dtype: the
+ * initial conditions of Vlasov.initialize (vlasov2D2V.py:1319-1355, Landau:
+ * space = 1 + eps cos(kx x) cos(ky y), vel = exp(-|v|^2/2)/sqrt(2 pi);
+ * vlasov1D1V.py:881-911), which the reference builds as a broadcast tensor
+ * product; the result has the same bits as that product rounded by
+ * .to(dtype). */
+int vp_init_product(const double* space, const double* vel, void* f, int dtype, int64_t n_points, int64_t n_v,
+                    void* stream);
+
 /* ---- interpolation helpers ---------------------------------------------- */
 
 /* The 6-point Lagrange sum of lagrange5_interp_sum (vlasov2D2V.py:238-260;

@@ -106,6 +106,7 @@ SIGNATURES = {
     "vp_advect_gather": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, P, I64, I64, I64, D, D, ctypes.c_int, P]),
     "vp_rho": (ctypes.c_int, [P, ctypes.c_int, I64, I64, D, D, P, ctypes.c_int, P]),
     "vp_lagrange_interp": (ctypes.c_int, [P, P, P, ctypes.c_int, I64, P]),
+    "vp_init_product": (ctypes.c_int, [P, P, P, ctypes.c_int, I64, I64, P]),
     "vp_lagrange_weights": (ctypes.c_int, [P, P, ctypes.c_int, I64, P]),
     "vp_poisson2d": (ctypes.c_int, [P, I64, I64, P, P, P, D, D, P, P, P, P, P, P, SZ, P]),
     "vp_poisson2d_workspace_bytes": (SZ, [I64, I64]),

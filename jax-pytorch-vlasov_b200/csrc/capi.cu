@@ -254,6 +254,15 @@ int vp_lagrange_weights(const void* alpha, void* weights, int dtype, int64_t n, 
     return run_lagrange(dtype, alpha, nullptr, weights, n, 1, S(stream));
 }
 
+int vp_init_product(const double* space, const double* vel, void* f, int dtype, int64_t n_points, int64_t n_v,
+                    void* stream) {
+    if (!dtype_ok(dtype)) return set_error(VP_ERR_DTYPE, "vp_init_product: unknown dtype");
+    VP_CHECK(n_points >= 0 && n_v >= 0, "vp_init_product: negative size");
+    if (n_points == 0 || n_v == 0) return VP_OK;
+    VP_CHECK(space && vel && f, "vp_init_product: null pointer");
+    return run_init_product(dtype, space, vel, f, n_points, n_v, S(stream));
+}
+
 size_t vp_poisson2d_workspace_bytes(int64_t nx, int64_t ny) { return poisson2d_ws_bytes(nx, ny); }
 
 int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,

@@ -146,6 +146,9 @@ bool kick2d_fits(int dtype, int64_t nvy, const void* a, const void* b, const voi
 // Both position drifts of f[nx][ny][nvx][nvy] in one pass (x then y, or y
 // then x), with the density row sums of x-then-y into part
 // ([nx][plane_part_tiles][ny], tiles returned) when part is not null.
+// f[p][v] = S[p] * V[v] (FP64 product, rounded once to the storage type)
+int run_init_product(int dtype, const double* S, const double* V, void* f, int64_t n_points, int64_t n_v,
+                     cudaStream_t st);
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* in);
 int64_t plane_part_tiles(int64_t nvx, int64_t nvy);
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,

@@ -187,6 +187,20 @@ def advect_gather(f: torch.Tensor, vel: torch.Tensor, axis: int, dt: float, dx: 
     return out
 
 
+def init_product(space: torch.Tensor, vel: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
+    """f = space (x) vel: shape space.shape + vel.shape, each element the FP64
+    product space[p] * vel[v] rounded once to dtype (the drivers' initial
+    conditions, vlasov2D2V.py:1319-1355; the same bits as
+    (space[..., None] * vel).to(dtype))."""
+    L.require_cuda(space)
+    s = space.to(torch.float64).contiguous()
+    v = vel.to(device=space.device, dtype=torch.float64).contiguous()
+    f = torch.empty(tuple(space.shape) + tuple(vel.shape), dtype=dtype, device=space.device)
+    L.call("vp_init_product", L.ptr(s), L.ptr(v), L.ptr(f), L.dtype_code(dtype), s.numel(), v.numel(),
+           L.stream_of(f))
+    return f
+
+
 def velocity_moment(f: torch.Tensor, dvx: float, dvy: float, n_v_dims: int, out_dtype=torch.float64):
     """sum over the trailing n_v_dims dims, times dvx*dvy (FP64 accumulation)."""
     L.require_cuda(f)

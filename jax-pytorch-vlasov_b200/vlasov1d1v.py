@@ -287,7 +287,8 @@ class Vlasov:
         v = g.v.double()[None, :]
         if self.physics_mode:
             maxw = (1.0 / math.sqrt(2.0 * math.pi)) * torch.exp(-0.5 * v ** 2)
-            f = (1.0 + self.epsilon * torch.cos(2.0 * math.pi / g.L * x)) * maxw
+            f = ops.init_product((1.0 + self.epsilon * torch.cos(2.0 * math.pi / g.L * x))[:, 0], maxw[0],
+                                 self.dtype)
             f0 = maxw.squeeze(0)
         else:
             sx, sv = g.L / 10.0, g.V_max / 4.0

@@ -480,7 +480,8 @@ class Vlasov:
         if self.physics_mode:
             kxm, kym = 2.0 * math.pi / g.Lx, 2.0 * math.pi / g.Ly
             f0 = (1.0 / math.sqrt(2.0 * math.pi)) * torch.exp(-0.5 * (vx ** 2 + vy ** 2))
-            f = (1.0 + self.epsilon * torch.cos(kxm * x) * torch.cos(kym * y)) * f0[None, None]
+            space = (1.0 + self.epsilon * torch.cos(kxm * x) * torch.cos(kym * y))[:, :, 0, 0]
+            f = ops.init_product(space, f0, self.dtype)
         else:
             sx, sv = g.Lx / 10.0, g.Vx_max / 4.0
             f = torch.exp(-0.5 * ((x - g.Lx / 2) ** 2 / sx ** 2 + (y - g.Ly / 2) ** 2 / sx ** 2

@@ -15,6 +15,8 @@ import math
 import numpy as np
 import torch
 
+from . import ops
+
 # draws of the batched configuration (64 runs of uneven size)
 BATCH_SEED = 20261203
 BATCH_NX = (16, 24, 32, 48, 64)
@@ -46,8 +48,8 @@ def initial_2d(kind: str, Nx: int, Ny: int, Nvx: int, Nvy: int, Lx: float, Ly: f
     vy = torch.linspace(-Vy_max, Vy_max, Nvy, dtype=torch.float64, device=device)
     sp = 1.0 + eps * (torch.cos(k * x)[:, None] + torch.cos(k * y)[None, :])
     A, B = velocity_factors(kind, vx, vy, v0)
-    f = sp[:, :, None, None] * (A[:, None] * B[None, :])[None, None]
-    return f.to(dtype).contiguous()
+    # the product sp (x) (A B) in FP64, rounded once, in one write of f
+    return ops.init_product(sp, A[:, None] * B[None, :], dtype)
 
 
 def batch_runs(n: int = 64, seed: int = BATCH_SEED, dt: float = 0.05) -> list[dict]:

@@ -233,3 +233,36 @@ def test_fused_step_returns_fresh_fields(v1, v2, dt):
     s2, r2, p2 = v1.vlasov_step_gather_free(s1, *a1)
     assert r1.data_ptr() != r2.data_ptr() and p1.data_ptr() != p2.data_ptr()
     assert torch.equal(r1, keep[0]) and torch.equal(p1, keep[1])
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32, torch.bfloat16])
+@pytest.mark.parametrize("shape", [((8, 6), (10, 12)), ((33,), (17,)), ((4, 4), (3, 5)), ((0, 3), (4, 4))])
+def test_init_product(vp, dt, shape):
+    """vp_init_product: the same bits as torch's broadcast product rounded
+    by .to(dtype), vectorised (v a multiple of 4) and scalar paths."""
+    g = np.random.default_rng(9)
+    space = torch.from_numpy(1.0 + 0.1 * g.standard_normal(shape[0])).cuda()
+    vel = torch.from_numpy(np.exp(-g.random(shape[1]) * 3)).cuda()
+    got = vp.ops.init_product(space, vel, dt)
+    want = (space.reshape(space.shape + (1,) * vel.dim()) * vel).to(dt)
+    assert got.shape == want.shape and torch.equal(got, want)
+
+
+def test_initialize_matches_reference_formula(v1, v2):
+    """The drivers' initial conditions through the IC kernel equal the
+    reference's broadcast expressions (vlasov2D2V.py:1328-1333,
+    vlasov1D1V.py:890-896) bit for bit."""
+    for dt in ("float64", "float32"):
+        sim = v2.Vlasov(Nx=8, Ny=12, Nvx=16, Nvy=20, nbiter=1, physics_mode=True, epsilon=0.05, dtype=dt,
+                        write_snapshots=False)
+        g = sim.grid
+        x, y = g.x[:, None, None, None].double(), g.y[None, :, None, None].double()
+        vx, vy = g.vx[:, None].double(), g.vy[None, :].double()
+        f0 = (1.0 / math.sqrt(2.0 * math.pi)) * torch.exp(-0.5 * (vx ** 2 + vy ** 2))
+        want = ((1.0 + 0.05 * torch.cos(2 * math.pi / g.Lx * x) * torch.cos(2 * math.pi / g.Ly * y)) * f0[None, None])
+        assert torch.equal(sim.initialize().variables.fn, want.to(sim.dtype))
+        s1 = v1.Vlasov(Nx=24, Nv=20, nbiter=1, physics_mode=True, epsilon=0.05, dtype=dt, write_snapshots=False)
+        h = s1.grid
+        maxw = (1.0 / math.sqrt(2.0 * math.pi)) * torch.exp(-0.5 * h.v.double()[None, :] ** 2)
+        want1 = (1.0 + 0.05 * torch.cos(2.0 * math.pi / h.L * h.x.double()[:, None])) * maxw
+        assert torch.equal(s1.initialize().variables.fn, want1.to(s1.dtype))
