@@ -26,7 +26,7 @@ __all__ = ["BatchStepper2D", "Stepper1D", "Stepper2D", "VlasovError", "load", "o
 
 
 def __getattr__(name):
-    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune", "corrector"):
+    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune", "corrector", "slab"):
         import importlib
 
         return importlib.import_module(f"{__name__}.{name}")
