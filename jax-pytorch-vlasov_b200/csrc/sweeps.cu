@@ -655,12 +655,23 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
         for (int j = 0; j < 5; ++j) win[j] = raw_vec<TS, VEC>(load_row(r0 + j));
         int rnext = r0 + 5;
-
-        for (int l = 0; l < nvx; l += KK) {
-            R nx[KK];
+        // 4-byte and 2-byte storage load each chunk's rows one chunk ahead
+        // (under the previous chunk's vy kick); 8-byte storage and the
+        // split / moment variants would spill and load them in place
+        constexpr bool AHEAD = sizeof(TS) <= 4 && !EQ && !DIAG;
+        R nx[KK];
+        if constexpr (AHEAD) {
 #pragma unroll
             for (int u = 0; u < KK; ++u) nx[u] = load_row(rnext + u);
             rnext += KK;
+        }
+
+        for (int l = 0; l < nvx; l += KK) {
+            if constexpr (!AHEAD) {
+#pragma unroll
+                for (int u = 0; u < KK; ++u) nx[u] = load_row(rnext + u);
+                rnext += KK;
+            }
             // vx kick of rows l..l+KK-1 into the team's row buffer (rounded to
             // the storage type, as the reference stores f between the kicks)
 #pragma unroll
@@ -687,6 +698,22 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
                         for (int e = 0; e < VEC; ++e) rowbuf[u * nvy + li * VEC + e] = rv[e];
                     }
+                }
+            }
+            // the window moves on (the last 5 rows of [win; nx], KK may be
+            // < 5) and the next chunk's loads go out before the vy kick,
+            // which then hides their latency
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const int idx = j + KK;
+                if (idx < 5) win[j] = win[idx];
+                else win[j] = raw_vec<TS, VEC>(nx[idx - 5]);
+            }
+            if constexpr (AHEAD) {
+                if (l + KK < nvx) {
+#pragma unroll
+                    for (int u = 0; u < KK; ++u) nx[u] = load_row(rnext + u);
+                    rnext += KK;
                 }
             }
             __syncwarp();
@@ -753,12 +780,6 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                 }
             }
             __syncwarp();
-#pragma unroll
-            for (int j = 0; j < 5; ++j) {  // the last 5 rows of [win; nx] (KK may be < 5)
-                const int idx = j + KK;
-                if (idx < 5) win[j] = win[idx];
-                else win[j] = raw_vec<TS, VEC>(nx[idx - 5]);
-            }
         }
         if constexpr (DIAG) {
             for (int off = team >> 1; off > 0; off >>= 1) {
