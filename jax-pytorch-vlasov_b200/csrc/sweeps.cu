@@ -20,6 +20,7 @@
 //  * k_gather: the general per-element-departure sweep (advect_1d semantics).
 //  * k_rho: compute_rho as a standalone reduction.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "launch.h"
@@ -132,6 +133,20 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
         }
         const TS* src = in + (o * n) * ni + col;
         TS* dst = out + (o * n) * ni + col;
+        // FP32 compute: neighbouring elements go through the paired FMA of
+        // sm_100 (per lane the same IEEE operations); wp[h][j] holds the tap
+        // weights of elements 2h and 2h+1. Not for the 7-row FP32 windows,
+        // whose per-element weight pairs would spill (and which are
+        // memory-bound anyway); BF16 storage, bound by instructions, pairs both.
+        constexpr bool PAIRS = std::is_same<C, float>::value && VEC % 2 == 0 && (NT == 6 || sizeof(TS) == 2);
+        float2 wp[PAIRS ? VEC / 2 : 1][NT];
+        if constexpr (PAIRS) {
+#pragma unroll
+            for (int h = 0; h < VEC / 2; ++h)
+#pragma unroll
+                for (int j = 0; j < NT; ++j)
+                    wp[h][j] = make_float2(wt[NT == 6 ? 0 : 2 * h][j], wt[NT == 6 ? 0 : 2 * h + 1][j]);
+        }
 
         using R = typename Raw<TS, VEC>::type;  // a held row (packed for 4 x bf16)
         const R rzero = raw_zero<TS, VEC>();
@@ -219,16 +234,36 @@ __device__ __forceinline__ void strided_item(const StridedArgs& a, const int64_t
 #pragma unroll
             for (int u = 0; u < KU; ++u) {
                 V res;
+                if constexpr (PAIRS) {
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) {
-                    auto g = [&](int j) -> C { return j < NW ? win[j].v[e] : raw_get<TS, VEC>(nx[j - NW], e); };
-                    const int we = NT == 6 ? 0 : e;
-                    // ascending stencil tap k = descending window row j
-                    C acc = wt[we][NT - 1] * g(u + NT - 1);
+                    for (int h = 0; h < VEC / 2; ++h) {
+                        auto g2 = [&](int j) -> float2 {
+                            return j < NW ? make_float2(win[j].v[2 * h], win[j].v[2 * h + 1])
+                                          : make_float2(raw_get<TS, VEC>(nx[j - NW], 2 * h),
+                                                        raw_get<TS, VEC>(nx[j - NW], 2 * h + 1));
+                        };
+                        float2 acc = __fmul2_rn(wp[h][NT - 1], g2(u + NT - 1));
 #pragma unroll
-                    for (int j = NT - 2; j >= 0; --j) acc = fma(wt[we][j], g(u + j), acc);
-                    if constexpr (EQ) acc += bias[e];
-                    res.v[e] = acc;
+                        for (int j = NT - 2; j >= 0; --j) acc = __ffma2_rn(wp[h][j], g2(u + j), acc);
+                        if constexpr (EQ) {
+                            acc.x += bias[2 * h];
+                            acc.y += bias[2 * h + 1];
+                        }
+                        res.v[2 * h] = acc.x;
+                        res.v[2 * h + 1] = acc.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) {
+                        auto g = [&](int j) -> C { return j < NW ? win[j].v[e] : raw_get<TS, VEC>(nx[j - NW], e); };
+                        const int we = NT == 6 ? 0 : e;
+                        // ascending stencil tap k = descending window row j
+                        C acc = wt[we][NT - 1] * g(u + NT - 1);
+#pragma unroll
+                        for (int j = NT - 2; j >= 0; --j) acc = fma(wt[we][j], g(u + j), acc);
+                        if constexpr (EQ) acc += bias[e];
+                        res.v[e] = acc;
+                    }
                 }
                 const bool row_ok = active && l + u < l_end;
                 if (row_ok) stv<TS, VEC>(dst + (int64_t)(l + u) * ni, res);
@@ -596,6 +631,9 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         }
         sx = max(-(1 << 28), min(1 << 28, sx));
         sy = max(-(1 << 28), min(1 << 28, sy));
+        float2 wx2[6];  // the vx weights paired, for the paired FMA (FP32 compute)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) wx2[k] = make_float2((float)wx[k], (float)wx[k]);
         // equilibrium split: the kicks of feq = A(vx) B(vy) add
         // (Kx A - A)(vx) B(vy) after the vx kick and A(vx) (Ky B - B)(vy) after
         // the vy kick (K: the plane's kick operator, zero outside the grid)
@@ -679,17 +717,38 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                 C rv[VEC];
                 double dA = 0.0;
                 if constexpr (EQ) dA = (l + u < nvx) ? dA_row(l + u) : 0.0;
+                if constexpr (std::is_same<C, float>::value && VEC % 2 == 0 && !EQ && !DIAG) {
+                    // pairs of elements through the paired FMA (same IEEE
+                    // operations per lane)
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) {
-                    auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : raw_get<TS, VEC>(nx[j - 5], e); };
-                    C acc = wx[0] * g(u + 5);
-                    acc = fma(wx[1], g(u + 4), acc);
-                    acc = fma(wx[2], g(u + 3), acc);
-                    acc = fma(wx[3], g(u + 2), acc);
-                    acc = fma(wx[4], g(u + 1), acc);
-                    acc = fma(wx[5], g(u + 0), acc);
-                    if constexpr (EQ) acc += C(dA * Be[e]);
-                    rv[e] = as_stored<TS>(acc);
+                    for (int h = 0; h < VEC / 2; ++h) {
+                        auto g2 = [&](int j) -> float2 {
+                            return j < 5 ? make_float2(win[j].v[2 * h], win[j].v[2 * h + 1])
+                                         : make_float2(raw_get<TS, VEC>(nx[j - 5], 2 * h),
+                                                       raw_get<TS, VEC>(nx[j - 5], 2 * h + 1));
+                        };
+                        float2 acc = __fmul2_rn(wx2[0], g2(u + 5));
+                        acc = __ffma2_rn(wx2[1], g2(u + 4), acc);
+                        acc = __ffma2_rn(wx2[2], g2(u + 3), acc);
+                        acc = __ffma2_rn(wx2[3], g2(u + 2), acc);
+                        acc = __ffma2_rn(wx2[4], g2(u + 1), acc);
+                        acc = __ffma2_rn(wx2[5], g2(u + 0), acc);
+                        rv[2 * h] = as_stored<TS>(acc.x);
+                        rv[2 * h + 1] = as_stored<TS>(acc.y);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) {
+                        auto g = [&](int j) -> C { return j < 5 ? win[j].v[e] : raw_get<TS, VEC>(nx[j - 5], e); };
+                        C acc = wx[0] * g(u + 5);
+                        acc = fma(wx[1], g(u + 4), acc);
+                        acc = fma(wx[2], g(u + 3), acc);
+                        acc = fma(wx[3], g(u + 2), acc);
+                        acc = fma(wx[4], g(u + 1), acc);
+                        acc = fma(wx[5], g(u + 0), acc);
+                        if constexpr (EQ) acc += C(dA * Be[e]);
+                        rv[e] = as_stored<TS>(acc);
+                    }
                 }
                 if (lane_ok) {
                     if constexpr (VEC == 4) {
