@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--dtype", choices=["float32", "bfloat16", "float64"], default=None)
     ap.add_argument("--size", type=int, default=None, help="override N of a 2D2V workload (N^4 grid)")
     ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweeps-only", action="store_true",
                     help="2D2V: one sweep per axis even where the fused (x, y) plane passes apply")
