@@ -11,7 +11,10 @@ pytestmark = pytest.mark.gpu
 # (Nx, Ny, Nvx, Nvy): Ny not a multiple of 8, Ny = 1, Nx below the stencil
 # width, groups of 32 columns inside wider vy rows, the 128-row maximum
 SHAPES = [(16, 16, 32, 32), (8, 6, 16, 64), (12, 100, 4, 32), (5, 3, 2, 32), (33, 128, 8, 64), (7, 1, 3, 32),
-          (64, 128, 16, 128)]
+          (64, 128, 16, 128),
+          # fused edge cases: x lines shorter than the stencil (window rows
+          # repeat), two vx, the 16-row minimum, 17 rows (a part-filled warp)
+          (3, 16, 2, 32), (2, 24, 2, 64), (5, 17, 3, 32), (9, 64, 2, 32), (4, 65, 2, 32)]
 
 
 def seeded(shape, seed):
@@ -33,7 +36,8 @@ def test_plane_pairs_equal_sweeps(vp, shape, dt):
     assert torch.equal(got, want)
 
 
-@pytest.mark.parametrize("shape", [(16, 16, 32, 32), (12, 100, 4, 32), (64, 128, 16, 128)])
+@pytest.mark.parametrize("shape", [(16, 16, 32, 32), (12, 100, 4, 32), (64, 128, 16, 128), (3, 16, 2, 32),
+                                   (5, 17, 3, 32), (4, 65, 2, 32)])
 def test_plane_density(vp, shape):
     Nx, Ny, Nvx, Nvy = shape
     st = vp.Stepper2D(Nx, Ny, Nvx, Nvy, 4 * math.pi, 3.0, 6.0, 5.0, 0.4, dtype=torch.float32, physics_mode=True)
