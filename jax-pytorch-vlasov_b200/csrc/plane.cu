@@ -10,8 +10,11 @@
 //    shift) over all y, 8 y rows per thread, and walks x.
 //  * Each x row of the group (ny rows of 32 contiguous floats, 128 B) comes
 //    in as one TMA box into a ring of DEPTH shared-memory slabs, completion
-//    on one mbarrier per slab (waits are bounded); output rows leave the
-//    same way, staged in shared memory and written by TMA stores.
+//    on one mbarrier per slab (waits are bounded). x first stages its output
+//    rows in shared memory (its density sums read them there) and writes
+//    them by TMA stores; y first stores them from registers (a warp writes
+//    128 contiguous bytes per row) and needs a block barrier only to hand
+//    back slabs, which it does every second row.
 //  * The x drift is a 6-row sliding window in registers. The y drift (shift
 //    per vy, i.e. per lane) reads 13 consecutive rows of a whole row plane
 //    in shared memory: the slab itself (y first) or a double-buffered plane
@@ -211,8 +214,8 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     constexpr int BUF = buf_floats(YM), STG = stage_floats(YM);
     extern __shared__ __align__(1024) unsigned char smem[];
     float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][BUF]
-    float* stage = slabs + DEPTH * BUF;             // [2][STG]
-    float* planes = stage + 2 * STG;                // [2][BUF] (x first)
+    float* stage = slabs + DEPTH * BUF;             // [2][STG] (x first)
+    float* planes = stage + (XFIRST ? 2 * STG : 0); // [2][BUF] (x first)
     uint64_t* bars = reinterpret_cast<uint64_t*>(planes + (XFIRST ? 2 * BUF : 0));
     Producer* prod = reinterpret_cast<Producer*>(bars + DEPTH);
     const int nx = a.nx, ny = a.ny;
@@ -257,6 +260,7 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     bool pend = false;      // x first: a row waiting for its y drift
     int pend_x = 0, pend_cg = 0;
     bool failed = false;
+    bool okacc = true;  // y first: waits since the last barrier all ended
     int last = 0;
 
     // x first: y drift of the pending row from plane PL into stage PL
@@ -342,20 +346,21 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
         } else {
             // y drift of the new row from its slab, then the x drift
             y_drift(sl + yoff, wy, nv);
-            {  // unconditional: a stage written without output is never stored
-                float* st = stage + (P & 1) * STG;
+            if (emit) {
+                float* dst = a.out + ((int64_t)(cons.xa + cons.q - 5) * ny + y0) * a.m + (int64_t)cons.cg * CG + lane;
 #pragma unroll
                 for (int p = 0; p < YT / 2; ++p) {
                     const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
                                           win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
                     const int y = y0 + 2 * p;
-                    if (FULL || y < ny) st[y * CG + lane] = o.x;
-                    if (FULL || y + 1 < ny) st[(y + 1) * CG + lane] = o.y;
+                    if (FULL || y < ny) dst[(int64_t)(2 * p) * a.m] = o.x;
+                    if (FULL || y + 1 < ny) dst[(int64_t)(2 * p + 1) * a.m] = o.y;
                 }
             }
         }
 #pragma unroll
         for (int p = 0; p < YT / 2; ++p) win[p][P] = nv[p];
+        if constexpr (XFIRST) {
         // staged rows become visible to the TMA store; the previous store
         // has read its stage before that buffer is written again
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -367,13 +372,7 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
         if (P == DEPTH - 1) parity ^= 1u;
         ++L;
         if (tid == 0) {
-            if constexpr (XFIRST) {
-                if (pend) tma_store(&tout, stage0 + (uint32_t)(((P + 1) & 1) * STG * 4), pend_cg * CG, pend_x * ny);
-            } else {
-                if (emit)
-                    tma_store(&tout, stage0 + (uint32_t)((P & 1) * STG * 4), cons.cg * CG,
-                              (cons.xa + cons.q - 5) * ny);
-            }
+            if (pend) tma_store(&tout, stage0 + (uint32_t)(((P + 1) & 1) * STG * 4), pend_cg * CG, pend_x * ny);
             Seq& p = prod->seq;
             if (p.valid()) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -381,6 +380,27 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
                 p.next(a);
                 prod->issued += 1;
             }
+        }
+        } else {
+            okacc = okacc && ok;
+            if (P & 1) {  // slabs P-1 and P are free once every warp is past both
+                if (__syncthreads_or(!okacc)) {
+                    failed = true;
+                    return false;
+                }
+                if (tid == 0) {
+                    Seq& p = prod->seq;
+#pragma unroll
+                    for (int d = P - 1; d <= P; ++d)
+                        if (p.valid()) {
+                            issue(d, p);
+                            p.next(a);
+                            prod->issued += 1;
+                        }
+                }
+            }
+            if (P == DEPTH - 1) parity ^= 1u;
+            ++L;
         }
         if constexpr (XFIRST) {
             rho_on = pend;
@@ -401,6 +421,10 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
 
     while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
            body(Step<5>{})) {
+    }
+    if constexpr (!XFIRST) {
+        // a wait on a last, even row has had no barrier vote yet
+        if (!failed && __syncthreads_or(!okacc)) failed = true;
     }
 
     if constexpr (XFIRST) {
@@ -484,7 +508,7 @@ static bool make_map(CUtensorMap* tm, const void* base, int64_t m, int64_t rows_
 }
 
 static constexpr size_t smem_bytes(bool xfirst, int ym) {
-    return (size_t)(DEPTH * buf_floats(ym) + 2 * stage_floats(ym) + (xfirst ? 2 * buf_floats(ym) : 0)) * 4 +
+    return (size_t)(DEPTH * buf_floats(ym) + (xfirst ? 2 * stage_floats(ym) + 2 * buf_floats(ym) : 0)) * 4 +
            DEPTH * 8 + sizeof(Producer);
 }
 
