@@ -221,10 +221,15 @@ size_t vp_poisson1d_workspace_bytes(int64_t nx);
 /* One Strang step of the 2D2V system, the schedule of
  * vlasov_step_gather_free_impl (vlasov2D2V.py:1043-1083):
  * x(dt/2), y(dt/2) fused with rho, Poisson, vx(dt)+vy(dt) fused,
- * y(dt/2), x(dt/2). With physics_mode == 0 the field is zero, the kicks are
- * the identity and are skipped, and drho/phi are zeroed (as the reference
- * returns zeros). f_in is read only; the result is written to f_out;
- * f_tmp is a third buffer of the same size. Buffers must not overlap. */
+ * y(dt/2), x(dt/2). Where the layout allows (FP32, 16 <= ny <= 128, nvy a
+ * multiple of 32, 16-byte aligned buffers, no equilibrium split,
+ * sweeps_only == 0) each pair of position drifts runs as one pass over f
+ * with the intermediate on chip: f is the same bits, rho is summed in
+ * another (fixed) order. With physics_mode == 0 the field is zero, the
+ * kicks are the identity and are skipped, and drho/phi are zeroed (as the
+ * reference returns zeros). f_in is read only; the result is written to
+ * f_out; f_tmp is a third buffer of the same size. Buffers must not
+ * overlap. */
 typedef struct vp_step2d_desc {
     int32_t dtype;
     int64_t nx, ny, nvx, nvy;
