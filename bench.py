@@ -4,9 +4,12 @@ Default workload (the headline line): the bandwidth-roofline configuration,
 2D2V linear Landau damping on a 128^4 grid (268,435,456 cells), FP32 storage
 of f, amplitude 0.05, k = 0.5 (Lx = Ly = 4 pi), v in [-6, 6], dt = 0.1. A
 "step" is one full Strang step (x, y + rho, FP64 Poisson, vx + vy kick, y, x,
-field-energy and mass diagnostics). Metric: cell-updates/s = cells * steps /
-seconds. The input is synthetic (the initial condition is generated on the
-device); f is 1 GiB per buffer, 8x the 126 MB L2, so no flush is needed.
+field-energy and mass diagnostics; in FP32 each pair of position drifts runs
+as one fused pass, so the step reads and writes f three times, reported as
+passes_over_f). Metric: cell-updates/s = cells * steps / seconds. The input
+is synthetic (the initial condition is generated on the device); f is 1 GiB
+per buffer, 8x the 126 MB L2, so no flush is needed. --sweeps-only runs one
+sweep per axis for comparison.
 
 Other workloads (--workload): c1 (Landau 32^4 FP64), c2 (two-stream 64^4
 FP32), oned (1D1V Landau 4096 x 4096 FP32, the reference's 1D benchmark
