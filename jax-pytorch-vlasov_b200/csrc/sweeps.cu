@@ -1202,10 +1202,116 @@ __global__ void __launch_bounds__(kBlock) k_kick_contig(const TS* __restrict__ i
     }
 }
 
+// The same kick for rows whose length is a multiple of 4 (4- and 2-byte
+// storage, no equilibrium split): a thread owns groups of 4 elements (16- or
+// 8-byte accesses), the block walks rows through a double-buffered
+// shared-memory row while the next row's loads are in flight, one thread per
+// row evaluates the weights, and the 6 taps of a group come from 3 aligned
+// 4-element reads (vy_taps: the same operations, in the same order, as the
+// scalar kernel's, zero outside the row).
+constexpr int kContigGroups = 8;  // groups of 4 per thread: rows up to 8192
+
+template <typename TS>
+__global__ void __launch_bounds__(kBlock) k_kick_contig4(const TS* __restrict__ in, TS* __restrict__ out,
+                                                         int64_t n_rows, int n, const void* E, int e_f64,
+                                                         int64_t e_div, double dt, double dv, int window) {
+    using C = compute_t<TS>;
+    static_assert(sizeof(C) == 4, "4- and 2-byte storage");
+    using R = typename Raw<TS, 4>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* rows = reinterpret_cast<C*>(smem_raw);          // [2][n]
+    float* wts = reinterpret_cast<float*>(rows + 2 * n);  // [2][8]: 6 weights, the shift's bits
+    const int groups = n / 4, tid = threadIdx.x;
+    R cur[kContigGroups];
+    auto load = [&](int64_t o) {
+#pragma unroll
+        for (int k = 0; k < kContigGroups; ++k) {
+            const int g = tid + k * kBlock;
+            cur[k] = (o < n_rows && g < groups) ? ldraw<TS, 4>(in + o * n + g * 4) : raw_zero<TS, 4>();
+        }
+    };
+    int b = 0;
+    load(blockIdx.x);
+    for (int64_t o = blockIdx.x; o < n_rows; o += gridDim.x, b ^= 1) {
+        C* row = rows + b * n;
+#pragma unroll
+        for (int k = 0; k < kContigGroups; ++k) {
+            const int g = tid + k * kBlock;
+            if (g < groups) {
+                C v[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) v[e] = raw_get<TS, 4>(cur[k], e);
+                sts4<C>(row + g * 4, v);
+            }
+        }
+        if (tid == 0) {
+            double wd[6];
+            const int64_t ei = o / e_div;
+            int sh = e_f64 ? kick_weights<double, double>(static_cast<const double*>(E)[ei], dt, dv, window, wd)
+                           : kick_weights<float, double>(static_cast<const float*>(E)[ei], dt, dv, window, wd);
+            sh = max(-(1 << 28), min(1 << 28, sh));
+#pragma unroll
+            for (int k = 0; k < 6; ++k) wts[b * 8 + k] = (float)C(wd[k]);
+            wts[b * 8 + 6] = __int_as_float(sh);
+        }
+        load(o + gridDim.x);  // the next row's loads go out before the kick
+        __syncthreads();
+        C w[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) w[k] = wts[b * 8 + k];
+        const int sh = __float_as_int(wts[b * 8 + 6]);
+        // the window of a group's first element starts gshift elements away:
+        // group offset gd (floor division) and remainder r in [0, 4)
+        const int gshift = -sh - 3;
+        const int gd = gshift >= 0 ? gshift / 4 : -((-gshift + 3) / 4);
+        const int r = gshift - 4 * gd;
+#pragma unroll
+        for (int k = 0; k < kContigGroups; ++k) {
+            const int g = tid + k * kBlock;
+            if (g >= groups) continue;
+            C t[12];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int gi = g + gd + j;
+                C q[4] = {C(0), C(0), C(0), C(0)};
+                if (gi >= 0 && gi < groups) lds4<C>(row + gi * 4, q);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) t[4 * j + e] = q[e];
+            }
+            Vec<TS, 4> res;
+            switch (r) {
+                case 0: vy_taps<0, C>(t, w, res.v); break;
+                case 1: vy_taps<1, C>(t, w, res.v); break;
+                case 2: vy_taps<2, C>(t, w, res.v); break;
+                default: vy_taps<3, C>(t, w, res.v); break;
+            }
+            stv<TS, 4>(out + o * n + g * 4, res);
+        }
+        // one barrier per row: buffer b is written again two rows on, after
+        // the next row's barrier, when every thread is done reading it
+    }
+}
+
 template <typename TS>
 static int launch_kick_contig_t(const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                                 int64_t e_div, double dt, double dv, int window, const EqSplit* eq,
                                 cudaStream_t st) {
+    if constexpr (sizeof(TS) <= 4) {
+        const size_t align = sizeof(TS) * 4;
+        if (n % 4 == 0 && n / 4 <= kBlock * kContigGroups && !(eq && eq->B) &&
+            reinterpret_cast<uintptr_t>(in) % align == 0 && reinterpret_cast<uintptr_t>(out) % align == 0) {
+            const size_t smem = 2 * (size_t)n * sizeof(compute_t<TS>) + 16 * sizeof(float);
+            auto kern = k_kick_contig4<TS>;
+            if (smem > 48 * 1024 &&
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                return set_cuda_error("cudaFuncSetAttribute(k_kick_contig4)");
+            const int occ = occupancy(kern, kBlock, smem);
+            const int64_t grid = std::min<int64_t>(n_rows, (int64_t)sm_count() * occ);
+            kern<<<(unsigned)std::max<int64_t>(grid, 1), kBlock, smem, st>>>(
+                static_cast<const TS*>(in), static_cast<TS*>(out), n_rows, (int)n, E, e_f64, e_div, dt, dv, window);
+            return check_launch("k_kick_contig4");
+        }
+    }
     int tpr = 32;
     while (tpr < n && tpr < kBlock) tpr <<= 1;
     const int rpb = kBlock / tpr;

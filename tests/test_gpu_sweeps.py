@@ -180,3 +180,26 @@ def test_contiguous_kick_long_rows(vp):
         want = O.kick_static(f, E, 0.05, dv, 1, window=window)
         got = vp.ops.kick(to_dev(f, torch.float64), to_dev(E, torch.float64), 0.05, dv, 1, window=window)
         assert relerr(got, want) < 1e-14
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+@pytest.mark.parametrize("n", [4, 12, 48, 256, 4096, 8192])
+@pytest.mark.parametrize("window", [-1, 0, 1])
+def test_contiguous_kick_vector_rows_equal_scalar_rows(vp, dtype, n, window):
+    """Rows of a multiple of 4 elements at 16-byte (8-byte for BF16) aligned
+    addresses take the 4-wide kernel; the same rows one element off that
+    alignment take the one-element-per-thread kernel. Both apply the 6 taps in
+    the same order with zero fill, so the results agree bit for bit."""
+    rows = 37
+    f = to_dev(seeded(8, (rows, n), torch.float32) + 0.25, dtype)
+    dv = 10.0 / (n - 1) if n > 1 else 1.0
+    # shifts from a fraction of a cell to several times the row length
+    E = to_dev(np.linspace(-1.0, 1.0, rows) * (3.0 * n * dv / 0.05) * np.geomspace(1e-3, 1.0, rows), torch.float32)
+    want = vp.ops.kick(f, E, 0.05, dv, 1, window=window)
+    flat = torch.empty(rows * n + 1, dtype=dtype, device="cuda")
+    off = flat[1:].view(rows, n)
+    off.copy_(f)
+    out_flat = torch.empty(rows * n + 1, dtype=dtype, device="cuda")
+    got = vp.ops.kick(off, E, 0.05, dv, 1, window=window, out=out_flat[1:].view(rows, n))
+    assert torch.equal(got.view(torch.int16 if dtype == torch.bfloat16 else torch.int32),
+                       want.view(torch.int16 if dtype == torch.bfloat16 else torch.int32))
