@@ -599,6 +599,244 @@ __global__ void __launch_bounds__(1024) k_p1(const double* __restrict__ nrho, in
     }
 }
 
+// ---- 1D, power-of-two lengths ------------------------------------------------
+// The same solve for n = 2^k <= 8192 as a Stockham autosort FFT (radix-16
+// passes, then one radix-2/4/8 pass for the remainder) in one block of
+// max(32, n/16) threads. Pass with span p and radix R: butterfly b takes
+// x_j = a[b + j n/R] (j < R), multiplies x_j by w^j (w = exp(-+2 pi i k/(pR)),
+// k = b mod p), applies the R-point DFT in registers and stores its output m
+// at (b - k) R + k + m p; after the last pass the array is in natural order.
+// Each thread keeps 16 values per pass, every pass reads its inputs, waits for
+// the block, then overwrites the same buffer, and the buffer is padded by one
+// entry every 16 so that the strided accesses of every pass spread over all
+// shared-memory banks. The R-point DFT is a radix-2 decimation in frequency
+// over registers with the 16th roots of unity as constants.
+namespace p1 {
+constexpr int kMaxN = 8192;
+constexpr int kMaxThreads = kMaxN / 16;
+
+__host__ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 w) {
+    return make_double2(fma(a.x, w.x, -a.y * w.y), fma(a.x, w.y, a.y * w.x));
+}
+
+// cos and sin of 2 pi q / 16
+__host__ __device__ constexpr double cos16(int q) {
+    constexpr double C = 0.92387953251128675613, S = 0.38268343236508977173, H = 0.70710678118654752440;
+    switch (q & 15) {
+        case 0: return 1.0;
+        case 1: return C;
+        case 2: return H;
+        case 3: return S;
+        case 4: return 0.0;
+        case 5: return -S;
+        case 6: return -H;
+        case 7: return -C;
+        case 8: return -1.0;
+        case 9: return -C;
+        case 10: return -H;
+        case 11: return -S;
+        case 12: return 0.0;
+        case 13: return S;
+        case 14: return H;
+        default: return C;
+    }
+}
+__host__ __device__ constexpr double sin16(int q) { return cos16(q - 4); }
+
+// a * exp(-+2 pi i q/16) (minus for the forward transform); q is a constant
+// once the calling loops are unrolled
+template <bool INV>
+__device__ __forceinline__ double2 rot16(double2 a, int q) {
+    q &= 15;
+    if (q == 0) return a;
+    if (q == 8) return make_double2(-a.x, -a.y);
+    if (q == 4) return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+    if (q == 12) return INV ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+    return cmul(a, make_double2(cos16(q), INV ? sin16(q) : -sin16(q)));
+}
+
+__host__ __device__ constexpr int bitrev(int m, int bits) {
+    int r = 0;
+    for (int i = 0; i < bits; ++i) r |= ((m >> i) & 1) << (bits - 1 - i);
+    return r;
+}
+
+// R-point DFT of x in place, natural order in and out
+template <int R, bool INV>
+__device__ __forceinline__ void dft(double2* x) {
+    constexpr int bits = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+#pragma unroll
+    for (int len = R; len >= 2; len >>= 1) {
+#pragma unroll
+        for (int s = 0; s < R; s += len) {
+#pragma unroll
+            for (int j = 0; j < len / 2; ++j) {
+                const double2 a = x[s + j], b = x[s + j + len / 2];
+                x[s + j] = make_double2(a.x + b.x, a.y + b.y);
+                x[s + j + len / 2] = rot16<INV>(make_double2(a.x - b.x, a.y - b.y), j * (16 / len));
+            }
+        }
+    }
+    double2 y[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) y[bitrev(m, bits)] = x[m];
+#pragma unroll
+    for (int m = 0; m < R; ++m) x[m] = y[m];
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void pass(double2* buf, int n, int p) {
+    constexpr int NB = 16 / R;
+    const int nb = n / R, T = blockDim.x;
+    double2 x[NB][R];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const int b = threadIdx.x + q * T;
+        if (b < nb) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) x[q][j] = buf[pad(b + j * nb)];
+        }
+    }
+    __syncthreads();
+    const double inv_pr = 2.0 / (double)(p * R);  // a power of two: exact
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const int b = threadIdx.x + q * T;
+        if (b < nb) {
+            const int k = b & (p - 1);
+            if (k) {
+                double sn, cs;
+                sincospi((double)k * inv_pr, &sn, &cs);
+                const double2 w = make_double2(cs, INV ? sn : -sn);
+                double2 wj = w;
+#pragma unroll
+                for (int j = 1; j < R; ++j) {
+                    x[q][j] = cmul(x[q][j], wj);
+                    if (j + 1 < R) wj = cmul(wj, w);
+                }
+            }
+            dft<R, INV>(x[q]);
+            const int base = (b - k) * R + k;
+#pragma unroll
+            for (int m = 0; m < R; ++m) buf[pad(base + m * p)] = x[q][m];
+        }
+    }
+    __syncthreads();
+}
+
+template <bool INV>
+__device__ void fft(double2* buf, int n) {
+    int p = 1;
+    while (p * 16 <= n) {
+        pass<16, INV>(buf, n, p);
+        p *= 16;
+    }
+    const int r = n / p;
+    if (r == 2) pass<2, INV>(buf, n, p);
+    else if (r == 4) pass<4, INV>(buf, n, p);
+    else if (r == 8) pass<8, INV>(buf, n, p);
+}
+
+// deterministic block reduction (sum, or max of non-negative values); the
+// result is valid in thread 0
+template <bool MAX>
+__device__ double reduce(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = MAX ? fmax(v, o) : v + o;
+    }
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_xor_sync(0xffffffffu, v, off);
+            v = MAX ? fmax(v, o) : v + o;
+        }
+    }
+    return v;
+}
+}  // namespace p1
+
+__global__ void __launch_bounds__(p1::kMaxThreads) k_p1_pow2(const double* __restrict__ nrho, int n,
+                                                            const double* __restrict__ inv_kx,
+                                                            const double* __restrict__ inv_kx_sq,
+                                                            double* __restrict__ e, double* __restrict__ rho_out,
+                                                            double* __restrict__ phi,
+                                                            double* __restrict__ parts /* mass, we, emax, 0 */) {
+    using namespace p1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* buf = reinterpret_cast<double2*>(smem_raw);  // pad(n) entries
+    double* red = reinterpret_cast<double*>(buf + pad(n));  // 3 x 32
+    const int T = blockDim.x, t = threadIdx.x;
+    double m = 0.0;
+    for (int i = t; i < n; i += T) {
+        const double v = nrho[i];
+        m += v;
+        const double r = v - 1.0;
+        if (rho_out) rho_out[i] = r;
+        buf[pad(i)] = make_double2(r, 0.0);
+    }
+    m = reduce<false>(m, red);
+    __syncthreads();
+    fft<false>(buf, n);
+    // the hermitian spectrum of Z = E + i phi from the bins 0..n/2 (imaginary
+    // parts of the DC and Nyquist bins dropped, as a c2r transform does)
+    const int nh = n / 2 + 1;
+    double2 z[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int k = t + q * T;
+        if (k < n) {
+            const int kk = k < nh ? k : n - k;
+            const double2 r = buf[pad(kk)];
+            const double ik = __ldg(inv_kx + kk), ik2 = __ldg(inv_kx_sq + kk);
+            double er = r.y * ik, ei = -r.x * ik;
+            double pr = r.x * ik2, pi = r.y * ik2;
+            if (kk == 0 || kk == n / 2) {
+                ei = 0.0;
+                pi = 0.0;
+            }
+            if (k >= nh) {
+                ei = -ei;
+                pi = -pi;
+            }
+            z[q] = make_double2(er - pi, ei + pr);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int k = t + q * T;
+        if (k < n) buf[pad(k)] = z[q];
+    }
+    __syncthreads();
+    fft<true>(buf, n);
+    const double sc = 1.0 / (double)n;
+    double we = 0.0, em = 0.0;
+    for (int i = t; i < n; i += T) {
+        const double2 v = buf[pad(i)];
+        const double ev = v.x * sc, pv = v.y * sc;
+        e[i] = ev;
+        if (phi) phi[i] = pv;
+        we = fma(ev, ev, we);
+        em = fmax(em, fabs(ev));
+    }
+    we = reduce<false>(we, red + 32);
+    em = reduce<true>(em, red + 64);
+    if (t == 0 && parts) {
+        parts[0] = m;
+        parts[1] = we;
+        parts[2] = em;
+        parts[3] = 0.0;
+    }
+}
+
 size_t poisson1d_ws_bytes(int64_t nx) {
     (void)nx;
     return 256;
@@ -606,9 +844,16 @@ size_t poisson1d_ws_bytes(int64_t nx) {
 
 int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double* e,
                   double* rho, double* phi, double* parts, cudaStream_t st) {
+    int rc;
+    if (nx >= 2 && nx <= p1::kMaxN && (nx & (nx - 1)) == 0) {
+        const int len = (int)nx;
+        const size_t smem_p = (size_t)p1::pad(len) * sizeof(double2) + 96 * sizeof(double);
+        if ((rc = set_smem((const void*)k_p1_pow2, smem_p))) return rc;
+        k_p1_pow2<<<1, std::max(32, len / 16), smem_p, st>>>(n, len, inv_kx, inv_kx_sq, e, rho, phi, parts);
+        return check_launch("k_p1_pow2");
+    }
     const size_t smem = 3 * (size_t)nx * sizeof(double2) + 1024 * sizeof(double);
     if (smem > 220 * 1024) return set_error(VP_ERR_UNSUPPORTED, "1D Poisson: nx too large for one block");
-    int rc;
     if ((rc = set_smem((const void*)k_p1, smem))) return rc;
     k_p1<<<1, 1024, smem, st>>>(n, (int)nx, inv_kx, inv_kx_sq, e, rho, phi, parts);
     return check_launch("k_p1");

@@ -51,7 +51,7 @@ def test_poisson2d_analytic(vp, mode):
     np.testing.assert_allclose(ey.cpu().numpy(), ey_a, atol=1e-12)
 
 
-@pytest.mark.parametrize("nx", [64, 4096, 24, 48, 1000])
+@pytest.mark.parametrize("nx", [2, 4, 8, 16, 32, 64, 128, 256, 512, 2048, 4096, 8192, 24, 48, 1000])
 def test_poisson1d(vp, nx):
     L = 4.0 * math.pi
     g = O.make_grid1d(nx, 16, L, 5.0, dtype=np.float64)
