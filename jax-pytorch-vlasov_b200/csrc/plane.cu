@@ -34,6 +34,10 @@
 //    8 columns each, then two shuffles) into per-group partials of the
 //    charge density, [nx][groups][ny], reduced in a fixed order by
 //    k_rho_finalize_wide.
+//  * Above 112 rows the x-first pair runs as k_plane_xr instead: 16 y rows
+//    per thread, the x window of the 21 rows its y drift reads kept in
+//    registers (the 5 rows past a warp's own are recomputed), so neither a
+//    plane exchange nor a per-row barrier is needed; same partials layout.
 // A wait that runs out (1 s) makes the CTA wait for its stores, fill its
 // whole share of the output (and its density partials) with NaN, wait
 // (bounded) for its loads in flight and leave, so a failure shows in the
@@ -478,6 +482,229 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     }
 }
 
+// ---- x then y with the x window in registers --------------------------------
+// The x-first pair without a plane exchange: a thread owns 16 y rows and
+// keeps the x window of the 21 rows its y drift reads (its 16 rows shifted by
+// its lane's y shift, plus the 5 more the 6 taps reach; neighbouring warps
+// recompute the x drift of those 5 rows for themselves). Slabs carry 20 halo
+// rows, the x-drifted rows stay in registers for the y drift, outputs leave
+// from registers (a warp writes 128 contiguous bytes per row), and a block
+// barrier is needed only to hand back slabs, every second row, as in the
+// y-first kernel. The density sums each output row over the group's 32
+// columns in FP64 with a butterfly reduce-scatter over the warp's lanes.
+// The FMA chains are those of k_plane, so f is bit-identical to it.
+constexpr int YT2 = 16;             // y rows per thread
+constexpr int WR = YT2 + 5;         // rows of the x window per thread
+constexpr int HALO2 = 20;           // rows after row ny: copies of rows 0..19
+__host__ __device__ constexpr int buf2_floats(int ym) { return (ym + HALO2) * CG; }
+
+// the 6-tap chain of taps() for one row
+__device__ __forceinline__ float tap1(const float2 (&w)[6], float t0, float t1, float t2, float t3, float t4,
+                                      float t5) {
+    float acc = __fmul_rn(w[5].x, t5);
+    acc = __fmaf_rn(w[4].x, t4, acc);
+    acc = __fmaf_rn(w[3].x, t3, acc);
+    acc = __fmaf_rn(w[2].x, t2, acc);
+    acc = __fmaf_rn(w[1].x, t1, acc);
+    return __fmaf_rn(w[0].x, t0, acc);
+}
+
+// density staging: per warp and buffer, 16 rows of 32 columns, rows padded
+// to 36 floats so that the 16-byte reads of 8 lanes (4 rows, 2 halves) hit
+// distinct banks
+constexpr int RSTRIDE = CG + 4;
+constexpr int RFLOATS = YT2 * RSTRIDE;
+
+template <bool RHO, bool FULL, int YM>
+__global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
+    k_plane_xr(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap thalo,
+               const __grid_constant__ Args a) {
+    constexpr int BUF = buf2_floats(YM), NW = YM / YT2;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][BUF]
+    float* red = slabs + DEPTH * BUF;               // [2][NW][RFLOATS] (density)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(red + (RHO ? 2 * NW * RFLOATS : 0));
+    Producer* prod = reinterpret_cast<Producer*>(bars + DEPTH);
+    const int nx = a.nx, ny = a.ny;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int y0 = warp * YT2;
+    Seq cons;
+    cons.init(a, blockIdx.x, gridDim.x);
+    if (!cons.valid()) return;
+    const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
+    const uint32_t in_bytes = (uint32_t)((ny + HALO2) * CG * 4);
+    auto issue = [&](int d, const Seq& s) {
+        const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
+        const int r = s.row(nx) * ny;
+        expect_bytes(bar, in_bytes);
+        tma_load(&tin, dst, bar, s.cg * CG, r);
+        tma_load(&thalo, dst + (uint32_t)(ny * CG * 4), bar, s.cg * CG, r);
+    };
+    if (tid == 0) {
+        for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        Seq p = cons;
+        long long n = 0;
+        for (; n < DEPTH && p.valid(); ++n) {
+            issue((int)n, p);
+            p.next(a);
+        }
+        prod->seq = p;
+        prod->issued = n;
+    }
+    __syncthreads();
+
+    float2 win[WR / 2][6];  // rows 0..19 of the window, in pairs
+    float wl[6];            // row 20
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+#pragma unroll
+        for (int p = 0; p < WR / 2; ++p) win[p][s] = make_float2(0.f, 0.f);
+        wl[s] = 0.f;
+    }
+    float2 wx[6], wy[6];
+    int yoff = 0;  // float offset of row y0 - sy - 3 (mod ny), column lane
+    uint32_t parity = 0;
+    long long L = 0;
+    bool failed = false, okacc = true;
+    bool rho_on = false;  // a staged row waiting for its density
+    int rho_x = 0, rho_cg = 0;
+    // density of the row staged in buffer SP: lanes 2r and 2r + 1 add the
+    // two halves of row r in FP64, then each other's sums
+    auto rho_flush = [&](auto sp) {
+        constexpr int SP = decltype(sp)::value;
+        __syncwarp();
+        const float4* src =
+            reinterpret_cast<const float4*>(red + (SP * NW + warp) * RFLOATS + (lane >> 1) * RSTRIDE + (lane & 1) * 16);
+        const float4 q0 = src[0], q1 = src[1], q2 = src[2], q3 = src[3];
+        const double s0 = ((double)q0.x + (double)q0.y) + ((double)q0.z + (double)q0.w);
+        const double s1 = ((double)q1.x + (double)q1.y) + ((double)q1.z + (double)q1.w);
+        const double s2 = ((double)q2.x + (double)q2.y) + ((double)q2.z + (double)q2.w);
+        const double s3 = ((double)q3.x + (double)q3.y) + ((double)q3.z + (double)q3.w);
+        double t = (s0 + s1) + (s2 + s3);
+        t += __shfl_xor_sync(0xffffffffu, t, 1);
+        const int yr = y0 + (lane >> 1);
+        if (rho_on && !(lane & 1) && yr < ny) a.part[((int64_t)rho_x * a.n_cg + rho_cg) * ny + yr] = t;
+    };
+
+    auto tables = [&]() {
+        const int jx = (int)(((int64_t)cons.cg * CG / a.nvy) % a.nvx);
+        const int jy = (int)(((int64_t)cons.cg * CG) % a.nvy) + lane;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
+            wx[j] = make_float2(u, u);
+            wy[j] = make_float2(v, v);
+        }
+        int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
+        if (r < 0) r += ny;
+        yoff = r * CG + lane;
+    };
+    tables();
+
+    auto body = [&](auto step) -> bool {
+        constexpr int P = decltype(step)::value;
+        const bool ok = wait_phase(bar0 + 8 * P, parity);
+        // the previous row's density goes along with this row's drifts
+        if constexpr (RHO) rho_flush(Step<(P + 1) & 1>{});
+        const float* sl = slabs + P * BUF + yoff;
+        // the new row replaces the oldest (load L - 6) in slot P
+#pragma unroll
+        for (int p = 0; p < WR / 2; ++p) win[p][P] = make_float2(sl[(2 * p) * CG], sl[(2 * p + 1) * CG]);
+        wl[P] = sl[(WR - 1) * CG];
+        if (cons.q >= 5) {
+            float xd[WR];
+#pragma unroll
+            for (int p = 0; p < WR / 2; ++p) {
+                const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                      win[p][(P + 4) % 6], win[p][(P + 5) % 6], win[p][P]);
+                xd[2 * p] = o.x;
+                xd[2 * p + 1] = o.y;
+            }
+            xd[WR - 1] = tap1(wx, wl[(P + 1) % 6], wl[(P + 2) % 6], wl[(P + 3) % 6], wl[(P + 4) % 6],
+                              wl[(P + 5) % 6], wl[P]);
+            float o16[YT2];
+#pragma unroll
+            for (int p = 0; p < YT2 / 2; ++p) {
+                const int i = 2 * p;
+                const float2 o = taps(wy, make_float2(xd[i], xd[i + 1]), make_float2(xd[i + 1], xd[i + 2]),
+                                      make_float2(xd[i + 2], xd[i + 3]), make_float2(xd[i + 3], xd[i + 4]),
+                                      make_float2(xd[i + 4], xd[i + 5]), make_float2(xd[i + 5], xd[i + 6]));
+                o16[i] = o.x;
+                o16[i + 1] = o.y;
+            }
+            const int x = cons.xa + cons.q - 5;
+            float* dst = a.out + ((int64_t)x * ny + y0) * a.m + (int64_t)cons.cg * CG + lane;
+#pragma unroll
+            for (int e = 0; e < YT2; ++e)
+                if (FULL || y0 + e < ny) dst[(int64_t)e * a.m] = o16[e];
+            if constexpr (RHO) {
+                // stage the row for its density (rows past ny add zero)
+                float* rb = red + ((P & 1) * NW + warp) * RFLOATS + lane;
+                __syncwarp();
+#pragma unroll
+                for (int e = 0; e < YT2; ++e) rb[e * RSTRIDE] = (FULL || y0 + e < ny) ? o16[e] : 0.f;
+                rho_x = x;
+                rho_cg = cons.cg;
+            }
+        }
+        if constexpr (RHO) rho_on = cons.q >= 5;
+        okacc = okacc && ok;
+        if (P & 1) {  // slabs P-1 and P are free once every warp is past both
+            if (__syncthreads_or(!okacc)) {
+                failed = true;
+                return false;
+            }
+            if (tid == 0) {
+                Seq& p = prod->seq;
+#pragma unroll
+                for (int d = P - 1; d <= P; ++d)
+                    if (p.valid()) {
+                        issue(d, p);
+                        p.next(a);
+                        prod->issued += 1;
+                    }
+            }
+        }
+        if (P == DEPTH - 1) parity ^= 1u;
+        ++L;
+        cons.next(a);
+        if (cons.valid() && cons.q == 0) tables();
+        return cons.valid();
+    };
+
+    while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
+           body(Step<5>{})) {
+    }
+    // a wait on a last, even row has had no barrier vote yet
+    if (!failed && __syncthreads_or(!okacc)) failed = true;
+    if (RHO && !failed) {  // the density of the last row
+        if (L & 1)
+            rho_flush(Step<0>{});
+        else
+            rho_flush(Step<1>{});
+    }
+    if (failed) {
+        // the whole share reads NaN, then the loads in flight land
+        __syncthreads();
+        Seq z;
+        z.init(a, blockIdx.x, gridDim.x);
+        while (z.valid()) {
+            if (z.q >= 5) {
+                const int x = z.xa + z.q - 5;
+                for (int i = 0; i < YT2 && y0 + i < ny; ++i) {
+                    a.out[((int64_t)x * ny + y0 + i) * a.m + (int64_t)z.cg * CG + lane] = NAN;
+                    if (RHO && lane == 0) a.part[((int64_t)x * a.n_cg + z.cg) * ny + y0 + i] = (double)NAN;
+                }
+            }
+            z.next(a);
+        }
+        if (tid == 0)
+            for (long long k = L; k < prod->issued; ++k)
+                wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+    }
+}
+
 // cuTensorMapEncodeTiled from the driver, looked up once
 static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -534,6 +761,28 @@ static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUte
     return check_launch("k_plane");
 }
 
+template <bool RHO, bool FULL, int YM>
+static int launch_xr(const CUtensorMap& tin, const CUtensorMap& thalo, const Args& a, cudaStream_t st) {
+    auto kern = k_plane_xr<RHO, FULL, YM>;
+    constexpr size_t smem = (size_t)(DEPTH * buf2_floats(YM) + (RHO ? 2 * (YM / YT2) * RFLOATS : 0)) * 4 +
+                            DEPTH * 8 + sizeof(Producer);
+    const int block = 32 * ((a.ny + YT2 - 1) / YT2);
+    static int raised[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(VP_ERR_CUDA, "run_plane: device index out of range");
+    if (!raised[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return set_cuda_error("cudaFuncSetAttribute(k_plane_xr)");
+        raised[dev] = 1;
+    }
+    const int occ = occupancy(kern, block, smem);
+    const int64_t total = (int64_t)a.n_cg * a.nx;
+    const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
+    kern<<<(unsigned)grid, block, smem, st>>>(tin, thalo, a);
+    return check_launch("k_plane_xr");
+}
+
 }  // namespace plane
 
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* f) {
@@ -568,6 +817,21 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
     a.part = part;
     if (tiles) *tiles = a.n_cg;
     CUtensorMap tin, thalo, tout;
+    if (xfirst && ny > YMAX - YT2) {
+        // x then y with the window in registers: 8 warps per CTA. With
+        // fewer rows (fewer warps, one CTA per SM) the plane exchange of
+        // k_plane is faster.
+        if (!make_map(&tin, in, a.m, nx * ny, (int)ny) || !make_map(&thalo, in, a.m, nx * ny, HALO2))
+            return set_error(VP_ERR_CUDA, "run_plane: cuTensorMapEncodeTiled failed");
+        const bool full2 = ny % YT2 == 0;
+        auto go2 = [&](auto ym) {
+            constexpr int YM = decltype(ym)::value;
+            if (part)
+                return full2 ? launch_xr<true, true, YM>(tin, thalo, a, st) : launch_xr<true, false, YM>(tin, thalo, a, st);
+            return full2 ? launch_xr<false, true, YM>(tin, thalo, a, st) : launch_xr<false, false, YM>(tin, thalo, a, st);
+        };
+        return go2(Step<YMAX>{});
+    }
     if (!make_map(&tin, in, a.m, nx * ny, (int)ny) || !make_map(&thalo, in, a.m, nx * ny, HALO) ||
         !make_map(&tout, out, a.m, nx * ny, (int)ny))
         return set_error(VP_ERR_CUDA, "run_plane: cuTensorMapEncodeTiled failed");

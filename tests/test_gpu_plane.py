@@ -14,7 +14,10 @@ SHAPES = [(16, 16, 32, 32), (8, 6, 16, 64), (12, 100, 4, 32), (5, 3, 2, 32), (33
           (64, 128, 16, 128),
           # fused edge cases: x lines shorter than the stencil (window rows
           # repeat), two vx, the 16-row minimum, 17 rows (a part-filled warp)
-          (3, 16, 2, 32), (2, 24, 2, 64), (5, 17, 3, 32), (9, 64, 2, 32), (4, 65, 2, 32)]
+          (3, 16, 2, 32), (2, 24, 2, 64), (5, 17, 3, 32), (9, 64, 2, 32), (4, 65, 2, 32),
+          # x first with the register window (more than 112 rows): a part-filled
+          # last warp, and the 113-row minimum
+          (6, 120, 2, 32), (5, 113, 3, 64)]
 
 
 def seeded(shape, seed):
@@ -37,7 +40,7 @@ def test_plane_pairs_equal_sweeps(vp, shape, dt):
 
 
 @pytest.mark.parametrize("shape", [(16, 16, 32, 32), (12, 100, 4, 32), (64, 128, 16, 128), (3, 16, 2, 32),
-                                   (5, 17, 3, 32), (4, 65, 2, 32)])
+                                   (5, 17, 3, 32), (4, 65, 2, 32), (6, 120, 2, 32), (5, 113, 3, 64)])
 def test_plane_density(vp, shape):
     Nx, Ny, Nvx, Nvy = shape
     st = vp.Stepper2D(Nx, Ny, Nvx, Nvy, 4 * math.pi, 3.0, 6.0, 5.0, 0.4, dtype=torch.float32, physics_mode=True)
