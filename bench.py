@@ -440,7 +440,9 @@ def run_ours(a):
         from oracle import core as O
 
         grid = cpu_sample_grid(a, a.cpu_budget / 2)
-        c_steps = 2
+        # one warm-up step sets how many timed steps fill half the budget
+        t_one = time_oracle(a, grid, 1, 0)
+        c_steps = max(2, min(50, int(a.cpu_budget / 2 / max(t_one, 1e-3))))
         sec = time_oracle(a, grid, c_steps, 1)
         cpu = {"value": math.prod(grid) * c_steps / sec, "unit": "cell-updates/s", "cores": O.num_threads(),
                "kind": "port",

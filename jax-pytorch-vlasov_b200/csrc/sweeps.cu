@@ -376,12 +376,24 @@ static StridedPlan plan_strided(int64_t n_outer, int64_t n_line, int64_t n_inner
     p.nt = nt;
     p.ncg = n_inner / vec;
     p.tiles = (int)((p.ncg + kBlock - 1) / kBlock);
-    // whole lines when there are enough of them to fill the GPU; otherwise
-    // split lines into segments (each costs NT-1 extra halo rows)
-    const int64_t want = (int64_t)sms * std::max(occ_blocks, 1) * 2;
-    int seg = (int)n_line;
+    // Lines may be split into segments (each costs NT-1 extra halo rows).
+    // The number of segments per line minimises waves x (segment + halo)
+    // rows, the time of the busiest block slot, with items handed out in
+    // waves over the resident slots; ties keep fewer segments.
+    const int64_t slots = (int64_t)sms * std::max(occ_blocks, 1);
     const int64_t base = n_outer * p.tiles;
-    while (seg > 64 && base * ((n_line + seg - 1) / seg) < want) seg = (seg + 1) / 2;
+    int seg = (int)n_line;
+    int64_t best = -1;
+    for (int64_t k = 1; k <= std::min<int64_t>(n_line, 4 * slots); ++k) {
+        const int s = (int)((n_line + k - 1) / k);
+        if (s < 16 && k > 1) break;
+        const int64_t items = base * ((n_line + s - 1) / s);
+        const int64_t cost = ((items + slots - 1) / slots) * (s + (k > 1 ? nt - 1 : 0));
+        if (best < 0 || cost < best) {
+            best = cost;
+            seg = s;
+        }
+    }
     if (rho) seg = std::min(seg, 1024);
     p.seg = seg;
     p.nseg = (int)((n_line + seg - 1) / seg);
