@@ -513,6 +513,10 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     Marks mk{d->events, st};
     if ((rc = mk.begin(VP_PHASE_DRIFT_X1))) return rc;
     void* dst = dst_of(i++);
+    // power-of-two nx: the field solve also writes the diagnostics (summing
+    // the density partials there instead of in k_rho_finalize was slower:
+    // one CTA would wait on all their loads)
+    const bool fused_field = phys && poisson1d_fuses(nx);
     if (phys || want_diag) {
         int tiles = 0;
         rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1,
@@ -529,7 +533,11 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     if ((rc = mk.begin(VP_PHASE_FIELD))) return rc;
     if (phys) {
         double* e = d->e ? d->e : w.e;
-        rc = run_poisson1d(w.n, nx, d->inv_kx, d->inv_kx_sq, e, d->rho, d->phi, w.parts, st);
+        if (fused_field)
+            rc = run_poisson1d_fused(w.n, nullptr, 0, 0.0, 0.0, nx, d->inv_kx, d->inv_kx_sq, e, d->rho, d->phi,
+                                     w.parts, want_diag ? d->diag : nullptr, d->dx, 0.5 * d->dx, d->dt / d->dv, st);
+        else
+            rc = run_poisson1d(w.n, nx, d->inv_kx, d->inv_kx_sq, e, d->rho, d->phi, w.parts, st);
         if (rc || (rc = mk.end(VP_PHASE_FIELD)) || (rc = mk.begin(VP_PHASE_KICK))) return rc;
         dst = dst_of(i++);
         rc = run_kick_contig(d->dtype, src, dst, nx, nv, e, 1, 1, d->dt, d->dv, d->window, EQ, st);
@@ -551,7 +559,7 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
     rc = run_strided(d->dtype, src, dst, 1, nx, nv, false, 1, nv, d->shift_spread, d->shift, d->W, nullptr, 0, 1, 0.0, 1.0, -1, nullptr,
                      nullptr, EQ, st);
     if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
-    if (want_diag) {
+    if (want_diag && !fused_field) {
         if (phys) {
             // parts = {sum n, sum e^2, max|e|, 0}: the emax pair reads (max|e|, 0)
             Pois2dWsView v{w.parts, w.parts + 1, w.parts + 2, 1};

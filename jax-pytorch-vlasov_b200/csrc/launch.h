@@ -204,5 +204,13 @@ int launch_diag_finalize_batch(const DiagArgs* runs, int n_runs, int slot, cudaS
 size_t poisson1d_ws_bytes(int64_t nx);
 int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double* e,
                   double* rho, double* phi, double* parts, cudaStream_t st);
+// The 1D solve that also writes the diagnostics (optional), its density
+// given (n) or summed from per-tile partials (n null); only for
+// poisson1d_fuses(nx).
+bool poisson1d_fuses(int64_t nx);
+int run_poisson1d_fused(const double* n, const double* part, int tiles, double scale, double offset, int64_t nx,
+                        const double* inv_kx, const double* inv_kx_sq, double* e, double* rho, double* phi,
+                        double* parts, double* diag, double mass_scale, double we_scale, double shift,
+                        cudaStream_t st);
 
 }  // namespace vp

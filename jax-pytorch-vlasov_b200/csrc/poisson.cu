@@ -686,6 +686,31 @@ __device__ __forceinline__ void dft(double2* x) {
     for (int m = 0; m < R; ++m) x[m] = y[m];
 }
 
+// x[j] *= w^j (j < R), the powers from a product tree of depth log2(R)
+template <int R>
+__device__ __forceinline__ void twiddle(double2* x, double2 w) {
+    x[1] = cmul(x[1], w);
+    if constexpr (R > 2) {
+        const double2 w2 = cmul(w, w);
+        x[2] = cmul(x[2], w2);
+        x[3] = cmul(x[3], cmul(w2, w));
+        if constexpr (R > 4) {
+            const double2 w4 = cmul(w2, w2);
+            x[4] = cmul(x[4], w4);
+#pragma unroll
+            for (int j = 5; j < 8; ++j) x[j] = cmul(x[j], cmul(w4, j == 5 ? w : j == 6 ? w2 : cmul(w2, w)));
+            if constexpr (R > 8) {
+                const double2 w8 = cmul(w4, w4);
+                x[8] = cmul(x[8], w8);
+                const double2 w3 = cmul(w2, w);
+                const double2 lo[8] = {w, w, w2, w3, w4, cmul(w4, w), cmul(w4, w2), cmul(w4, w3)};
+#pragma unroll
+                for (int j = 9; j < 16; ++j) x[j] = cmul(x[j], cmul(w8, lo[j - 8]));
+            }
+        }
+    }
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void pass(double2* buf, int n, int p) {
     constexpr int NB = 16 / R;
@@ -709,13 +734,7 @@ __device__ __forceinline__ void pass(double2* buf, int n, int p) {
             if (k) {
                 double sn, cs;
                 sincospi((double)k * inv_pr, &sn, &cs);
-                const double2 w = make_double2(cs, INV ? sn : -sn);
-                double2 wj = w;
-#pragma unroll
-                for (int j = 1; j < R; ++j) {
-                    x[q][j] = cmul(x[q][j], wj);
-                    if (j + 1 < R) wj = cmul(wj, w);
-                }
+                twiddle<R>(x[q], make_double2(cs, INV ? sn : -sn));
             }
             dft<R, INV>(x[q]);
             const int base = (b - k) * R + k;
@@ -763,20 +782,61 @@ __device__ double reduce(double v, double* red) {
 }
 }  // namespace p1
 
-__global__ void __launch_bounds__(p1::kMaxThreads) k_p1_pow2(const double* __restrict__ nrho, int n,
-                                                            const double* __restrict__ inv_kx,
-                                                            const double* __restrict__ inv_kx_sq,
-                                                            double* __restrict__ e, double* __restrict__ rho_out,
-                                                            double* __restrict__ phi,
-                                                            double* __restrict__ parts /* mass, we, emax, 0 */) {
+// Arguments of k_p1_pow2. The density is either given (nrho) or summed from
+// per-tile partials as k_rho_finalize does (t = 0, 1, ... in order, then
+// * scale + offset); the diagnostics (optional) are those k_diag_finalize
+// writes for one line of partials {mass, we, max |E|, 0}.
+struct P1Args {
+    const double* nrho;
+    const double* part;
+    int tiles;
+    double scale, offset;
+    int n;
+    const double* inv_kx;
+    const double* inv_kx_sq;
+    double* e;
+    double* rho_out;
+    double* phi;
+    double* parts;  // [4]: mass, we, emax, 0
+    double* diag;   // [VP_DIAG_COUNT]
+    double mass_scale, we_scale, shift;
+};
+
+__global__ void __launch_bounds__(p1::kMaxThreads) k_p1_pow2(const __grid_constant__ P1Args a) {
     using namespace p1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n;
     double2* buf = reinterpret_cast<double2*>(smem_raw);  // pad(n) entries
     double* red = reinterpret_cast<double*>(buf + pad(n));  // 3 x 32
     const int T = blockDim.x, t = threadIdx.x;
+    double* __restrict__ rho_out = a.rho_out;
+    double* __restrict__ e = a.e;
+    double* __restrict__ phi = a.phi;
+    const double* __restrict__ inv_kx = a.inv_kx;
+    const double* __restrict__ inv_kx_sq = a.inv_kx_sq;
+    // the thread's (at most 16) densities, all loads issued before any store
+    double dens[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int i = t + q * T;
+        double v = 0.0;
+        if (i < n) {
+            if (a.nrho) {
+                v = __ldg(a.nrho + i);
+            } else {
+                double acc = 0.0;
+                for (int k = 0; k < a.tiles; ++k) acc += __ldg(a.part + (int64_t)k * n + i);
+                v = acc * a.scale + a.offset;
+            }
+        }
+        dens[q] = v;
+    }
     double m = 0.0;
-    for (int i = t; i < n; i += T) {
-        const double v = nrho[i];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int i = t + q * T;
+        if (i >= n) break;
+        const double v = dens[q];
         m += v;
         const double r = v - 1.0;
         if (rho_out) rho_out[i] = r;
@@ -829,12 +889,62 @@ __global__ void __launch_bounds__(p1::kMaxThreads) k_p1_pow2(const double* __res
     }
     we = reduce<false>(we, red + 32);
     em = reduce<true>(em, red + 64);
-    if (t == 0 && parts) {
-        parts[0] = m;
-        parts[1] = we;
-        parts[2] = em;
-        parts[3] = 0.0;
+    if (t == 0) {
+        if (a.parts) {
+            a.parts[0] = m;
+            a.parts[1] = we;
+            a.parts[2] = em;
+            a.parts[3] = 0.0;
+        }
+        if (a.diag) {
+            const double nan = __longlong_as_double(0x7ff8000000000000ULL);
+            a.diag[VP_DIAG_FIELD_ENERGY] = we * a.we_scale;
+            a.diag[VP_DIAG_MASS] = m * a.mass_scale;
+            a.diag[VP_DIAG_L2] = nan;
+            a.diag[VP_DIAG_KINETIC] = nan;
+            a.diag[VP_DIAG_KINETIC_PRE] = nan;
+            a.diag[VP_DIAG_MAX_SHIFT] = fmax(em * a.shift, 0.0 * 0.0);
+            a.diag[6] = 0.0;
+            a.diag[7] = 0.0;
+        }
     }
+}
+
+static bool p1_pow2(int64_t nx) { return nx >= 2 && nx <= p1::kMaxN && (nx & (nx - 1)) == 0; }
+
+static int launch_p1_pow2(const P1Args& a, cudaStream_t st) {
+    const size_t smem = (size_t)p1::pad(a.n) * sizeof(double2) + 96 * sizeof(double);
+    int rc;
+    if ((rc = set_smem((const void*)k_p1_pow2, smem))) return rc;
+    k_p1_pow2<<<1, std::max(32, a.n / 16), smem, st>>>(a);
+    return check_launch("k_p1_pow2");
+}
+
+bool poisson1d_fuses(int64_t nx) { return p1_pow2(nx); }
+
+int run_poisson1d_fused(const double* n, const double* part, int tiles, double scale, double offset, int64_t nx,
+                        const double* inv_kx, const double* inv_kx_sq, double* e, double* rho, double* phi,
+                        double* parts, double* diag, double mass_scale, double we_scale, double shift,
+                        cudaStream_t st) {
+    if (!p1_pow2(nx)) return set_error(VP_ERR_UNSUPPORTED, "1D Poisson: fused form needs a power-of-two nx <= 8192");
+    P1Args a{};
+    a.nrho = n;
+    a.part = part;
+    a.tiles = tiles;
+    a.scale = scale;
+    a.offset = offset;
+    a.n = (int)nx;
+    a.inv_kx = inv_kx;
+    a.inv_kx_sq = inv_kx_sq;
+    a.e = e;
+    a.rho_out = rho;
+    a.phi = phi;
+    a.parts = parts;
+    a.diag = diag;
+    a.mass_scale = mass_scale;
+    a.we_scale = we_scale;
+    a.shift = shift;
+    return launch_p1_pow2(a, st);
 }
 
 size_t poisson1d_ws_bytes(int64_t nx) {
@@ -845,12 +955,17 @@ size_t poisson1d_ws_bytes(int64_t nx) {
 int run_poisson1d(const double* n, int64_t nx, const double* inv_kx, const double* inv_kx_sq, double* e,
                   double* rho, double* phi, double* parts, cudaStream_t st) {
     int rc;
-    if (nx >= 2 && nx <= p1::kMaxN && (nx & (nx - 1)) == 0) {
-        const int len = (int)nx;
-        const size_t smem_p = (size_t)p1::pad(len) * sizeof(double2) + 96 * sizeof(double);
-        if ((rc = set_smem((const void*)k_p1_pow2, smem_p))) return rc;
-        k_p1_pow2<<<1, std::max(32, len / 16), smem_p, st>>>(n, len, inv_kx, inv_kx_sq, e, rho, phi, parts);
-        return check_launch("k_p1_pow2");
+    if (p1_pow2(nx)) {
+        P1Args a{};
+        a.nrho = n;
+        a.n = (int)nx;
+        a.inv_kx = inv_kx;
+        a.inv_kx_sq = inv_kx_sq;
+        a.e = e;
+        a.rho_out = rho;
+        a.phi = phi;
+        a.parts = parts;
+        return launch_p1_pow2(a, st);
     }
     const size_t smem = 3 * (size_t)nx * sizeof(double2) + 1024 * sizeof(double);
     if (smem > 220 * 1024) return set_error(VP_ERR_UNSUPPORTED, "1D Poisson: nx too large for one block");

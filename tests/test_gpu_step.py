@@ -177,6 +177,12 @@ def test_step1d_fp64(vp, shape, physics):
     if physics:
         we = O.field_energy_1d(r.Ex, g.dx)
         assert abs(float(st.diag[0]) - we) <= 1e-10 * we
+        # power-of-two Nx: the field solve writes the diagnostics itself
+        d = st.diag.cpu().numpy()
+        np.testing.assert_allclose(d[1], (r.drho + 1.0).sum() * g.dx, rtol=1e-12)
+        assert np.isnan(d[2]) and np.isnan(d[3]) and np.isnan(d[4])
+        np.testing.assert_allclose(d[5], np.abs(r.Ex).max() * 0.3 / g.dv, rtol=1e-12)
+        assert d[6] == 0.0 and d[7] == 0.0
 
 
 def test_history_oned_against_reference(vp, golden):
