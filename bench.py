@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--dtype", choices=["float32", "bfloat16", "float64"], default=None)
     ap.add_argument("--size", type=int, default=None, help="override N of a 2D2V workload (N^4 grid)")
     ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
-    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweeps-only", action="store_true",
                     help="2D2V: one sweep per axis even where the fused (x, y) plane passes apply")
@@ -152,6 +152,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.samples.append((time.monotonic(), line.strip()))
+
+    def ready(self, timeout=5.0):
+        """Wait (bounded) for nvidia-smi's first sample, so that the timed
+        region that follows is covered from its start."""
+        t = time.monotonic()
+        while self.proc is not None and not self.samples and time.monotonic() - t < timeout:
+            time.sleep(0.02)
 
     def mark(self, t0, t1):
         self.window = (t0, t1)
@@ -361,6 +368,7 @@ def run_ours(a):
             # graph captured here expects at the start of the timed run
             x = st.run(x, max(20, 2 * (a.warmup // 2)), graph=True, graph_chunk=10)
         torch.cuda.synchronize(dev)
+        clk.ready()
         dist.barrier()
         torch.cuda.synchronize(dev)
         launches0 = L.load().vp_launch_count()
@@ -657,6 +665,7 @@ def run_batch(a):
         per_step_launches = L.load().vp_launch_count() - c0
         st.run(max(a.warmup, 3) + 10, graph=True)  # captures the graph, then replays it
         torch.cuda.synchronize(dev)
+        clk.ready()
         dist.barrier()
         torch.cuda.synchronize(dev)
         t_start = torch.cuda.Event(enable_timing=True)
