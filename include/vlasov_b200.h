@@ -38,6 +38,13 @@ extern "C" {
 #define VP_ERR_CUDA 4        /* a CUDA call or kernel launch failed (see vp_last_error) */
 #define VP_ERR_UNSUPPORTED 5 /* shape outside what the kernels implement */
 
+/* Bits a step ORs into its device status word (vp_step2d_desc.status,
+ * vp_step1d_desc.status) while it runs; the caller reads and clears it when
+ * it synchronises (the launch itself has returned VP_OK by then). */
+#define VP_STATUS_WAIT_TIMEOUT 1 /* a bounded device wait (TMA load completion) ran out after 1 s;
+                                    the CTA filled its share of f (and of the density) with NaN */
+#define VP_STATUS_NONFINITE 2    /* the step's field energy or mass is not finite */
+
 /* ---- storage types of f ------------------------------------------------ */
 #define VP_F32 0  /* float storage, float arithmetic */
 #define VP_F64 1  /* double storage, double arithmetic */
@@ -277,6 +284,12 @@ typedef struct vp_step2d_desc {
      * fused (x, y) plane passes apply; f is the same either way, the
      * density then also has the single-axis sweeps' summation order. */
     int32_t sweeps_only;
+    /* optional device int32 (NULL to skip): VP_STATUS_* bits ORed in. */
+    int32_t* status;
+    /* test hook, 0 in normal use: nonzero makes the first TMA load of every
+     * fused-plane CTA expect 16 more bytes than it brings, so that its wait
+     * runs out (after 1 s) and the timeout path is exercised. */
+    int32_t test_stall;
 } vp_step2d_desc;
 
 int vp_step2d(const vp_step2d_desc* desc, void* stream);
@@ -320,6 +333,7 @@ typedef struct vp_step1d_desc {
      * eq_moment = sum(eq_v) * dv. */
     const double* eq_v;
     double eq_moment;
+    int32_t* status; /* optional device int32: VP_STATUS_* bits ORed in */
 } vp_step1d_desc;
 
 int vp_step1d(const vp_step1d_desc* desc, void* stream);

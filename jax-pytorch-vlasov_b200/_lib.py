@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(HERE, "libvlasov_b200.so")
 
 VP_F32, VP_F64, VP_BF16 = 0, 1, 2
 DIAG_COUNT = 8
+STATUS_WAIT_TIMEOUT = 1  # VP_STATUS_* bits of the steps' device status word
+STATUS_NONFINITE = 2
 DIAG_NAMES = ("field_energy", "mass", "l2", "kinetic", "kinetic_pre", "max_shift")
 
 _DTYPE_CODE = {torch.float32: VP_F32, torch.float64: VP_F64, torch.bfloat16: VP_BF16}
@@ -56,6 +58,7 @@ class Step2dDesc(ctypes.Structure):
         ("workspace", P), ("workspace_bytes", SZ), ("events", P),
         ("eq_vx", P), ("eq_vy", P), ("eq_moment", D),
         ("sweeps_only", I32),
+        ("status", P), ("test_stall", I32),
     ]
 
 
@@ -69,6 +72,7 @@ class Step1dDesc(ctypes.Structure):
         ("rho", P), ("phi", P), ("e", P), ("diag", P),
         ("workspace", P), ("workspace_bytes", SZ), ("events", P),
         ("eq_v", P), ("eq_moment", D),
+        ("status", P),
     ]
 
 

@@ -374,7 +374,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         dst = dst_of(i++);
         int tiles = 0;
         rc = run_plane(d->dtype, true, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y,
-                       want_rho ? w.part : nullptr, &tiles, st);
+                       want_rho ? w.part : nullptr, &tiles, d->status, d->test_stall, st);
         if (!rc && want_rho) rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, 0.0, w.rho, st);
         if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
         if ((rc = mk.begin(VP_PHASE_DRIFT_Y1)) || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
@@ -449,7 +449,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
         dst = dst_of(i++);
         rc = run_plane(d->dtype, false, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y, nullptr,
-                       nullptr, st);
+                       nullptr, d->status, d->test_stall, st);
         if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     } else {
     // y drift (dt/2)
@@ -471,11 +471,11 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         if (!phys) {
             // mass straight from rho: sum rho * dx * dy (rho already carries dvx*dvy)
             Pois2dWsView mv{w.rho, nullptr, nullptr, (int)(nx * ny)};
-            rc = run_diag_finalize(mv, nullptr, 0, d->dx * d->dy, 0.0, dV, 0.0, 0.0, nullptr, d->diag, st);
+            rc = run_diag_finalize(mv, nullptr, 0, d->dx * d->dy, 0.0, dV, 0.0, 0.0, nullptr, d->diag, st, d->status);
         } else {
             // without the fused kick the L2 / kinetic moments are not computed (NaN)
             rc = run_diag_finalize(pv, moments, nx * ny, d->dx * d->dy, 0.5 * d->dx * d->dy, dV, d->dt / d->dvx,
-                                   d->dt / d->dvy, nullptr, d->diag, st);
+                                   d->dt / d->dvy, nullptr, d->diag, st, d->status);
         }
         if (rc) return rc;
     }
@@ -535,7 +535,8 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
         double* e = d->e ? d->e : w.e;
         if (fused_field)
             rc = run_poisson1d_fused(w.n, nullptr, 0, 0.0, 0.0, nx, d->inv_kx, d->inv_kx_sq, e, d->rho, d->phi,
-                                     w.parts, want_diag ? d->diag : nullptr, d->dx, 0.5 * d->dx, d->dt / d->dv, st);
+                                     w.parts, want_diag ? d->diag : nullptr, d->dx, 0.5 * d->dx, d->dt / d->dv,
+                                     d->status, st);
         else
             rc = run_poisson1d(w.n, nx, d->inv_kx, d->inv_kx_sq, e, d->rho, d->phi, w.parts, st);
         if (rc || (rc = mk.end(VP_PHASE_FIELD)) || (rc = mk.begin(VP_PHASE_KICK))) return rc;
@@ -563,10 +564,11 @@ int vp_step1d(const vp_step1d_desc* d, void* stream) {
         if (phys) {
             // parts = {sum n, sum e^2, max|e|, 0}: the emax pair reads (max|e|, 0)
             Pois2dWsView v{w.parts, w.parts + 1, w.parts + 2, 1};
-            rc = run_diag_finalize(v, nullptr, 0, d->dx, 0.5 * d->dx, 0.0, d->dt / d->dv, 0.0, nullptr, d->diag, st);
+            rc = run_diag_finalize(v, nullptr, 0, d->dx, 0.5 * d->dx, 0.0, d->dt / d->dv, 0.0, nullptr, d->diag, st,
+                                   d->status);
         } else {
             Pois2dWsView v{w.n, nullptr, nullptr, (int)nx};
-            rc = run_diag_finalize(v, nullptr, 0, d->dx, 0.0, 0.0, 0.0, 0.0, nullptr, d->diag, st);
+            rc = run_diag_finalize(v, nullptr, 0, d->dx, 0.0, 0.0, 0.0, 0.0, nullptr, d->diag, st, d->status);
         }
         if (rc) return rc;
     }

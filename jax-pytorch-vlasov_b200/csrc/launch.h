@@ -114,6 +114,7 @@ struct DiagArgs {
     double* energy;                         // optional [2]: {W_E, mass}
     double* diag;                           // optional [VP_DIAG_COUNT]
     int64_t slot_stride;                    // batched form: doubles between history slots
+    int* status;                            // optional: VP_STATUS_NONFINITE ORed in
 };
 
 struct Pois2dWsView {
@@ -153,7 +154,7 @@ bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, con
 int64_t plane_part_tiles(int64_t nvx, int64_t nvy);
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
               const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
-              cudaStream_t st);
+              int* status, int stall, cudaStream_t st);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                     int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,
@@ -192,7 +193,7 @@ int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, c
                   Pois2dWsView* view, cudaStream_t st);
 int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_mom, double mass_scale,
                       double we_scale, double dv_scale, double shift_x, double shift_y, double* energy,
-                      double* diag, cudaStream_t st);
+                      double* diag, cudaStream_t st, int* status = nullptr);
 int run_poisson2d_static(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
                          const double* inv_ksq, double dx, double dy, double* ex, double* ey, double* drho,
                          double* phi, double* energy, cudaStream_t st);
@@ -211,6 +212,6 @@ bool poisson1d_fuses(int64_t nx);
 int run_poisson1d_fused(const double* n, const double* part, int tiles, double scale, double offset, int64_t nx,
                         const double* inv_kx, const double* inv_kx_sq, double* e, double* rho, double* phi,
                         double* parts, double* diag, double mass_scale, double we_scale, double shift,
-                        cudaStream_t st);
+                        int* status, cudaStream_t st);
 
 }  // namespace vp

@@ -76,6 +76,8 @@ struct Args {
     const int* shift_y;
     const float* W_y;   // [6][nvy]
     double* part;       // [nx][n_cg][ny] FP64 row sums (x first with the density)
+    int* status;        // optional: VP_STATUS_WAIT_TIMEOUT ORed in by a CTA whose wait ran out
+    int stall;          // test hook: the first load of each CTA expects 16 bytes too many
 };
 
 // The rows a CTA loads. Work comes in segments (one group, output rows
@@ -231,10 +233,11 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     const uint32_t slab0 = smem_u32(slabs), stage0 = smem_u32(stage), bar0 = smem_u32(bars);
     const uint32_t in_bytes = (uint32_t)((ny + (XFIRST ? 0 : HALO)) * CG * 4);
     // the producer's current row into slab d
+    uint32_t extra = a.stall ? 16u : 0u;  // test hook, first load only
     auto issue = [&](int d, const Seq& s) {
         const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
         const int r = s.row(nx) * ny;
-        expect_bytes(bar, in_bytes);
+        expect_bytes(bar, in_bytes + extra);
         tma_load(&tin, dst, bar, s.cg * CG, r);
         if constexpr (!XFIRST) tma_load(&thalo, dst + (uint32_t)(ny * CG * 4), bar, s.cg * CG, r);
     };
@@ -245,6 +248,7 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
         long long n = 0;
         for (; n < DEPTH && p.valid(); ++n) {
             issue((int)n, p);
+            extra = 0;
             p.next(a);
         }
         prod->seq = p;
@@ -476,9 +480,11 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
             }
             z.next(a);
         }
-        if (tid == 0)
+        if (tid == 0) {
+            if (a.status) atomicOr(a.status, VP_STATUS_WAIT_TIMEOUT);
             for (long long k = L; k < prod->issued; ++k)
                 wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+        }
     }
 }
 
@@ -533,10 +539,11 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
     if (!cons.valid()) return;
     const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
     const uint32_t in_bytes = (uint32_t)((ny + HALO2) * CG * 4);
+    uint32_t extra = a.stall ? 16u : 0u;  // test hook, first load only
     auto issue = [&](int d, const Seq& s) {
         const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
         const int r = s.row(nx) * ny;
-        expect_bytes(bar, in_bytes);
+        expect_bytes(bar, in_bytes + extra);
         tma_load(&tin, dst, bar, s.cg * CG, r);
         tma_load(&thalo, dst + (uint32_t)(ny * CG * 4), bar, s.cg * CG, r);
     };
@@ -547,6 +554,7 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
         long long n = 0;
         for (; n < DEPTH && p.valid(); ++n) {
             issue((int)n, p);
+            extra = 0;
             p.next(a);
         }
         prod->seq = p;
@@ -699,9 +707,11 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
             }
             z.next(a);
         }
-        if (tid == 0)
+        if (tid == 0) {
+            if (a.status) atomicOr(a.status, VP_STATUS_WAIT_TIMEOUT);
             for (long long k = L; k < prod->issued; ++k)
                 wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+        }
     }
 }
 
@@ -798,7 +808,7 @@ int64_t plane_part_tiles(int64_t nvx, int64_t nvy) { return nvx * nvy / plane::C
 
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
               const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
-              cudaStream_t st) {
+              int* status, int stall, cudaStream_t st) {
     using namespace plane;
     if (!plane_fits(dtype, nx, ny, nvx, nvy, in) || !plane_fits(dtype, nx, ny, nvx, nvy, out))
         return set_error(VP_ERR_UNSUPPORTED, "run_plane: layout not fused");
@@ -815,6 +825,8 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
     a.shift_y = shift_y;
     a.W_y = static_cast<const float*>(W_y);
     a.part = part;
+    a.status = status;
+    a.stall = stall;
     if (tiles) *tiles = a.n_cg;
     CUtensorMap tin, thalo, tout;
     if (xfirst && ny > YMAX - YT2) {

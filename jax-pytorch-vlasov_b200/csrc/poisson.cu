@@ -288,6 +288,8 @@ __device__ __forceinline__ void diag_finalize(const DiagArgs& a, double* scratch
     l2 = block_sum(l2, scratch);
     if (threadIdx.x == 0) {
         const double we = w * a.we_scale, mass = m * a.mass_scale;
+        if (a.status && ((a.n_we && !isfinite(we)) || (a.n_mass && !isfinite(mass))))
+            atomicOr(a.status, VP_STATUS_NONFINITE);
         if (a.energy) {
             a.energy[0] = we;
             a.energy[1] = mass;
@@ -444,7 +446,7 @@ int launch_diag_finalize_batch(const DiagArgs* runs, int n_runs, int slot, cudaS
 
 int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_mom, double mass_scale,
                       double we_scale, double dv_scale, double shift_x, double shift_y, double* energy,
-                      double* diag, cudaStream_t st) {
+                      double* diag, cudaStream_t st, int* status) {
     DiagArgs a{};
     a.mass_part = pv.mass_part;
     a.n_mass = pv.mass_part ? pv.n_lines : 0;
@@ -461,6 +463,7 @@ int run_diag_finalize(const Pois2dWsView& pv, const double* moments, int64_t n_m
     a.shift_y = shift_y;
     a.energy = energy;
     a.diag = diag;
+    a.status = status;
     k_diag_finalize<<<1, kPBlock, 0, st>>>(a);
     return check_launch("k_diag_finalize");
 }
@@ -800,6 +803,7 @@ struct P1Args {
     double* parts;  // [4]: mass, we, emax, 0
     double* diag;   // [VP_DIAG_COUNT]
     double mass_scale, we_scale, shift;
+    int* status;    // optional: VP_STATUS_NONFINITE ORed in
 };
 
 __global__ void __launch_bounds__(p1::kMaxThreads) k_p1_pow2(const __grid_constant__ P1Args a) {
@@ -898,6 +902,8 @@ __global__ void __launch_bounds__(p1::kMaxThreads) k_p1_pow2(const __grid_consta
         }
         if (a.diag) {
             const double nan = __longlong_as_double(0x7ff8000000000000ULL);
+            if (a.status && (!isfinite(we * a.we_scale) || !isfinite(m * a.mass_scale)))
+                atomicOr(a.status, VP_STATUS_NONFINITE);
             a.diag[VP_DIAG_FIELD_ENERGY] = we * a.we_scale;
             a.diag[VP_DIAG_MASS] = m * a.mass_scale;
             a.diag[VP_DIAG_L2] = nan;
@@ -925,7 +931,7 @@ bool poisson1d_fuses(int64_t nx) { return p1_pow2(nx); }
 int run_poisson1d_fused(const double* n, const double* part, int tiles, double scale, double offset, int64_t nx,
                         const double* inv_kx, const double* inv_kx_sq, double* e, double* rho, double* phi,
                         double* parts, double* diag, double mass_scale, double we_scale, double shift,
-                        cudaStream_t st) {
+                        int* status, cudaStream_t st) {
     if (!p1_pow2(nx)) return set_error(VP_ERR_UNSUPPORTED, "1D Poisson: fused form needs a power-of-two nx <= 8192");
     P1Args a{};
     a.nrho = n;
@@ -944,6 +950,7 @@ int run_poisson1d_fused(const double* n, const double* part, int tiles, double s
     a.mass_scale = mass_scale;
     a.we_scale = we_scale;
     a.shift = shift;
+    a.status = status;
     return launch_p1_pow2(a, st);
 }
 

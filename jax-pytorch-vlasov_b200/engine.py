@@ -32,11 +32,29 @@ class _Stepper:
         self.window = int(window)
         self.diagnostics = int(diagnostics)  # 0 none, 1 field energy + mass, 2 + L2 / kinetic moments
         self.diag = torch.zeros(L.DIAG_COUNT, dtype=torch.float64, device=self.device)
+        # device status word the steps OR VP_STATUS_* bits into (read by check())
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.test_stall = 0  # test hook of vp_step2d (see vlasov_b200.h); 0 in normal use
         self._graphs = {}
         self._bufs = [None, None]
 
     def empty_f(self) -> torch.Tensor:
         return torch.empty(self.shape, dtype=self.dtype, device=self.device)
+
+    def check(self) -> None:
+        """Synchronise with the steps issued so far and raise VlasovError if
+        one of them reported a device wait that ran out (its share of f was
+        filled with NaN) or a non-finite field energy or mass; the status
+        word is cleared either way."""
+        bits = int(self.status.item())
+        if bits:
+            self.status.zero_()
+            what = []
+            if bits & L.STATUS_WAIT_TIMEOUT:
+                what.append("a device wait ran out (the affected part of f is NaN)")
+            if bits & L.STATUS_NONFINITE:
+                what.append("non-finite field energy or mass")
+            raise L.VlasovError(f"{type(self).__name__}: " + "; ".join(what or [f"status {bits:#x}"]))
 
     # ---- equilibrium split -------------------------------------------------
     def _set_equilibrium(self, factors, spacings):
@@ -227,6 +245,8 @@ class Stepper2D(_Stepper):
             d.eq_vx, d.eq_vy = self.eq[0].data_ptr(), self.eq[1].data_ptr()
             d.eq_moment = self.eq_moment
         d.sweeps_only = 0 if getattr(self, "fuse_drifts", True) else 1
+        d.status = self.status.data_ptr()
+        d.test_stall = int(self.test_stall)
         return d
 
 
@@ -279,6 +299,7 @@ class Stepper1D(_Stepper):
         if self.eq is not None:
             d.eq_v = self.eq[0].data_ptr()
             d.eq_moment = self.eq_moment
+        d.status = self.status.data_ptr()
         return d
 
 

@@ -214,6 +214,8 @@ def _fused(f, dt, table, grid_inv_kx, grid_inv_kx_sq, grid_dx, grid_dv, physics_
         st._graphs = {}
         st._bufs = [None, None]
         st.eq, st.eq_moment = None, 0.0
+        st.status = torch.zeros(1, dtype=torch.int32, device=f.device)
+        st.test_stall = 0
         if len(_PLANS) > 16:
             _PLANS.clear()
         _PLANS[key] = st

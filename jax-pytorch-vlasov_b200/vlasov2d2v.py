@@ -362,6 +362,8 @@ def _fused_step(f, dt, tables, spectral, grid_dx, grid_dy, grid_dvx, grid_dvy, p
         st._graphs = {}
         st._bufs = [None, None]
         st.eq, st.eq_moment = None, 0.0
+        st.status = torch.zeros(1, dtype=torch.int32, device=f.device)
+        st.test_stall = 0
         if len(_PLANS) > 16:
             _PLANS.clear()
         _PLANS[key] = plan = st
