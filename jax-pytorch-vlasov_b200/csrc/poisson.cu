@@ -36,30 +36,36 @@ __device__ __forceinline__ void fill_twiddles(double2* tw, int n) {
     }
 }
 
-// fixed-order block sum (blockDim.x a power of two, scratch >= blockDim.x)
-__device__ double block_sum(double v, double* scratch) {
-    scratch[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
-        if (threadIdx.x < off) scratch[threadIdx.x] += scratch[threadIdx.x + off];
-        __syncthreads();
+// Fixed-order block reductions (blockDim.x a multiple of 32, at most 1024;
+// scratch >= 32 doubles): a shuffle tree in each warp, then one over the
+// warps' results in warp 0. Every thread gets the result.
+template <bool MAX>
+__device__ double block_reduce(double v, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = MAX ? fmax(v, o) : v + o;
     }
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nw ? scratch[lane] : (MAX ? -INFINITY : 0.0);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_xor_sync(0xffffffffu, v, off);
+            v = MAX ? fmax(v, o) : v + o;
+        }
+        if (lane == 0) scratch[0] = v;
+    }
+    __syncthreads();
     const double r = scratch[0];
     __syncthreads();
     return r;
 }
 
-__device__ double block_max(double v, double* scratch) {
-    scratch[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = blockDim.x >> 1; off > 0; off >>= 1) {
-        if (threadIdx.x < off) scratch[threadIdx.x] = fmax(scratch[threadIdx.x], scratch[threadIdx.x + off]);
-        __syncthreads();
-    }
-    const double r = scratch[0];
-    __syncthreads();
-    return r;
-}
+__device__ double block_sum(double v, double* scratch) { return block_reduce<false>(v, scratch); }
+__device__ double block_max(double v, double* scratch) { return block_reduce<true>(v, scratch); }
 
 // ---- 2D: rows, forward ------------------------------------------------------
 __device__ __forceinline__ void p2_rows_fwd(const double* __restrict__ rho, int nx, int ny, double* __restrict__ drho,
