@@ -210,3 +210,13 @@ def test_graph_replay_matches_eager(vp):
     fb = b.run(f0.clone(), 23, history=hb, graph=True, graph_chunk=6)
     assert torch.equal(fa, fb)
     assert torch.equal(ha, hb)
+
+
+@pytest.mark.parametrize("nx", [16384, 4600])
+def test_poisson1d_beyond_one_block_is_rejected(vp, nx):
+    """Power-of-two lengths above 8192 and other lengths above 4522 do not fit
+    the one-block solvers: a clear error, no launch."""
+    n = torch.ones(nx, dtype=torch.float64, device="cuda")
+    inv, inv2 = vp.ops.spectral_1d(nx, 4.0 * math.pi, "cuda")
+    with pytest.raises(vp._lib.VlasovError, match="too large|power-of-two"):
+        vp.ops.poisson1d(n, inv, inv2)
