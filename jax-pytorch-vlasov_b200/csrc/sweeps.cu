@@ -649,7 +649,6 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         // equilibrium split: the kicks of feq = A(vx) B(vy) add
         // (Kx A - A)(vx) B(vy) after the vx kick and A(vx) (Ky B - B)(vy) after
         // the vy kick (K: the plane's kick operator, zero outside the grid)
-        constexpr bool eq = EQ;
         double Be[EQ ? VEC : 1], dBe[EQ ? VEC : 1];
         if constexpr (EQ) {
 #pragma unroll
