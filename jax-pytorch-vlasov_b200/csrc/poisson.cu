@@ -67,13 +67,37 @@ __device__ double block_reduce(double v, double* scratch) {
 __device__ double block_sum(double v, double* scratch) { return block_reduce<false>(v, scratch); }
 __device__ double block_max(double v, double* scratch) { return block_reduce<true>(v, scratch); }
 
+// ---- 2D ----------------------------------------------------------------------
+// The three transforms are direct DFTs over shared-memory twiddle tables
+// (any size). Each output's sum is cut into H = max(1, threads / outputs)
+// consecutive slices so that every thread of the block works; the slices'
+// partial sums are added in slice order (a fixed order).
+__host__ __device__ constexpr int p2_slices(int outputs, int threads) {
+    return outputs >= threads ? 1 : threads / outputs;
+}
+__host__ __device__ constexpr size_t p2_parts(int outputs, int threads) {
+    return (size_t)(outputs > threads ? outputs : threads);  // >= outputs * slices
+}
+__host__ __device__ constexpr size_t p2_fwd_smem(int ny) {
+    return (size_t)ny * sizeof(double2) + (size_t)(ny + 1) * sizeof(double) + kPBlock * sizeof(double) +
+           p2_parts(ny / 2 + 1, kPBlock) * sizeof(double2);
+}
+__host__ __device__ constexpr size_t p2_cols_smem(int nx) {
+    return 5 * (size_t)nx * sizeof(double2) + 3 * p2_parts(nx, kPBlock) * sizeof(double2);
+}
+__host__ __device__ constexpr size_t p2_inv_smem(int ny) {
+    return (size_t)ny * sizeof(double2) + 3 * (size_t)(ny / 2 + 1) * sizeof(double2) + kPBlock * sizeof(double) +
+           3 * p2_parts(ny, kPBlock) * sizeof(double);
+}
+
 // ---- 2D: rows, forward ------------------------------------------------------
 __device__ __forceinline__ void p2_rows_fwd(const double* __restrict__ rho, int nx, int ny, double* __restrict__ drho,
                                             double2* __restrict__ R, double* __restrict__ mass_part, const int ix,
                                             unsigned char* smem_raw) {
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double* row = reinterpret_cast<double*>(tw + ny);
-    double* scratch = row + ny;
+    double* scratch = row + ny + (ny & 1);  // even: part stays 16-byte aligned
+    double2* part = reinterpret_cast<double2*>(scratch + kPBlock);
     const int nyh = ny / 2 + 1;
     fill_twiddles(tw, ny);
     double m = 0.0;
@@ -84,19 +108,32 @@ __device__ __forceinline__ void p2_rows_fwd(const double* __restrict__ rho, int 
         if (drho) drho[(int64_t)ix * ny + iy] = d;
         m += v;
     }
-    m = block_sum(m, scratch);
+    m = block_sum(m, scratch);  // its barriers also publish row and tw
     if (threadIdx.x == 0 && mass_part) mass_part[ix] = m;
-    for (int ky = threadIdx.x; ky < nyh; ky += blockDim.x) {
+    const int H = p2_slices(nyh, blockDim.x);
+    for (int t = threadIdx.x; t < nyh * H; t += blockDim.x) {
+        const int ky = t % nyh, h = t / nyh;
+        const int i0 = h * ny / H, i1 = (h + 1) * ny / H;
         double re = 0.0, im = 0.0;
-        int idx = 0;
-        for (int iy = 0; iy < ny; ++iy) {
-            const double2 t = tw[idx];
-            re = fma(row[iy], t.x, re);
-            im = fma(-row[iy], t.y, im);
+        int idx = (int)(((int64_t)ky * i0) % ny);
+        for (int iy = i0; iy < i1; ++iy) {
+            const double2 w = tw[idx];
+            re = fma(row[iy], w.x, re);
+            im = fma(-row[iy], w.y, im);
             idx += ky;
             if (idx >= ny) idx -= ny;
         }
-        R[(int64_t)ix * nyh + ky] = make_double2(re, im);
+        part[t] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int ky = threadIdx.x; ky < nyh; ky += blockDim.x) {
+        double2 acc = part[ky];
+        for (int h = 1; h < H; ++h) {
+            const double2 q = part[h * nyh + ky];
+            acc.x += q.x;
+            acc.y += q.y;
+        }
+        R[(int64_t)ix * nyh + ky] = acc;
     }
 }
 
@@ -118,21 +155,35 @@ __device__ __forceinline__ void p2_cols(const double2* __restrict__ R, int nx, i
     double2* P = col + nx;
     double2* X = P + nx;
     double2* Y = X + nx;
+    const size_t np = p2_parts(nx, blockDim.x);
+    double2* part = Y + nx;  // [3][np]
     fill_twiddles(tw, nx);
     for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) col[ix] = R[(int64_t)ix * nyh + k];
     __syncthreads();
-    const double kyv = ky[k];
-    for (int q = threadIdx.x; q < nx; q += blockDim.x) {
+    const int H = p2_slices(nx, blockDim.x);
+    for (int t = threadIdx.x; t < nx * H; t += blockDim.x) {
+        const int q = t % nx, h = t / nx;
+        const int i0 = h * nx / H, i1 = (h + 1) * nx / H;
         double re = 0.0, im = 0.0;
-        int idx = 0;
-        for (int ix = 0; ix < nx; ++ix) {
-            const double2 t = tw[idx];
+        int idx = (int)(((int64_t)q * i0) % nx);
+        for (int ix = i0; ix < i1; ++ix) {
+            const double2 w = tw[idx];
             const double2 c = col[ix];
-            // c * conj(t)
-            re = fma(c.x, t.x, fma(c.y, t.y, re));
-            im = fma(c.y, t.x, fma(-c.x, t.y, im));
+            // c * conj(w)
+            re = fma(c.x, w.x, fma(c.y, w.y, re));
+            im = fma(c.y, w.x, fma(-c.x, w.y, im));
             idx += q;
             if (idx >= nx) idx -= nx;
+        }
+        part[t] = make_double2(re, im);
+    }
+    __syncthreads();
+    const double kyv = ky[k];
+    for (int q = threadIdx.x; q < nx; q += blockDim.x) {
+        double re = part[q].x, im = part[q].y;
+        for (int h = 1; h < H; ++h) {
+            re += part[h * nx + q].x;
+            im += part[h * nx + q].y;
         }
         const double inv = inv_ksq[(int64_t)q * nyh + k];
         const double pr = re * inv, pi = im * inv;
@@ -142,26 +193,44 @@ __device__ __forceinline__ void p2_cols(const double2* __restrict__ R, int nx, i
         Y[q] = make_double2(pi * kyv, -pr * kyv);
     }
     __syncthreads();
-    const double sc = 1.0 / (double)nx;
-    for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) {
+    for (int t = threadIdx.x; t < nx * H; t += blockDim.x) {
+        const int ix = t % nx, h = t / nx;
+        const int q0 = h * nx / H, q1 = (h + 1) * nx / H;
         double pr = 0.0, pi = 0.0, xr = 0.0, xi = 0.0, yr = 0.0, yi = 0.0;
-        int idx = 0;
-        for (int q = 0; q < nx; ++q) {
-            const double2 t = tw[idx];
+        int idx = (int)(((int64_t)ix * q0) % nx);
+        for (int q = q0; q < q1; ++q) {
+            const double2 w = tw[idx];
             const double2 a = P[q], b = X[q], c = Y[q];
-            pr = fma(a.x, t.x, fma(-a.y, t.y, pr));
-            pi = fma(a.y, t.x, fma(a.x, t.y, pi));
-            xr = fma(b.x, t.x, fma(-b.y, t.y, xr));
-            xi = fma(b.y, t.x, fma(b.x, t.y, xi));
-            yr = fma(c.x, t.x, fma(-c.y, t.y, yr));
-            yi = fma(c.y, t.x, fma(c.x, t.y, yi));
+            pr = fma(a.x, w.x, fma(-a.y, w.y, pr));
+            pi = fma(a.y, w.x, fma(a.x, w.y, pi));
+            xr = fma(b.x, w.x, fma(-b.y, w.y, xr));
+            xi = fma(b.y, w.x, fma(b.x, w.y, xi));
+            yr = fma(c.x, w.x, fma(-c.y, w.y, yr));
+            yi = fma(c.y, w.x, fma(c.x, w.y, yi));
             idx += ix;
             if (idx >= nx) idx -= nx;
         }
+        part[t] = make_double2(pr, pi);
+        part[np + t] = make_double2(xr, xi);
+        part[2 * np + t] = make_double2(yr, yi);
+    }
+    __syncthreads();
+    const double sc = 1.0 / (double)nx;
+    for (int ix = threadIdx.x; ix < nx; ix += blockDim.x) {
+        double2 p = part[ix], x = part[np + ix], y = part[2 * np + ix];
+        for (int h = 1; h < H; ++h) {
+            const double2 a = part[h * nx + ix], b = part[np + h * nx + ix], c = part[2 * np + h * nx + ix];
+            p.x += a.x;
+            p.y += a.y;
+            x.x += b.x;
+            x.y += b.y;
+            y.x += c.x;
+            y.y += c.y;
+        }
         const int64_t o = (int64_t)ix * nyh + k;
-        Zp[o] = make_double2(pr * sc, pi * sc);
-        Zx[o] = make_double2(xr * sc, xi * sc);
-        Zy[o] = make_double2(yr * sc, yi * sc);
+        Zp[o] = make_double2(p.x * sc, p.y * sc);
+        Zx[o] = make_double2(x.x * sc, x.y * sc);
+        Zy[o] = make_double2(y.x * sc, y.y * sc);
     }
 }
 
@@ -185,6 +254,8 @@ __device__ __forceinline__ void p2_rows_inv(const double2* __restrict__ Zp, cons
     double2* zx = zp + nyh;
     double2* zy = zx + nyh;
     double* scratch = reinterpret_cast<double*>(zy + nyh);
+    const size_t np = p2_parts(ny, blockDim.x);
+    double* part = scratch + kPBlock;  // [3][np]
     fill_twiddles(tw, ny);
     for (int q = threadIdx.x; q < nyh; q += blockDim.x) {
         const int64_t o = (int64_t)ix * nyh + q;
@@ -195,18 +266,34 @@ __device__ __forceinline__ void p2_rows_inv(const double2* __restrict__ Zp, cons
     __syncthreads();
     const bool even = (ny % 2) == 0;
     const int last = (ny - 1) / 2;  // last bin that appears twice
+    // sums over the bins 1..last, cut into H slices
+    const int H = p2_slices(ny, blockDim.x);
+    for (int t = threadIdx.x; t < ny * H; t += blockDim.x) {
+        const int iy = t % ny, h = t / ny;
+        const int q0 = 1 + h * last / H, q1 = 1 + (h + 1) * last / H;
+        double sp = 0.0, sx = 0.0, sy = 0.0;
+        int idx = (int)(((int64_t)iy * q0) % ny);
+        for (int q = q0; q < q1; ++q) {
+            const double2 w = tw[idx];
+            sp = fma(zp[q].x, w.x, fma(-zp[q].y, w.y, sp));
+            sx = fma(zx[q].x, w.x, fma(-zx[q].y, w.y, sx));
+            sy = fma(zy[q].x, w.x, fma(-zy[q].y, w.y, sy));
+            idx += iy;
+            if (idx >= ny) idx -= ny;
+        }
+        part[t] = sp;
+        part[np + t] = sx;
+        part[2 * np + t] = sy;
+    }
+    __syncthreads();
     const double sc = 1.0 / (double)ny;
     double we = 0.0, exm = 0.0, eym = 0.0;
     for (int iy = threadIdx.x; iy < ny; iy += blockDim.x) {
-        double sp = 0.0, sx = 0.0, sy = 0.0;
-        int idx = iy;
-        for (int q = 1; q <= last; ++q) {
-            const double2 t = tw[idx];
-            sp = fma(zp[q].x, t.x, fma(-zp[q].y, t.y, sp));
-            sx = fma(zx[q].x, t.x, fma(-zx[q].y, t.y, sx));
-            sy = fma(zy[q].x, t.x, fma(-zy[q].y, t.y, sy));
-            idx += iy;
-            if (idx >= ny) idx -= ny;
+        double sp = part[iy], sx = part[np + iy], sy = part[2 * np + iy];
+        for (int h = 1; h < H; ++h) {
+            sp += part[h * ny + iy];
+            sx += part[np + h * ny + iy];
+            sy += part[2 * np + h * ny + iy];
         }
         double vp = zp[0].x + 2.0 * sp, vx = zx[0].x + 2.0 * sx, vy = zy[0].x + 2.0 * sy;
         if (even) {
@@ -374,15 +461,15 @@ int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, c
     pois2d_layout(nx, ny, static_cast<char*>(ws), &w);
     const int64_t nyh = ny / 2 + 1;
     int rc;
-    const size_t s1 = ny * sizeof(double2) + ny * sizeof(double) + kPBlock * sizeof(double);
+    const size_t s1 = p2_fwd_smem((int)ny);
     if ((rc = set_smem((const void*)k_p2_rows_fwd, s1))) return rc;
     k_p2_rows_fwd<<<(unsigned)nx, kPBlock, s1, st>>>(rho, (int)nx, (int)ny, drho, w.R, w.mass_part);
     if ((rc = check_launch("k_p2_rows_fwd"))) return rc;
-    const size_t s2 = 5 * nx * sizeof(double2);
+    const size_t s2 = p2_cols_smem((int)nx);
     if ((rc = set_smem((const void*)k_p2_cols, s2))) return rc;
     k_p2_cols<<<(unsigned)nyh, kPBlock, s2, st>>>(w.R, (int)nx, (int)ny, kx, ky, inv_ksq, w.Zp, w.Zx, w.Zy);
     if ((rc = check_launch("k_p2_cols"))) return rc;
-    const size_t s3 = ny * sizeof(double2) + 3 * nyh * sizeof(double2) + kPBlock * sizeof(double);
+    const size_t s3 = p2_inv_smem((int)ny);
     if ((rc = set_smem((const void*)k_p2_rows_inv, s3))) return rc;
     k_p2_rows_inv<<<(unsigned)nx, kPBlock, s3, st>>>(w.Zp, w.Zx, w.Zy, (int)nx, (int)ny, phi, ex, ey, w.we_part,
                                                      w.emax_part);
@@ -431,15 +518,15 @@ void pois2d_run_args(const double* rho, int64_t nx, int64_t ny, const double* kx
 int launch_poisson2d_batch(const Pois2dRun* runs, int n_runs, int max_nx, int max_ny, cudaStream_t st) {
     const int max_nyh = max_ny / 2 + 1;
     int rc;
-    const size_t s1 = max_ny * sizeof(double2) + max_ny * sizeof(double) + kPBlock * sizeof(double);
+    const size_t s1 = p2_fwd_smem(max_ny);
     if ((rc = set_smem((const void*)k_p2_rows_fwd_batch, s1))) return rc;
     k_p2_rows_fwd_batch<<<dim3((unsigned)max_nx, (unsigned)n_runs), kPBlock, s1, st>>>(runs);
     if ((rc = check_launch("k_p2_rows_fwd_batch"))) return rc;
-    const size_t s2 = 5 * max_nx * sizeof(double2);
+    const size_t s2 = p2_cols_smem(max_nx);
     if ((rc = set_smem((const void*)k_p2_cols_batch, s2))) return rc;
     k_p2_cols_batch<<<dim3((unsigned)max_nyh, (unsigned)n_runs), kPBlock, s2, st>>>(runs);
     if ((rc = check_launch("k_p2_cols_batch"))) return rc;
-    const size_t s3 = max_ny * sizeof(double2) + 3 * max_nyh * sizeof(double2) + kPBlock * sizeof(double);
+    const size_t s3 = p2_inv_smem(max_ny);
     if ((rc = set_smem((const void*)k_p2_rows_inv_batch, s3))) return rc;
     k_p2_rows_inv_batch<<<dim3((unsigned)max_nx, (unsigned)n_runs), kPBlock, s3, st>>>(runs);
     return check_launch("k_p2_rows_inv_batch");
