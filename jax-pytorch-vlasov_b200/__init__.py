@@ -8,6 +8,7 @@ Modules:
   engine      -- Stepper2D / Stepper1D: one library call per Strang step, CUDA graphs;
                  BatchStepper2D: many uneven runs, one launch per substep for all
   workloads   -- seeded initial conditions and the batched-runs parameter draws
+  rates       -- damping and growth rates from a field-energy history
   autotune    -- tile shapes of the batched sweeps, measured and cached in JSON
   corrector   -- learned drift-weight correction on tcgen05 tensor cores: network,
                  training on coarse / refined pairs, LearnedStepper2D
@@ -26,7 +27,7 @@ __all__ = ["BatchStepper2D", "Stepper1D", "Stepper2D", "VlasovError", "load", "o
 
 
 def __getattr__(name):
-    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune", "corrector", "slab"):
+    if name in ("vlasov2d2v", "vlasov1d1v", "snapshot", "workloads", "autotune", "corrector", "slab", "rates"):
         import importlib
 
         return importlib.import_module(f"{__name__}.{name}")

@@ -1,5 +1,6 @@
 """Parity of the field solves and of whole Strang steps with the CPU oracle,
 and of multi-step histories with the reference's own runs (golden files)."""
+import importlib
 import math
 
 import numpy as np
@@ -152,6 +153,12 @@ def test_history_c1_against_reference(vp, golden):
     we = hist[:, 0].cpu().numpy()
     rel = np.abs(we - H["W_E"]) / np.abs(H["W_E"])
     assert rel.max() < 1e-10, rel.max()
+    # the Landau damping rate, as the reference's post-processing checks it
+    R = importlib.import_module("jax-pytorch-vlasov_b200.rates")
+    t = 0.1 * np.arange(1, 101)
+    rate = R.damping_rate(t, we)
+    assert abs(rate - R.damping_rate(t, H["W_E"])) <= 1e-6 * rate
+    assert abs(rate - R.LANDAU_RATE_K05) <= 0.02 * R.LANDAU_RATE_K05
     mass = hist[:, 1].cpu().numpy()
     np.testing.assert_allclose(mass, H["mass"], rtol=1e-12)
     np.testing.assert_allclose(st.drho.cpu().numpy(), H["drho_final"], rtol=0, atol=1e-13)
