@@ -174,9 +174,10 @@ size_t vp_poisson2d_workspace_bytes(int64_t nx, int64_t ny);
 /* vp_poisson2d for callers that cannot allocate device memory. No
  * counterpart in the reference (whose field solve allocates through
  * torch.fft): this entry point serves hosts that must not call cudaMalloc or
- * any allocating routine at the point of the call, such as code recording a
- * CUDA stream capture, a foreign runtime that hands over only pre-registered
- * input and output buffers, or a solver with a fixed device-memory budget.
+ * any allocating routine at the point of the call, such as a foreign runtime
+ * that hands over only its own pre-registered input and output buffers and
+ * owns all other device memory, or an embedded solver that may not grow its
+ * device footprint after start-up.
  * The caller passes inputs and outputs exactly as for vp_poisson2d; the
  * scratch comes from a file-scope device array of the library, sized for
  * nx, ny <= VP_POISSON2D_STATIC_MAX_N (about 2 MiB, held on every GPU that

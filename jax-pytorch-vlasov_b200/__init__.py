@@ -10,8 +10,9 @@ Modules:
   workloads   -- seeded initial conditions and the batched-runs parameter draws
   rates       -- damping and growth rates from a field-energy history
   autotune    -- tile shapes of the batched sweeps, measured and cached in JSON
-  corrector   -- learned drift-weight correction on tcgen05 tensor cores: network,
-                 training on coarse / refined pairs, LearnedStepper2D
+  corrector   -- learned correction of the velocity-kick interpolation weights on
+                 tcgen05 tensor cores: network, training on coarse / refined
+                 pairs, LearnedStepper2D
   ops         -- tensor-level wrappers of the C ABI (include/vlasov_b200.h)
   build       -- compiles csrc/*.cu into libvlasov_b200.so for sm_100a
 

@@ -1,16 +1,16 @@
 """Generate the golden fixtures by running the reference solver itself.
 
 The reference's PyTorch modules are imported unmodified from a checkout of
-yasahi-hpc/JAX-PyTorch-Vlasov (default /root/reference, override with
-$VLASOV_REFERENCE) and run eagerly on the CPU (TORCHDYNAMO_DISABLE=1). They
+yasahi-hpc/JAX-PyTorch-Vlasov (its root given by $VLASOV_REFERENCE) and
+run eagerly on the CPU (TORCHDYNAMO_DISABLE=1). They
 import xarray only for their netCDF writer, which is never called here, so
 an empty stand-in module is registered first.
 
 Inputs are regenerated from the seeds recorded in each fixture
 (numpy.random.default_rng), so the files hold outputs only.
 
-    python tests/golden/make_golden.py            # small cases + C1 history
-    python tests/golden/make_golden.py --long     # also the C2 / C3 / 1D histories
+    VLASOV_REFERENCE=<checkout> python tests/golden/make_golden.py         # small cases + C1 history
+    VLASOV_REFERENCE=<checkout> python tests/golden/make_golden.py --long  # also the C2 / C3 / 1D histories
 """
 from __future__ import annotations
 
@@ -29,7 +29,9 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("VLASOV_REFERENCE", "/root/reference")
+REF = os.environ.get("VLASOV_REFERENCE", "")
+if not REF or not os.path.isdir(REF):
+    sys.exit("make_golden.py: set VLASOV_REFERENCE to the root of a yasahi-hpc/JAX-PyTorch-Vlasov checkout")
 
 
 def _load_reference():
@@ -166,7 +168,7 @@ def gen_poisson():
     """compute_poisson_real on seeded densities, even and odd sizes, plus
     the reference's analytic single-mode case (test_poisson.py)."""
     out = {}
-    for (nx, ny) in ((16, 12), (15, 9), (8, 10)):
+    for (nx, ny) in ((16, 12), (15, 9), (9, 15), (8, 10)):
         for dt_name in ("f64", "f32"):
             p = dict(Nx=nx, Ny=ny, Nvx=4, Nvy=4, Lx=4.0 * math.pi, Ly=3.3, Vx_max=1.0, Vy_max=1.0)
             g = grid2(p, dt_name)

@@ -16,7 +16,7 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-@pytest.mark.parametrize("shape", [(16, 12), (15, 9), (8, 10), (128, 128), (24, 48), (1, 6)])
+@pytest.mark.parametrize("shape", [(16, 12), (15, 9), (9, 15), (8, 10), (128, 128), (24, 48), (1, 6), (7, 5)])
 def test_poisson2d(vp, shape):
     nx, ny = shape
     g = O.make_grid2d(nx, ny, 4, 4, 4.0 * math.pi, 3.3, 1.0, 1.0, dtype=np.float64)

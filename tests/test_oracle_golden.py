@@ -104,7 +104,7 @@ def test_rho(golden, dt):
     np.testing.assert_allclose(rho, golden("sweeps2d")[f"rho_{dt}"], rtol=TOL[dt], atol=0)
 
 
-@pytest.mark.parametrize("shape", [(16, 12), (15, 9), (8, 10)])
+@pytest.mark.parametrize("shape", [(16, 12), (15, 9), (9, 15), (8, 10)])
 @pytest.mark.parametrize("dt", ["f64", "f32"])
 def test_poisson(golden, shape, dt):
     nx, ny = shape

@@ -1,8 +1,9 @@
 """The allocation-free field solve, vp_poisson2d_static.
 
-Some callers cannot allocate device memory where they call the library (a
-stream being captured into a CUDA graph, a foreign runtime that only hands
-over its own buffers, a fixed memory budget). For them vp_poisson2d_static
+Some callers cannot allocate device memory where they call the library: a
+foreign runtime that owns all device memory and only hands over its own input
+and output buffers, or an embedded solver whose device footprint is fixed at
+start-up. For them vp_poisson2d_static
 takes no workspace: its scratch is a device array inside the library. This
 test calls it through the C ABI, twice in a row on different grids (the
 second call reuses the scratch the first one left behind), and checks every
