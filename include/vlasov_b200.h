@@ -230,8 +230,8 @@ size_t vp_poisson1d_workspace_bytes(int64_t nx);
  * vlasov_step_gather_free_impl (vlasov2D2V.py:1043-1083):
  * x(dt/2), y(dt/2) fused with rho, Poisson, vx(dt)+vy(dt) fused,
  * y(dt/2), x(dt/2). Where the layout allows (FP32, 16 <= ny <= 128, nvy a
- * multiple of 32, 16-byte aligned buffers, no equilibrium split,
- * sweeps_only == 0) each pair of position drifts runs as one pass over f
+ * multiple of 32, 16-byte aligned buffers, sweeps_only == 0; with or
+ * without the equilibrium split) each pair of position drifts runs as one pass over f
  * with the intermediate on chip: f is the same bits, rho is summed in
  * another (fixed) order. With physics_mode == 0 the field is zero, the
  * kicks are the identity and are skipped, and drho/phi are zeroed (as the
@@ -299,8 +299,7 @@ size_t vp_step2d_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nv
  * of passes over f (each reads and writes f once; < 0 on a bad descriptor)
  * and sets *plane_fused (may be NULL) to 1 when the position drifts go in
  * pairs through the fused (x, y) plane passes (FP32 storage, 16 <= ny <=
- * 128, nvy a multiple of 32, 16-byte aligned buffers, no equilibrium
- * split). No counterpart in the reference, whose drifts are separate tensor
+ * 128, nvy a multiple of 32, 16-byte aligned buffers). No counterpart in the reference, whose drifts are separate tensor
  * operations; it tells a caller how much HBM traffic one step moves. */
 int vp_step2d_passes(const vp_step2d_desc* desc, int32_t* plane_fused);
 

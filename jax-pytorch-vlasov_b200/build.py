@@ -38,11 +38,26 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the CUDA sources into the package directory (skip if fresh)."""
+    """Compile the CUDA sources into the package directory (skip if fresh).
+    Each translation unit compiles in its own nvcc process (they share no
+    device code), then one nvcc call links the shared library."""
     if not force and not _stale():
         return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    jobs = []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
+        cmd = [_nvcc(), *compile_flags, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        jobs.append((subprocess.Popen(cmd), obj))
+    failed = [obj for p, obj in jobs if p.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed for " + ", ".join(os.path.basename(o) for o in failed))
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, "-o", tmp, *sources()]
+    cmd = [_nvcc(), *NVCC_FLAGS, "-o", tmp, *[obj for _, obj in jobs]]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -310,8 +310,7 @@ size_t vp_step2d_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nv
 
 // the position drifts go through the fused (x, y) plane passes
 static bool step2d_planar(const vp_step2d_desc* d) {
-    const bool eq_on = d->eq_vx || d->eq_vy;
-    return !eq_on && !d->sweeps_only && plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_in) &&
+    return !d->sweeps_only && plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_in) &&
            plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_out) &&
            plane_fits(d->dtype, d->nx, d->ny, d->nvx, d->nvy, d->f_tmp);
 }
@@ -374,8 +373,9 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         dst = dst_of(i++);
         int tiles = 0;
         rc = run_plane(d->dtype, true, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y,
-                       want_rho ? w.part : nullptr, &tiles, d->status, d->test_stall, st);
-        if (!rc && want_rho) rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, 0.0, w.rho, st);
+                       want_rho ? w.part : nullptr, &tiles, EQ, d->status, d->test_stall, st);
+        if (!rc && want_rho)
+            rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, eq_on ? d->eq_moment : 0.0, w.rho, st);
         if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
         if ((rc = mk.begin(VP_PHASE_DRIFT_Y1)) || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
         src = dst;
@@ -449,7 +449,7 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
         dst = dst_of(i++);
         rc = run_plane(d->dtype, false, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y, nullptr,
-                       nullptr, d->status, d->test_stall, st);
+                       nullptr, EQ, d->status, d->test_stall, st);
         if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     } else {
     // y drift (dt/2)

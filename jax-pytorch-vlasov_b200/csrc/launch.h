@@ -144,17 +144,20 @@ int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t n
                const double* Ey, double dt, double dvx, double dvy, int window, const double* vx,
                const double* vy, double* moments, const EqSplit* eq, cudaStream_t st);
 bool kick2d_fits(int dtype, int64_t nvy, const void* a, const void* b, const void* c);
-// Both position drifts of f[nx][ny][nvx][nvy] in one pass (x then y, or y
-// then x), with the density row sums of x-then-y into part
-// ([nx][plane_part_tiles][ny], tiles returned) when part is not null.
 // f[p][v] = S[p] * V[v] (FP64 product, rounded once to the storage type)
 int run_init_product(int dtype, const double* S, const double* V, void* f, int64_t n_points, int64_t n_v,
                      cudaStream_t st);
+// Both position drifts of f[nx][ny][nvx][nvy] in one pass (x then y, or y
+// then x), with the density row sums of x-then-y into part
+// ([nx][plane_part_tiles][ny], tiles returned) when part is not null. With
+// eq (equilibrium split, eq->A and eq->B both set) each drift of the stored
+// perturbation g adds feq * (sum of the column's weights - 1), as the
+// single-axis sweeps do.
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* in);
 int64_t plane_part_tiles(int64_t nvx, int64_t nvy);
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
               const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
-              int* status, int stall, cudaStream_t st);
+              const EqSplit* eq, int* status, int stall, cudaStream_t st);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                     int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,

@@ -38,6 +38,10 @@
 //    per thread, the x window of the 21 rows its y drift reads kept in
 //    registers (the 5 rows past a warp's own are recomputed), so neither a
 //    plane exchange nor a per-row barrier is needed; same partials layout.
+//  * Equilibrium split (EQ; the state holds g = f - A(vx) B(vy)): each drift
+//    adds the per-column constant feq * (sum of the column's 6 weights - 1)
+//    after its 6 taps, in the same operations as the single-axis sweep, so
+//    the split passes stay bit-identical to the split sweeps.
 // A wait that runs out (1 s) makes the CTA wait for its stores, fill its
 // whole share of the output (and its density partials) with NaN, wait
 // (bounded) for its loads in flight and leave, so a failure shows in the
@@ -76,6 +80,8 @@ struct Args {
     const int* shift_y;
     const float* W_y;   // [6][nvy]
     double* part;       // [nx][n_cg][ny] FP64 row sums (x first with the density)
+    const double* eqA;  // equilibrium split feq = eqA[vx] * eqB[vy] (EQ kernels)
+    const double* eqB;
     int* status;        // optional: VP_STATUS_WAIT_TIMEOUT ORed in by a CTA whose wait ran out
     int stall;          // test hook: the first load of each CTA expects 16 bytes too many
 };
@@ -195,24 +201,47 @@ __device__ __forceinline__ float2 taps(const float2 (&w)[6], float2 t0, float2 t
     return __ffma2_rn(w[0], t0, acc);
 }
 
+// the split's constant after the taps (a plain FP32 add per row, as the
+// single-axis sweep adds it)
+template <bool EQ>
+__device__ __forceinline__ float2 plus(float2 o, float b) {
+    if constexpr (EQ) {
+        o.x += b;
+        o.y += b;
+    }
+    return o;
+}
+
+// the split's constant of a lane's column: feq * (sum of its 6 weights - 1),
+// the weights summed from tap 5 down to tap 0 in FP64, rounded once
+__device__ __forceinline__ float split_bias(double feq, const float2 (&w)[6]) {
+    double s = -1.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) s += (double)w[j].x;
+    return (float)(feq * s);
+}
+
 // y drift of the thread's 8 rows from 13 consecutive rows of a buffer
 // (g: row y0 - s - 3 of the lane's column, halo included)
-__device__ __forceinline__ void y_drift(const float* g, const float2 (&wy)[6], float2 (&o)[YT / 2]) {
+template <bool EQ>
+__device__ __forceinline__ void y_drift(const float* g, const float2 (&wy)[6], float by, float2 (&o)[YT / 2]) {
     float r[YT + 5];
 #pragma unroll
     for (int k = 0; k < YT + 5; ++k) r[k] = g[k * CG];
 #pragma unroll
     for (int p = 0; p < YT / 2; ++p) {
         const int i = 2 * p;
-        o[p] = taps(wy, make_float2(r[i], r[i + 1]), make_float2(r[i + 1], r[i + 2]), make_float2(r[i + 2], r[i + 3]),
-                    make_float2(r[i + 3], r[i + 4]), make_float2(r[i + 4], r[i + 5]), make_float2(r[i + 5], r[i + 6]));
+        o[p] = plus<EQ>(taps(wy, make_float2(r[i], r[i + 1]), make_float2(r[i + 1], r[i + 2]),
+                             make_float2(r[i + 2], r[i + 3]), make_float2(r[i + 3], r[i + 4]),
+                             make_float2(r[i + 4], r[i + 5]), make_float2(r[i + 5], r[i + 6])),
+                        by);
     }
 }
 
 // FULL: ny is a multiple of 8, every thread row is a real row.
 // YM: the most rows the buffers hold (ny <= YM); 64 halves the shared memory
 // so that two CTAs share an SM.
-template <bool XFIRST, bool RHO, bool FULL, int YM>
+template <bool XFIRST, bool RHO, bool FULL, int YM, bool EQ>
 __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     k_plane(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap thalo,
             const __grid_constant__ CUtensorMap tout, const __grid_constant__ Args a) {
@@ -262,6 +291,7 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
 #pragma unroll
         for (int s = 0; s < 6; ++s) win[p][s] = make_float2(0.f, 0.f);
     float2 wx[6], wy[6];
+    float bx = 0.f, by = 0.f;  // the split's constants of the lane's column (EQ)
     int yoff = 0;           // float offset of row y0 - sy - 3 (mod ny), column lane
     uint32_t parity = 0;    // of the current pass over the ring
     long long L = 0;        // loads consumed
@@ -275,7 +305,7 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
     auto y_pending = [&](auto pl) {
         constexpr int PL = decltype(pl)::value;
         float2 o[YT / 2];
-        y_drift(planes + PL * BUF + yoff, wy, o);
+        y_drift<EQ>(planes + PL * BUF + yoff, wy, by, o);
         float* st = stage + PL * STG;
 #pragma unroll
         for (int p = 0; p < YT / 2; ++p) {
@@ -313,6 +343,11 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
             wx[j] = make_float2(u, u);
             wy[j] = make_float2(v, v);
         }
+        if constexpr (EQ) {
+            const double feq = __ldg(a.eqA + jx) * __ldg(a.eqB + jy);
+            bx = split_bias(feq, wx);
+            by = split_bias(feq, wy);
+        }
         int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
         if (r < 0) r += ny;
         yoff = r * CG + lane;
@@ -340,8 +375,9 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
                 float* pl = planes + (P & 1) * BUF;
 #pragma unroll
                 for (int p = 0; p < YT / 2; ++p) {
-                    const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
-                                          win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                    const float2 o = plus<EQ>(taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                                   win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]),
+                                              bx);
                     const int y = y0 + 2 * p;
                     if (FULL || y < ny) pl[y * CG + lane] = o.x;
                     if (FULL || y + 1 < ny) pl[(y + 1) * CG + lane] = o.y;
@@ -353,13 +389,14 @@ __global__ void __launch_bounds__(YM / YT * 32, YMAX / YM)
             }
         } else {
             // y drift of the new row from its slab, then the x drift
-            y_drift(sl + yoff, wy, nv);
+            y_drift<EQ>(sl + yoff, wy, by, nv);
             if (emit) {
                 float* dst = a.out + ((int64_t)(cons.xa + cons.q - 5) * ny + y0) * a.m + (int64_t)cons.cg * CG + lane;
 #pragma unroll
                 for (int p = 0; p < YT / 2; ++p) {
-                    const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
-                                          win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                    const float2 o = plus<EQ>(taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                                   win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]),
+                                              bx);
                     const int y = y0 + 2 * p;
                     if (FULL || y < ny) dst[(int64_t)(2 * p) * a.m] = o.x;
                     if (FULL || y + 1 < ny) dst[(int64_t)(2 * p + 1) * a.m] = o.y;
@@ -521,7 +558,7 @@ __device__ __forceinline__ float tap1(const float2 (&w)[6], float t0, float t1, 
 constexpr int RSTRIDE = CG + 4;
 constexpr int RFLOATS = YT2 * RSTRIDE;
 
-template <bool RHO, bool FULL, int YM>
+template <bool RHO, bool FULL, int YM, bool EQ>
 __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
     k_plane_xr(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap thalo,
                const __grid_constant__ Args a) {
@@ -571,6 +608,7 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
         wl[s] = 0.f;
     }
     float2 wx[6], wy[6];
+    float bx = 0.f, by = 0.f;  // the split's constants of the lane's column (EQ)
     int yoff = 0;  // float offset of row y0 - sy - 3 (mod ny), column lane
     uint32_t parity = 0;
     long long L = 0;
@@ -604,6 +642,11 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
             wx[j] = make_float2(u, u);
             wy[j] = make_float2(v, v);
         }
+        if constexpr (EQ) {
+            const double feq = __ldg(a.eqA + jx) * __ldg(a.eqB + jy);
+            bx = split_bias(feq, wx);
+            by = split_bias(feq, wy);
+        }
         int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
         if (r < 0) r += ny;
         yoff = r * CG + lane;
@@ -624,20 +667,23 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
             float xd[WR];
 #pragma unroll
             for (int p = 0; p < WR / 2; ++p) {
-                const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
-                                      win[p][(P + 4) % 6], win[p][(P + 5) % 6], win[p][P]);
+                const float2 o = plus<EQ>(taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                               win[p][(P + 4) % 6], win[p][(P + 5) % 6], win[p][P]),
+                                          bx);
                 xd[2 * p] = o.x;
                 xd[2 * p + 1] = o.y;
             }
             xd[WR - 1] = tap1(wx, wl[(P + 1) % 6], wl[(P + 2) % 6], wl[(P + 3) % 6], wl[(P + 4) % 6],
                               wl[(P + 5) % 6], wl[P]);
+            if constexpr (EQ) xd[WR - 1] += bx;
             float o16[YT2];
 #pragma unroll
             for (int p = 0; p < YT2 / 2; ++p) {
                 const int i = 2 * p;
-                const float2 o = taps(wy, make_float2(xd[i], xd[i + 1]), make_float2(xd[i + 1], xd[i + 2]),
-                                      make_float2(xd[i + 2], xd[i + 3]), make_float2(xd[i + 3], xd[i + 4]),
-                                      make_float2(xd[i + 4], xd[i + 5]), make_float2(xd[i + 5], xd[i + 6]));
+                const float2 o = plus<EQ>(taps(wy, make_float2(xd[i], xd[i + 1]), make_float2(xd[i + 1], xd[i + 2]),
+                                               make_float2(xd[i + 2], xd[i + 3]), make_float2(xd[i + 3], xd[i + 4]),
+                                               make_float2(xd[i + 4], xd[i + 5]), make_float2(xd[i + 5], xd[i + 6])),
+                                          by);
                 o16[i] = o.x;
                 o16[i + 1] = o.y;
             }
@@ -749,10 +795,10 @@ static constexpr size_t smem_bytes(bool xfirst, int ym) {
            DEPTH * 8 + sizeof(Producer);
 }
 
-template <bool XFIRST, bool RHO, bool FULL, int YM>
+template <bool XFIRST, bool RHO, bool FULL, int YM, bool EQ>
 static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUtensorMap& tout, const Args& a,
                     cudaStream_t st) {
-    auto kern = k_plane<XFIRST, RHO, FULL, YM>;
+    auto kern = k_plane<XFIRST, RHO, FULL, YM, EQ>;
     constexpr size_t smem = smem_bytes(XFIRST, YM);
     const int block = 32 * ((a.ny + YT - 1) / YT);
     static int raised[64] = {0};
@@ -771,9 +817,9 @@ static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUte
     return check_launch("k_plane");
 }
 
-template <bool RHO, bool FULL, int YM>
+template <bool RHO, bool FULL, int YM, bool EQ>
 static int launch_xr(const CUtensorMap& tin, const CUtensorMap& thalo, const Args& a, cudaStream_t st) {
-    auto kern = k_plane_xr<RHO, FULL, YM>;
+    auto kern = k_plane_xr<RHO, FULL, YM, EQ>;
     constexpr size_t smem = (size_t)(DEPTH * buf2_floats(YM) + (RHO ? 2 * (YM / YT2) * RFLOATS : 0)) * 4 +
                             DEPTH * 8 + sizeof(Producer);
     const int block = 32 * ((a.ny + YT2 - 1) / YT2);
@@ -808,7 +854,7 @@ int64_t plane_part_tiles(int64_t nvx, int64_t nvy) { return nvx * nvy / plane::C
 
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
               const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
-              int* status, int stall, cudaStream_t st) {
+              const EqSplit* eq, int* status, int stall, cudaStream_t st) {
     using namespace plane;
     if (!plane_fits(dtype, nx, ny, nvx, nvy, in) || !plane_fits(dtype, nx, ny, nvx, nvy, out))
         return set_error(VP_ERR_UNSUPPORTED, "run_plane: layout not fused");
@@ -825,6 +871,11 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
     a.shift_y = shift_y;
     a.W_y = static_cast<const float*>(W_y);
     a.part = part;
+    const bool eq_on = eq && eq->A && eq->B;
+    if (eq && !eq_on && (eq->A || eq->B))
+        return set_error(VP_ERR_UNSUPPORTED, "run_plane: the split needs both equilibrium factors");
+    a.eqA = eq_on ? eq->A : nullptr;
+    a.eqB = eq_on ? eq->B : nullptr;
     a.status = status;
     a.stall = stall;
     if (tiles) *tiles = a.n_cg;
@@ -836,31 +887,35 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
         if (!make_map(&tin, in, a.m, nx * ny, (int)ny) || !make_map(&thalo, in, a.m, nx * ny, HALO2))
             return set_error(VP_ERR_CUDA, "run_plane: cuTensorMapEncodeTiled failed");
         const bool full2 = ny % YT2 == 0;
-        auto go2 = [&](auto ym) {
-            constexpr int YM = decltype(ym)::value;
+        auto go2 = [&](auto eqc) {
+            constexpr bool E = decltype(eqc)::value != 0;
             if (part)
-                return full2 ? launch_xr<true, true, YM>(tin, thalo, a, st) : launch_xr<true, false, YM>(tin, thalo, a, st);
-            return full2 ? launch_xr<false, true, YM>(tin, thalo, a, st) : launch_xr<false, false, YM>(tin, thalo, a, st);
+                return full2 ? launch_xr<true, true, YMAX, E>(tin, thalo, a, st)
+                             : launch_xr<true, false, YMAX, E>(tin, thalo, a, st);
+            return full2 ? launch_xr<false, true, YMAX, E>(tin, thalo, a, st)
+                         : launch_xr<false, false, YMAX, E>(tin, thalo, a, st);
         };
-        return go2(Step<YMAX>{});
+        return eq_on ? go2(Step<1>{}) : go2(Step<0>{});
     }
     if (!make_map(&tin, in, a.m, nx * ny, (int)ny) || !make_map(&thalo, in, a.m, nx * ny, HALO) ||
         !make_map(&tout, out, a.m, nx * ny, (int)ny))
         return set_error(VP_ERR_CUDA, "run_plane: cuTensorMapEncodeTiled failed");
     const bool full = ny % YT == 0;
-    auto go = [&](auto ym) {
+    auto go = [&](auto ym, auto eqc) {
         constexpr int YM = decltype(ym)::value;
+        constexpr bool E = decltype(eqc)::value != 0;
         if (xfirst) {
             if (part)
-                return full ? launch_t<true, true, true, YM>(tin, thalo, tout, a, st)
-                            : launch_t<true, true, false, YM>(tin, thalo, tout, a, st);
-            return full ? launch_t<true, false, true, YM>(tin, thalo, tout, a, st)
-                        : launch_t<true, false, false, YM>(tin, thalo, tout, a, st);
+                return full ? launch_t<true, true, true, YM, E>(tin, thalo, tout, a, st)
+                            : launch_t<true, true, false, YM, E>(tin, thalo, tout, a, st);
+            return full ? launch_t<true, false, true, YM, E>(tin, thalo, tout, a, st)
+                        : launch_t<true, false, false, YM, E>(tin, thalo, tout, a, st);
         }
-        return full ? launch_t<false, false, true, YM>(tin, thalo, tout, a, st)
-                    : launch_t<false, false, false, YM>(tin, thalo, tout, a, st);
+        return full ? launch_t<false, false, true, YM, E>(tin, thalo, tout, a, st)
+                    : launch_t<false, false, false, YM, E>(tin, thalo, tout, a, st);
     };
-    return ny <= YMAX / 2 ? go(Step<YMAX / 2>{}) : go(Step<YMAX>{});
+    if (ny <= YMAX / 2) return eq_on ? go(Step<YMAX / 2>{}, Step<1>{}) : go(Step<YMAX / 2>{}, Step<0>{});
+    return eq_on ? go(Step<YMAX>{}, Step<1>{}) : go(Step<YMAX>{}, Step<0>{});
 }
 
 }  // namespace vp

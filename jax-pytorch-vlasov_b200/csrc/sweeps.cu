@@ -607,6 +607,10 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
     const bool lane_ok = li < a.groups;
     const int nvx = a.nvx, nvy = a.nvy, groups = a.groups;
     C* rowbuf = reinterpret_cast<C*>(smem_raw) + (size_t)tid_team * KK * nvy;
+    // equilibrium split: the team's tables of (Kx A - A)(vx) for its plane
+    // and of A(vx), after all teams' row buffers
+    C* dAt = reinterpret_cast<C*>(smem_raw) + (size_t)teams_per_block * KK * nvy + (size_t)tid_team * 2 * nvx;
+    C* At = dAt + nvx;
 
     double vy2[VEC];
     if constexpr (DIAG) {
@@ -648,9 +652,12 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         for (int k = 0; k < 6; ++k) wx2[k] = make_float2((float)wx[k], (float)wx[k]);
         // equilibrium split: the kicks of feq = A(vx) B(vy) add
         // (Kx A - A)(vx) B(vy) after the vx kick and A(vx) (Ky B - B)(vy) after
-        // the vy kick (K: the plane's kick operator, zero outside the grid)
+        // the vy kick (K: the plane's kick operator, zero outside the grid).
+        // Both factors are evaluated in FP64 and rounded to the compute type;
+        // each term is one more FMA after the element's 6 taps.
         double Be[EQ ? VEC : 1], dBe[EQ ? VEC : 1];
-        if constexpr (EQ) {
+        C Bc[EQ ? VEC : 1], dBc[EQ ? VEC : 1];
+        auto eq_factors = [&]() {
 #pragma unroll
             for (int e = 0; e < VEC; ++e) {
                 const int iv = li * VEC + e;
@@ -662,8 +669,10 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                     if (lane_ok && j >= 0 && j < nvy) k_b = fma(wyd[k], a.eqB[j], k_b);
                 }
                 dBe[e] = k_b - Be[e];
+                Bc[e] = C(Be[e]);
+                dBc[e] = C(dBe[e]);
             }
-        }
+        };
         auto dA_row = [&](int row) -> double {
             double k_a = 0.0;
 #pragma unroll
@@ -673,6 +682,19 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
             }
             return k_a - a.eqA[row];
         };
+        // the split's factors: before the first loads when the moments need
+        // them there, else after the first loads are in flight
+        auto eq_setup = [&]() {
+            eq_factors();
+            // the previous plane's readers of the table are past the
+            // warp barrier that ends its last chunk
+            for (int row = li; row < nvx; row += team) {
+                dAt[row] = pv ? C(dA_row(row)) : C(0);
+                At[row] = C(a.eqA[row]);
+            }
+            __syncwarp();
+        };
+        if constexpr (EQ && DIAG) eq_setup();
         // vy window of the lane's first element starts gshift elements away:
         // group offset gd (floor division) and element remainder r in [0, 4)
         const int gshift = -sy - 3;
@@ -706,14 +728,15 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
         int rnext = r0 + 5;
         // 4-byte and 2-byte storage load each chunk's rows one chunk ahead
         // (under the previous chunk's vy kick); 8-byte storage and the
-        // split / moment variants would spill and load them in place
-        constexpr bool AHEAD = sizeof(TS) <= 4 && !EQ && !DIAG;
+        // moment variant would spill and load them in place
+        constexpr bool AHEAD = sizeof(TS) <= 4 && !DIAG;
         R nx[KK];
         if constexpr (AHEAD) {
 #pragma unroll
             for (int u = 0; u < KK; ++u) nx[u] = load_row(rnext + u);
             rnext += KK;
         }
+        if constexpr (EQ && !DIAG) eq_setup();
 
         for (int l = 0; l < nvx; l += KK) {
             if constexpr (!AHEAD) {
@@ -726,9 +749,9 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
             for (int u = 0; u < KK; ++u) {
                 C rv[VEC];
-                double dA = 0.0;
-                if constexpr (EQ) dA = (l + u < nvx) ? dA_row(l + u) : 0.0;
-                if constexpr (std::is_same<C, float>::value && VEC % 2 == 0 && !EQ && !DIAG) {
+                C dA = C(0);
+                if constexpr (EQ) dA = dAt[min(l + u, nvx - 1)];
+                if constexpr (std::is_same<C, float>::value && VEC % 2 == 0 && !DIAG) {
                     // pairs of elements through the paired FMA (same IEEE
                     // operations per lane)
 #pragma unroll
@@ -744,6 +767,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                         acc = __ffma2_rn(wx2[3], g2(u + 2), acc);
                         acc = __ffma2_rn(wx2[4], g2(u + 1), acc);
                         acc = __ffma2_rn(wx2[5], g2(u + 0), acc);
+                        if constexpr (EQ) acc = __ffma2_rn(make_float2(dA, dA), make_float2(Bc[2 * h], Bc[2 * h + 1]), acc);
                         rv[2 * h] = as_stored<TS>(acc.x);
                         rv[2 * h + 1] = as_stored<TS>(acc.y);
                     }
@@ -757,7 +781,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                         acc = fma(wx[3], g(u + 2), acc);
                         acc = fma(wx[4], g(u + 1), acc);
                         acc = fma(wx[5], g(u + 0), acc);
-                        if constexpr (EQ) acc += C(dA * Be[e]);
+                        if constexpr (EQ) acc = fma(dA, Bc[e], acc);
                         rv[e] = as_stored<TS>(acc);
                     }
                 }
@@ -828,11 +852,9 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
                     }
                 }
                 if constexpr (EQ) {
-                    if (l + u < nvx) {
-                        const double A = a.eqA[l + u];
+                    const C A = At[min(l + u, nvx - 1)];
 #pragma unroll
-                        for (int e = 0; e < VEC; ++e) rres.v[e] += C(A * dBe[e]);
-                    }
+                    for (int e = 0; e < VEC; ++e) rres.v[e] = fma(A, dBc[e], rres.v[e]);
                 }
                 if (active && l + u < nvx) {
                     stv<TS, VEC>(dst + (int64_t)(l + u) * nvy, rres);
@@ -900,7 +922,8 @@ __global__ void __launch_bounds__(kBlock, 2)
 template <typename TS, int VEC, bool DIAG, bool EQ>
 static int launch_kick2d_t(Kick2dArgs a, cudaStream_t st) {
     const int teams = kBlock / a.team;
-    const size_t smem = (size_t)teams * kick2d_rows<TS, VEC>() * a.nvy * sizeof(compute_t<TS>);
+    const size_t smem =
+        (size_t)teams * (kick2d_rows<TS, VEC>() * a.nvy + (EQ ? 2 * a.nvx : 0)) * sizeof(compute_t<TS>);
     auto kern = k_kick2d<TS, VEC, DIAG, EQ>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

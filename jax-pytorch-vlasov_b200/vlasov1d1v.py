@@ -14,9 +14,10 @@ import torch
 from . import _lib as L
 from . import ops
 from .engine import Stepper1D
-from .vlasov2d2v import (STENCIL_OFFSETS, _blocks_to_shift, _check_offsets, check_v_window,  # noqa: F401
-                         get_lagrange5_weights, lagrange5_interp_sum, lagrange5_weights, precompute_x_drift,
-                         static_stencil_offsets)
+from . import vlasov2d2v as _v2
+from .vlasov2d2v import (STENCIL_OFFSETS, _blocks_to_shift, _check_offsets, build_v_tap_weights,  # noqa: F401
+                         check_v_window, get_lagrange5_weights, lagrange5_interp_sum, lagrange5_weights,
+                         precompute_x_drift, static_stencil_offsets)
 
 
 def _default_device():
@@ -129,6 +130,35 @@ def advect_1d_matrix_diag(f_batch, velocities, dt, dx, stencil_offsets, periodic
         table = ops.DriftTable.from_velocity(velocities, dt, dx, f_batch.dtype, f_batch.device)
         return ops.drift(f_batch.contiguous(), table, 0, 1)
     return ops.kick(f_batch.contiguous(), velocities, dt, dx, 1, window=-1)
+
+
+def _roll_columns(x, shifts):
+    """out[i, j] = x[(i - shifts[j]) % N, j] for x [N, M] (_roll_columns,
+    vlasov1D1V.py:258-267): a periodic sweep along dim 0 whose departure
+    points are whole cells (unit weight on the zero-offset tap, so finite
+    values move unchanged). Floating-point x only."""
+    if x.dim() != 2:
+        raise ValueError("x must be [N, M]")
+    v = shifts.to(L.compute_dtype(x.dtype))
+    return ops.advect_gather(x.contiguous(), v, 0, 1.0, 1.0, True, vel_strides=(0, 0, 1))
+
+
+def _roll_rows(x, shifts):
+    """out[i, j] = x[i, (j - shifts[i]) % M] (_roll_rows, vlasov1D1V.py:269-277)."""
+    return _v2._roll_batch(x, shifts)
+
+
+def build_v_diag_weights(stencil_offsets, shifts, alpha, n_points):
+    """Banded Dirichlet weights [6, Nx, Nv] of the v sweep
+    (build_v_diag_weights, vlasov1D1V.py:279-296)."""
+    return _v2.build_diag_weights(stencil_offsets, shifts, alpha, n_points)
+
+
+def block_roll(f, blocks):
+    """Roll each column block (start, stop, shift) of precompute_x_drift
+    along x (block_roll, vlasov1D1V.py:389-406), by the drift kernel with a
+    unit weight on the zero-offset tap."""
+    return _v2.block_roll(f, blocks, 0, 1)
 
 
 def advect_x_static(f, W_x, blocks, stencil_offsets):

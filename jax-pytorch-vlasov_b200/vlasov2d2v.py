@@ -201,6 +201,65 @@ def advect_1d(f_data, velocities, axis, dt, dx, periodic=True, point_indices=Non
     return ops.advect_gather(f_data, velocities, axis, dt, dx, periodic)
 
 
+def advect_1d_vectorized(f_batch, velocities, dt, dx, point_indices=None, stencil_offsets=None, periodic=True):
+    """Batched sweep along the last dim of f_batch [B, N] with per-row ([B])
+    or per-element ([B, N]) velocities (advect_1d_vectorized,
+    vlasov2D2V.py:287-353), by the per-element departure kernel. The grid
+    points are 0 .. N-1 (the reference's default point_indices, the only ones
+    its callers pass)."""
+    _check_offsets(stencil_offsets)
+    if f_batch.dim() != 2:
+        raise ValueError("f_batch must be [batch, n_points]")
+    B, N = f_batch.shape
+    if point_indices is not None and tuple(point_indices.shape) != (N,):
+        raise ValueError("point_indices must be the N grid indices 0 .. N-1")
+    f_batch = f_batch.contiguous()
+    v = velocities
+    if v.dim() == 1:
+        return ops.advect_gather(f_batch, v, 1, dt, dx, periodic, vel_strides=(1, 0, 0))
+    return ops.advect_gather(f_batch, v.expand(B, N), 1, dt, dx, periodic, vel_strides=(N, 1, 0))
+
+
+def _roll_batch(x, shifts):
+    """out[i, j] = x[i, (j - shifts[i]) % N] for x [B, N] (_roll_batch,
+    vlasov2D2V.py:526-535): a periodic sweep whose departure points are whole
+    cells. At a zero fraction the Lagrange weights are exactly (0, 0, 1, 0,
+    0, 0), so every finite value moves unchanged. Floating-point x only."""
+    if x.dim() != 2:
+        raise ValueError("x must be [batch, n_points]")
+    v = shifts.to(L.compute_dtype(x.dtype))
+    return ops.advect_gather(x.contiguous(), v, 1, 1.0, 1.0, True, vel_strides=(1, 0, 0))
+
+
+def build_diag_weights(stencil_offsets, shifts, alpha, n_points):
+    """Banded weights [6, B, n_points] of the Dirichlet per-row sweep
+    (build_diag_weights, vlasov2D2V.py:538-555): tap k of row b carries
+    w_k(alpha_b) at the points j whose source j - shifts[b] - o_k lies inside
+    the line, zero elsewhere."""
+    offs = torch.as_tensor(static_stencil_offsets(stencil_offsets), dtype=torch.int64, device=alpha.device)
+    W = lagrange5_weights(alpha)                                   # [6, B]
+    j = torch.arange(n_points, device=alpha.device)
+    src = j[None, None, :] - (offs[:, None] + shifts.to(torch.int64)[None, :])[..., None]
+    inside = (src >= 0) & (src < n_points)
+    return torch.where(inside, W[..., None], torch.zeros((), dtype=W.dtype, device=W.device))
+
+
+def advect_1d_matrix_diag_core(f_batch, velocities, dt, dx, stencil_offsets, periodic=True):
+    """Per-row sweep of f_batch [B, N] with one velocity per row
+    (advect_1d_matrix_diag_core, vlasov2D2V.py:558-589): shift s = floor(d)
+    and fraction of d = v dt / dx per row. Dirichlet rows (zero outside) run
+    the kick kernel, which uses exactly this shift and fraction; periodic rows
+    run the per-element departure kernel (the same interpolant, round-off
+    apart)."""
+    _check_offsets(stencil_offsets)
+    if f_batch.dim() != 2:
+        raise ValueError("f_batch must be [batch, n_points]")
+    f_batch = f_batch.contiguous()
+    if periodic:
+        return ops.advect_gather(f_batch, velocities.reshape(-1), 1, dt, dx, True, vel_strides=(1, 0, 0))
+    return ops.kick(f_batch, velocities.reshape(-1), dt, dx, 1, window=-1)
+
+
 def _line_velocity_structure(f_data, velocities, axis):
     """If velocities (broadcast to the batch shape) depend on a single dim
     of f after `axis` (a drift) or only on the dims before `axis` (a kick),
@@ -238,6 +297,53 @@ def advect_1d_matrix_diag(f_data, velocities, axis, dt, dx, periodic=True, point
     if st is not None and st[0] == "kick" and not periodic and axis > 0:
         return ops.kick(f_data, st[1].contiguous(), dt, dx, axis, window=-1)
     return ops.advect_gather(f_data, velocities, axis, dt, dx, periodic)
+
+
+def _unit_table(blocks, n, dtype, device):
+    """Drift table of whole-cell shifts: weight 1 on the tap at offset 0."""
+    W = np.zeros((6, n), dtype=np.float64)
+    W[STENCIL_OFFSETS.index(0)] = 1.0
+    return ops.DriftTable(_blocks_to_shift(blocks, n), W, dtype, device)
+
+
+def block_roll(f_data, blocks, axis, vel_axis):
+    """Roll each velocity block (start, stop, shift) of precompute_x_drift by
+    its whole-cell shift along the spatial `axis` (block_roll,
+    vlasov2D2V.py:717-753): the periodic drift kernel with a unit weight on
+    the zero-offset tap, so every finite value moves unchanged. Returns f_data
+    itself when no shift moves anything, as the reference does."""
+    if vel_axis <= axis:
+        raise ValueError("the velocity axis of the blocks must come after the rolled axis")
+    if all(sh % f_data.shape[axis] == 0 for _, _, sh in blocks):
+        return f_data
+    table = _unit_table(blocks, f_data.shape[vel_axis], f_data.dtype, f_data.device)
+    return ops.drift(f_data.contiguous(), table, axis, vel_axis)
+
+
+def build_v_tap_weights(E, dt, dv, S, stencil_offsets):
+    """Tap weights of the static kick window (build_v_tap_weights,
+    vlasov2D2V.py:822-865; vlasov1D1V.py:450-476): shape (2S+5, *E.shape),
+    row m + S + 2 holding w_k(alpha) where floor(E dt / dv) + o_k = m. Each
+    row takes at most one weight, so the table is exact. The small table is
+    built on the host with correctly rounded division (a CUDA tensor divided
+    by a Python number is multiplied by its reciprocal instead, which can
+    move the fraction by one unit in the last place); the weights are the
+    reference's closed form."""
+    Eh = E.detach().cpu()
+    d = (Eh * dt) / dv
+    s = torch.floor(d)
+    alpha = d - s
+    s = s.to(torch.int64)
+    W6 = lagrange5_weights(alpha)
+    offs = static_stencil_offsets(stencil_offsets)
+    zero = torch.zeros((), dtype=W6.dtype)
+    rows = []
+    for m in range(-(S + 2), S + 3):
+        row = torch.zeros_like(alpha)
+        for k, o in enumerate(offs):
+            row = torch.where(s == m - o, W6[k], row)
+        rows.append(torch.where(row == 0, zero, row))
+    return torch.stack(rows, dim=0).to(E.device)
 
 
 def advect_x_static(f_data, W, blocks, stencil_offsets, axis):

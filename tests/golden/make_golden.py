@@ -303,6 +303,53 @@ def gen_1d():
     save("oned", **out)
 
 
+def gen_helpers():
+    """The reference's smaller public helpers of both modules: block_roll,
+    build_v_tap_weights, the batched 2D sweep advect_1d_vectorized, the
+    per-row form advect_1d_matrix_diag_core and its roll / banded-weight
+    helpers, on seeded inputs. Inputs are regenerated from the seeds."""
+    out = {}
+    for dt_name in ("f64", "f32"):
+        T = TD[dt_name]
+        g = grid2(SMALL, dt_name)
+        f = rng_f(21, (g.Nx, g.Ny, g.Nvx, g.Nvy), dt_name)
+        for axis, vel in ((0, g.vx), (1, g.vy)):
+            h = g.dx if axis == 0 else g.dy
+            blocks, _ = R2.precompute_x_drift(vel * 3.1, 0.1, h, T)
+            out[f"broll_{dt_name}_a{axis}"] = R2.block_roll(f, blocks, axis, axis + 2)
+        E = (0.7 * torch.sin(torch.arange(g.Nx * g.Ny, dtype=T).reshape(g.Nx, g.Ny))).to(T)
+        for S in (1, 2):
+            out[f"vtap_{dt_name}_S{S}"] = R2.build_v_tap_weights(E, 0.1, g.dvx, S, g.stencil_offsets)
+        B, N = 7, 19
+        fb = rng_f(22, (B, N), dt_name)
+        vb = torch.linspace(-3.0, 4.0, B, dtype=T)
+        ve = (2.5 * torch.cos(torch.arange(B * N, dtype=T) * 0.37).reshape(B, N)).to(T)
+        for per in (True, False):
+            tag = "p" if per else "d"
+            out[f"avec_{dt_name}_rows_{tag}"] = R2.advect_1d_vectorized(fb, vb, 0.1, 0.25, periodic=per)
+            out[f"avec_{dt_name}_elem_{tag}"] = R2.advect_1d_vectorized(fb, ve, 0.1, 0.25, periodic=per)
+            out[f"mdcore_{dt_name}_{tag}"] = R2.advect_1d_matrix_diag_core(fb, vb, 0.1, 0.25, g.stencil_offsets,
+                                                                          periodic=per)
+        sh = torch.tensor([-3, 0, 2, 5, -7, 19, 40], dtype=torch.int64)
+        out[f"rollb_{dt_name}"] = R2._roll_batch(fb, sh)
+        al = torch.linspace(0.05, 0.95, B, dtype=T)
+        out[f"dw_{dt_name}"] = R2.build_diag_weights(g.stencil_offsets, sh, al, N)
+        # 1D1V forms
+        g1 = R1.Grid.create(24, 20, 4.0 * math.pi, 5.0, device="cpu", dtype=T)
+        f1 = rng_f(23, (24, 20), dt_name)
+        blocks1, _ = R1.precompute_x_drift(g1.v * 2.3, 0.1, g1.dx, T)
+        out[f"broll1_{dt_name}"] = R1.block_roll(f1, blocks1)
+        E1 = (0.9 * torch.sin(torch.arange(24, dtype=T))).to(T)
+        out[f"vtap1_{dt_name}"] = R1.build_v_tap_weights(E1, 0.1, g1.dv, 1, g1.stencil_offsets)
+        shc = torch.arange(20, dtype=torch.int64) - 9
+        shr = torch.arange(24, dtype=torch.int64) * 3 - 30
+        out[f"rollc1_{dt_name}"] = R1._roll_columns(f1, shc)
+        out[f"rollr1_{dt_name}"] = R1._roll_rows(f1, shr)
+        al1 = torch.linspace(0.1, 0.9, 24, dtype=T)
+        out[f"vdw1_{dt_name}"] = R1.build_v_diag_weights(g1.stencil_offsets, shr, al1, 20)
+    save("helpers", **out)
+
+
 def gen_history_1d(tag, nx, nv, L, vmax, eps, dt, steps):
     g = R1.Grid.create(nx, nv, L, vmax, device="cpu", dtype=torch.float64)
     f = (1.0 + eps * torch.cos(2 * math.pi / L * g.x))[:, None] * (
@@ -331,6 +378,7 @@ def main():
         "poisson": gen_poisson,
         "steps": gen_steps,
         "oned": gen_1d,
+        "helpers": gen_helpers,
         "c1": lambda: gen_history("c1", c1, 0.1, 100, lambda g: landau_ref(g, 0.01, 0.5), snap_every=25),
         "oned_landau": lambda: gen_history_1d("oned_landau", 128, 128, 4 * math.pi, 6.0, 0.01, 0.1, 200),
     }

@@ -51,6 +51,40 @@ def test_plane_density(vp, shape):
     np.testing.assert_allclose(st.drho.cpu().numpy(), rho.cpu().numpy() - 1.0, rtol=0, atol=1e-12)
 
 
+SPLIT_SHAPES = [(16, 16, 32, 32), (12, 100, 4, 32), (64, 128, 16, 128), (5, 17, 3, 32), (4, 65, 2, 32),
+                (6, 120, 2, 32), (5, 113, 3, 64)]
+
+
+@pytest.mark.parametrize("shape", SPLIT_SHAPES)
+def test_plane_pairs_equal_sweeps_split(vp, shape):
+    """Equilibrium split (the state holds g = f - A(vx) B(vy)): the fused
+    passes add each column's split constant exactly as the single-axis
+    sweeps do, so the drifts of g are the same bits."""
+    Nx, Ny, Nvx, Nvy = shape
+    args = (Nx, Ny, Nvx, Nvy, 4 * math.pi, 3.0, 6.0, 5.0, 0.7)
+    a = vp.Stepper2D(*args, dtype=torch.float32, physics_mode=False, equilibrium="maxwellian")
+    b = vp.Stepper2D(*args, dtype=torch.float32, physics_mode=False, equilibrium="maxwellian", fuse_drifts=False)
+    g = 0.01 * seeded(shape, 9)
+    assert a.passes(g, a.empty_f()) == (2, True)
+    assert b.passes(g, b.empty_f()) == (4, False)
+    assert torch.equal(a.step(g), b.step(g))
+
+
+@pytest.mark.parametrize("shape", [(16, 32, 8, 64), (8, 128, 4, 128)])
+def test_fused_and_sweeps_only_split_steps(vp, shape):
+    """A physics step of the split state: fused and single-axis drifts give
+    the same density (the equilibrium's included) to FP64 summation order,
+    and f to FP32 rounding."""
+    args = (*shape, 4 * math.pi, 4 * math.pi, 6.0, 6.0, 0.3)
+    a = vp.Stepper2D(*args, dtype=torch.float32, equilibrium="maxwellian")
+    b = vp.Stepper2D(*args, dtype=torch.float32, equilibrium="maxwellian", fuse_drifts=False)
+    g = 0.01 * seeded(shape, 13)
+    assert a.passes(g, a.empty_f()) == (3, True)
+    ga, gb = a.step(g), b.step(g)
+    np.testing.assert_allclose(a.drho.cpu().numpy(), b.drho.cpu().numpy(), rtol=0, atol=1e-13)
+    np.testing.assert_allclose(ga.cpu().numpy(), gb.cpu().numpy(), rtol=0, atol=1e-7)
+
+
 def test_plane_graph_replay(vp):
     """Captured steps (the TMA descriptors live in the kernel parameters)
     replay to the eager result."""

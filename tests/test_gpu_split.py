@@ -105,6 +105,9 @@ def test_split_fp32_c2_within_1e5(vp, golden):
     f = O.two_stream_2d(g, 0.001, 0.2, 2.4)
     eq = (0.5 * (maxwell(g.vx - 2.4) + maxwell(g.vx + 2.4)), maxwell(g.vy))
     ref = H["W_E"]
+    st = vp.Stepper2D(n, n, n, n, L, L, 8.0, 8.0, 0.05, dtype=torch.float32, window=1, equilibrium=eq,
+                      precise_tables=True)
+    assert st.passes(st.empty_f(), st.empty_f()) == (3, True)  # the fused passes carry the split
     h = _history(vp, n, L, 8.0, 0.05, 400, f, torch.float32, eq)
     assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-5
     t = 0.05 * np.arange(1, 401)
