@@ -761,6 +761,271 @@ __global__ void __launch_bounds__(YM / YT2 * 32, YMAX / YM)
     }
 }
 
+// ---- x then y with the density on its own warpgroup ---------------------------
+// The x-first pair of k_plane_xr for 113..128 rows when the density is wanted.
+// Warps 0..7 (the drift warps, 16 y rows each) only stage every output row in
+// shared memory next to its global store; warps 8..11 (the density warps, one
+// thread per y row) sum each staged row over its 32 columns in FP64 and store
+// the per-group partial. The FP64 conversions and sums thus run beside the
+// drifts instead of inside their dependency chains. The block barrier that
+// hands back slabs every second row also hands over the staged rows: rows of
+// pair j are staged between barriers j-1 and j and summed between barriers j
+// and j+1 while the drift warps stage pair j+1 into the other two slots.
+// Registers: launched at 168 a thread (384 threads fill the register file);
+// setmaxnreg then gives the drift warpgroups 216 and the density warpgroup 72
+// (256 * 216 + 128 * 72 = 64512 = 384 * 168: the density warps' release
+// covers the drift warps' increase exactly). Each role's code, its tail
+// included, stays inside its own branch so that it is compiled to its own
+// budget. The producer (TMA issue) is the first density thread.
+constexpr int XRD_CW = 8;                // drift warps
+constexpr int XRD_THREADS = 32 * (XRD_CW + 4);
+constexpr int DSTRIDE = CG + 4;          // staged row: 32 floats + 4 of padding (conflict-free 16-byte reads)
+constexpr int DSLOTS = 4;                // staged rows: two pairs
+struct RowMeta {
+    int x, cg, valid, pad;
+};
+__host__ __device__ constexpr size_t xrd_smem_bytes() {
+    return (size_t)(DEPTH * buf2_floats(YMAX) + DSLOTS * YMAX * DSTRIDE) * 4 + DSLOTS * sizeof(RowMeta) + DEPTH * 8 +
+           sizeof(Producer);
+}
+
+template <bool FULL, bool EQ>
+__global__ void __launch_bounds__(XRD_THREADS, 1)
+    k_plane_xrd(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap thalo,
+                const __grid_constant__ Args a) {
+    constexpr int YM = YMAX, BUF = buf2_floats(YM);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* slabs = reinterpret_cast<float*>(smem);            // [DEPTH][BUF]
+    float* stage = slabs + DEPTH * BUF;                        // [DSLOTS][YM][DSTRIDE]
+    RowMeta* meta = reinterpret_cast<RowMeta*>(stage + DSLOTS * YM * DSTRIDE);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(meta + DSLOTS);
+    Producer* prod = reinterpret_cast<Producer*>(bars + DEPTH);
+    const int nx = a.nx, ny = a.ny;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool drift = warp < XRD_CW;
+    constexpr int PTID = XRD_CW * 32;  // producer: the first density thread
+    const int dy = tid - PTID;         // density thread: its y row
+    const int y0 = warp * YT2;
+    Seq cons;
+    cons.init(a, blockIdx.x, gridDim.x);
+    if (!cons.valid()) return;
+    const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
+    const uint32_t in_bytes = (uint32_t)((ny + HALO2) * CG * 4);
+    uint32_t extra = a.stall ? 16u : 0u;  // test hook, first load only
+    auto issue = [&](int d, const Seq& s) {
+        const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
+        const int r = s.row(nx) * ny;
+        expect_bytes(bar, in_bytes + extra);
+        tma_load(&tin, dst, bar, s.cg * CG, r);
+        tma_load(&thalo, dst + (uint32_t)(ny * CG * 4), bar, s.cg * CG, r);
+    };
+    if (tid == PTID) {
+        for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        Seq p = cons;
+        long long n = 0;
+        for (; n < DEPTH && p.valid(); ++n) {
+            issue((int)n, p);
+            extra = 0;
+            p.next(a);
+        }
+        prod->seq = p;
+        prod->issued = n;
+    }
+    if (tid < DSLOTS) meta[tid].valid = 0;
+    __syncthreads();
+
+    uint32_t parity = 0;
+    long long L = 0;
+    bool failed = false, okacc = true;
+    int pp = 0;  // which pair of staging slots the current two rows use
+
+    // density threads: sum the staged rows of slot pair q in FP64 (fixed order)
+    auto density = [&](int q) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            const int slot = 2 * q + h;
+            const RowMeta m = meta[slot];
+            if (m.valid && dy < ny) {
+                const float4* r = reinterpret_cast<const float4*>(stage + ((size_t)slot * YM + dy) * DSTRIDE);
+                double t[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {  // two halves of 16 columns, each a fixed tree
+                    const float4 u0 = r[4 * k], u1 = r[4 * k + 1], u2 = r[4 * k + 2], u3 = r[4 * k + 3];
+                    t[k] = ((((double)u0.x + (double)u0.y) + ((double)u0.z + (double)u0.w)) +
+                            (((double)u1.x + (double)u1.y) + ((double)u1.z + (double)u1.w))) +
+                           ((((double)u2.x + (double)u2.y) + ((double)u2.z + (double)u2.w)) +
+                            (((double)u3.x + (double)u3.y) + ((double)u3.z + (double)u3.w)));
+                }
+                a.part[((int64_t)m.x * a.n_cg + m.cg) * ny + dy] = t[0] + t[1];
+            }
+        }
+    };
+
+    // the register budget of each role holds inside its own branch
+    if (drift) {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 216;" ::: "memory");
+        float2 win[WR / 2][6];  // rows 0..19 of the window, in pairs
+        float wl[6];            // row 20
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+#pragma unroll
+            for (int p = 0; p < WR / 2; ++p) win[p][s] = make_float2(0.f, 0.f);
+            wl[s] = 0.f;
+        }
+        float2 wx[6], wy[6];
+        float bx = 0.f, by = 0.f;
+        int yoff = 0;
+        auto tables = [&]() {
+            const int jx = (int)(((int64_t)cons.cg * CG / a.nvy) % a.nvx);
+            const int jy = (int)(((int64_t)cons.cg * CG) % a.nvy) + lane;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
+                wx[j] = make_float2(u, u);
+                wy[j] = make_float2(v, v);
+            }
+            if constexpr (EQ) {
+                const double feq = __ldg(a.eqA + jx) * __ldg(a.eqB + jy);
+                bx = split_bias(feq, wx);
+                by = split_bias(feq, wy);
+            }
+            int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
+            if (r < 0) r += ny;
+            yoff = r * CG + lane;
+        };
+        tables();
+
+        auto body = [&](auto step) -> bool {
+            constexpr int P = decltype(step)::value;
+            const bool ok = wait_phase(bar0 + 8 * P, parity);
+            const float* sl = slabs + P * BUF + yoff;
+#pragma unroll
+            for (int p = 0; p < WR / 2; ++p) win[p][P] = make_float2(sl[(2 * p) * CG], sl[(2 * p + 1) * CG]);
+            wl[P] = sl[(WR - 1) * CG];
+            const bool emit = cons.q >= 5;
+            const int slot = 2 * pp + (P & 1);
+            const int x = cons.xa + cons.q - 5;
+            if (emit) {
+                float xd[WR];
+#pragma unroll
+                for (int p = 0; p < WR / 2; ++p) {
+                    const float2 o = plus<EQ>(taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                                   win[p][(P + 4) % 6], win[p][(P + 5) % 6], win[p][P]),
+                                              bx);
+                    xd[2 * p] = o.x;
+                    xd[2 * p + 1] = o.y;
+                }
+                xd[WR - 1] = tap1(wx, wl[(P + 1) % 6], wl[(P + 2) % 6], wl[(P + 3) % 6], wl[(P + 4) % 6],
+                                  wl[(P + 5) % 6], wl[P]);
+                if constexpr (EQ) xd[WR - 1] += bx;
+                float o16[YT2];
+#pragma unroll
+                for (int p = 0; p < YT2 / 2; ++p) {
+                    const int i = 2 * p;
+                    const float2 o =
+                        plus<EQ>(taps(wy, make_float2(xd[i], xd[i + 1]), make_float2(xd[i + 1], xd[i + 2]),
+                                      make_float2(xd[i + 2], xd[i + 3]), make_float2(xd[i + 3], xd[i + 4]),
+                                      make_float2(xd[i + 4], xd[i + 5]), make_float2(xd[i + 5], xd[i + 6])),
+                                 by);
+                    o16[i] = o.x;
+                    o16[i + 1] = o.y;
+                }
+                float* dst = a.out + ((int64_t)x * ny + y0) * a.m + (int64_t)cons.cg * CG + lane;
+                float* st = stage + ((size_t)slot * YM + y0) * DSTRIDE + lane;
+#pragma unroll
+                for (int e = 0; e < YT2; ++e)
+                    if (FULL || y0 + e < ny) {
+                        dst[(int64_t)e * a.m] = o16[e];
+                        st[e * DSTRIDE] = o16[e];
+                    }
+            }
+            if (tid == 0) {
+                meta[slot] = RowMeta{x, cons.cg, emit ? 1 : 0, 0};
+                if (!(P & 1)) meta[slot + 1].valid = 0;  // a pair may end after one row
+            }
+            okacc = okacc && ok;
+            if (P & 1) {
+                if (__syncthreads_or(!okacc)) {
+                    failed = true;
+                    return false;
+                }
+                pp ^= 1;
+            }
+            if (P == DEPTH - 1) parity ^= 1u;
+            ++L;
+            cons.next(a);
+            if (cons.valid() && cons.q == 0) tables();
+            return cons.valid();
+        };
+        while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
+               body(Step<5>{})) {
+        }
+        // a wait on a last, even row has had no barrier vote yet
+        if (!failed && __syncthreads_or(!okacc)) failed = true;
+        if (failed) {
+            // the whole share reads NaN (after this barrier no store of a
+            // row lands any more)
+            __syncthreads();
+            Seq z;
+            z.init(a, blockIdx.x, gridDim.x);
+            while (z.valid()) {
+                if (z.q >= 5) {
+                    const int x = z.xa + z.q - 5;
+                    for (int i = 0; i < YT2 && y0 + i < ny; ++i) {
+                        a.out[((int64_t)x * ny + y0 + i) * a.m + (int64_t)z.cg * CG + lane] = NAN;
+                        if (lane == 0) a.part[((int64_t)x * a.n_cg + z.cg) * ny + y0 + i] = (double)NAN;
+                    }
+                }
+                z.next(a);
+            }
+        }
+    } else {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 72;" ::: "memory");
+        // the density warpgroup: the same steps and barriers, no waits
+        auto body = [&](auto step) -> bool {
+            constexpr int P = decltype(step)::value;
+            if (P & 1) {
+                if (__syncthreads_or(0)) {
+                    failed = true;
+                    return false;
+                }
+                if (tid == PTID) {  // slabs P-1 and P are free
+                    Seq& p = prod->seq;
+#pragma unroll
+                    for (int d = P - 1; d <= P; ++d)
+                        if (p.valid()) {
+                            issue(d, p);
+                            p.next(a);
+                            prod->issued += 1;
+                        }
+                }
+                density(pp);
+                pp ^= 1;
+            }
+            if (P == DEPTH - 1) parity ^= 1u;
+            ++L;
+            cons.next(a);
+            return cons.valid();
+        };
+        while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
+               body(Step<5>{})) {
+        }
+        // the drift warps' last vote (the same barrier, reached from their branch)
+        if (!failed && __syncthreads_or(0)) failed = true;
+        if (!failed && (L & 1)) density(pp);  // the last, single row
+        if (failed) {
+            __syncthreads();  // pairs with the drift warps' barrier before their NaN fill
+            if (tid == PTID) {
+                if (a.status) atomicOr(a.status, VP_STATUS_WAIT_TIMEOUT);
+                // the loads in flight land before the block leaves
+                for (long long k = L; k < prod->issued; ++k)
+                    wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+            }
+        }
+    }
+}
+
 // cuTensorMapEncodeTiled from the driver, looked up once
 static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -815,6 +1080,27 @@ static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUte
     const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
     kern<<<(unsigned)grid, block, smem, st>>>(tin, thalo, tout, a);
     return check_launch("k_plane");
+}
+
+template <bool FULL, bool EQ>
+static int launch_xrd(const CUtensorMap& tin, const CUtensorMap& thalo, const Args& a, cudaStream_t st) {
+    auto kern = k_plane_xrd<FULL, EQ>;
+    constexpr size_t smem = xrd_smem_bytes();
+    static int raised[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(VP_ERR_CUDA, "run_plane: device index out of range");
+    if (!raised[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return set_cuda_error("cudaFuncSetAttribute(k_plane_xrd)");
+        raised[dev] = 1;
+    }
+    const int occ = occupancy(kern, XRD_THREADS, smem);
+    if (occ < 1) return set_error(VP_ERR_UNSUPPORTED, "run_plane: the density pass does not fit an SM");
+    const int64_t total = (int64_t)a.n_cg * a.nx;
+    const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
+    kern<<<(unsigned)grid, XRD_THREADS, smem, st>>>(tin, thalo, a);
+    return check_launch("k_plane_xrd");
 }
 
 template <bool RHO, bool FULL, int YM, bool EQ>
@@ -889,9 +1175,8 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
         const bool full2 = ny % YT2 == 0;
         auto go2 = [&](auto eqc) {
             constexpr bool E = decltype(eqc)::value != 0;
-            if (part)
-                return full2 ? launch_xr<true, true, YMAX, E>(tin, thalo, a, st)
-                             : launch_xr<true, false, YMAX, E>(tin, thalo, a, st);
+            if (part)  // the density on its own warpgroup
+                return full2 ? launch_xrd<true, E>(tin, thalo, a, st) : launch_xrd<false, E>(tin, thalo, a, st);
             return full2 ? launch_xr<false, true, YMAX, E>(tin, thalo, a, st)
                          : launch_xr<false, false, YMAX, E>(tin, thalo, a, st);
         };

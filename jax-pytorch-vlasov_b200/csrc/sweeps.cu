@@ -611,6 +611,10 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
     // and of A(vx), after all teams' row buffers
     C* dAt = reinterpret_cast<C*>(smem_raw) + (size_t)teams_per_block * KK * nvy + (size_t)tid_team * 2 * nvx;
     C* At = dAt + nvx;
+    // and the block's copy of the equilibrium factors (FP64), after the tables
+    const double* eqA = reinterpret_cast<const double*>(reinterpret_cast<C*>(smem_raw) +
+                                                        (size_t)teams_per_block * (KK * nvy + 2 * nvx));
+    const double* eqB = eqA + nvx;
 
     double vy2[VEC];
     if constexpr (DIAG) {
@@ -661,12 +665,12 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
             for (int e = 0; e < VEC; ++e) {
                 const int iv = li * VEC + e;
-                Be[e] = (lane_ok && iv < nvy) ? a.eqB[iv] : 0.0;
+                Be[e] = (lane_ok && iv < nvy) ? eqB[iv] : 0.0;
                 double k_b = 0.0;
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
                     const int j = iv - sy + 2 - k;
-                    if (lane_ok && j >= 0 && j < nvy) k_b = fma(wyd[k], a.eqB[j], k_b);
+                    if (lane_ok && j >= 0 && j < nvy) k_b = fma(wyd[k], eqB[j], k_b);
                 }
                 dBe[e] = k_b - Be[e];
                 Bc[e] = C(Be[e]);
@@ -678,9 +682,9 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
                 const int j = row - sx + 2 - k;
-                if (j >= 0 && j < nvx) k_a = fma(wxd[k], a.eqA[j], k_a);
+                if (j >= 0 && j < nvx) k_a = fma(wxd[k], eqA[j], k_a);
             }
-            return k_a - a.eqA[row];
+            return k_a - eqA[row];
         };
         // the split's factors: before the first loads when the moments need
         // them there, else after the first loads are in flight
@@ -690,7 +694,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
             // warp barrier that ends its last chunk
             for (int row = li; row < nvx; row += team) {
                 dAt[row] = pv ? C(dA_row(row)) : C(0);
-                At[row] = C(a.eqA[row]);
+                At[row] = C(eqA[row]);
             }
             __syncwarp();
         };
@@ -713,7 +717,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
                     for (int e = 0; e < VEC; ++e) {
                         double fv = (double)raw_get<TS, VEC>(v, e);
-                        if constexpr (EQ) fv += a.eqA[rr] * Be[e];
+                        if constexpr (EQ) fv += eqA[rr] * Be[e];
                         m_pre += fv * (vx2 + vy2[e]);
                     }
                 }
@@ -863,7 +867,7 @@ __device__ __forceinline__ void kick2d_item(const Kick2dArgs& a, const int64_t b
 #pragma unroll
                         for (int e = 0; e < VEC; ++e) {
                             double fv = (double)as_stored<TS>(rres.v[e]);
-                            if constexpr (EQ) fv += a.eqA[l + u] * Be[e];
+                            if constexpr (EQ) fv += eqA[l + u] * Be[e];
                             m_post += fv * (vx2 + vy2[e]);
                             m_l2 += fv * fv;
                             m_sum += fv;
@@ -894,6 +898,14 @@ template <typename TS, int VEC, bool DIAG, bool EQ>
 __global__ void __launch_bounds__(kBlock, 2) k_kick2d(const __grid_constant__ Kick2dArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int teams_per_block = blockDim.x / a.team;
+    if constexpr (EQ) {
+        // the equilibrium factors, read by every plane, once per block
+        double* eq = reinterpret_cast<double*>(reinterpret_cast<compute_t<TS>*>(smem_raw) +
+                                               (size_t)teams_per_block * (kick2d_rows<TS, VEC>() * a.nvy + 2 * a.nvx));
+        for (int i = threadIdx.x; i < a.nvx + a.nvy; i += blockDim.x)
+            eq[i] = i < a.nvx ? a.eqA[i] : a.eqB[i - a.nvx];
+        __syncthreads();
+    }
     const int64_t stride = (int64_t)gridDim.x * teams_per_block;
     for (int64_t base = (int64_t)blockIdx.x * teams_per_block; base < a.n_planes; base += stride)
         kick2d_item<TS, VEC, DIAG, EQ>(a, base, smem_raw);
@@ -923,7 +935,8 @@ template <typename TS, int VEC, bool DIAG, bool EQ>
 static int launch_kick2d_t(Kick2dArgs a, cudaStream_t st) {
     const int teams = kBlock / a.team;
     const size_t smem =
-        (size_t)teams * (kick2d_rows<TS, VEC>() * a.nvy + (EQ ? 2 * a.nvx : 0)) * sizeof(compute_t<TS>);
+        (size_t)teams * (kick2d_rows<TS, VEC>() * a.nvy + (EQ ? 2 * a.nvx : 0)) * sizeof(compute_t<TS>) +
+        (EQ ? (size_t)(a.nvx + a.nvy) * sizeof(double) : 0);
     auto kern = k_kick2d<TS, VEC, DIAG, EQ>;
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
