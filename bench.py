@@ -274,7 +274,8 @@ def run_reference(a):
         "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": short_dtype(a.dtype),
-        "data": "synthetic", "config": {"workload": a.desc + f", {a.dtype} storage", "sample_grid": list(grid)},
+        "data": "synthetic", "config": {"workload": a.desc + f", {a.dtype} storage", "grid": list(a.grid),
+                                        "cpu_sample_grid": list(grid)},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -432,8 +433,10 @@ def run_ours(a):
         phase_gbs = {p: (sweep_bytes / (ph[p] * 1e-3) / 1e9 if ph[p] > busy and p not in ("field", "diag") else None)
                      for p in PHASES}
         if planar:
-            # x then y (with the density partials and their finalize) and y
-            # then x each make one pass over f; their phases carry the x names
+            # x then y (with the density partials) and y then x each make one
+            # pass over f; their phases carry the x names. The y1 phase is the
+            # separate kernel that sums the density partials (no pass over f).
+            phase_gbs["drift_y1_rho"] = phase_gbs["drift_y2"] = None
             groups = {"plane_xy_rho": ph["drift_x1"], "kick_vx_vy": ph["kick_vx_vy"], "plane_yx": ph["drift_x2"]}
             dom = max(groups, key=groups.get)
             dom_ms = groups[dom]
@@ -447,6 +450,8 @@ def run_ours(a):
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": ncu_traffic(f"{dom}_{'x'.join(map(str, a.grid))}_{a.dtype}"),
                 "algorithmic_bytes_per_launch": sweep_bytes}
+        if planar:
+            roof["density_partials_sum_ms"] = ph["drift_y1_rho"]
     else:
         # graph-replayed small grids: whole-step bandwidth (the f-sized sweeps
         # dominate; the grid fits the L2, so this may exceed the HBM figure)
@@ -645,13 +650,16 @@ def run_batch_reference(a):
             sec += t
             used = u
     value = cells / sec
+    all_runs = importlib.import_module("jax-pytorch-vlasov_b200.workloads").batch_runs()
     sample = (f"oracle Strang step (C + OpenMP restatement of the reference's vlasov_step_gather_free) over the "
               f"first {used} runs of the batch per step, {a.steps} steps after {a.warmup} warm-up")
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": short_dtype(a.dtype),
-        "data": "synthetic", "config": {"workload": a.desc + f", {a.dtype} storage", "sample_runs": used},
+        "data": "synthetic", "config": {"workload": a.desc + f", {a.dtype} storage", "runs": len(all_runs),
+                                        "cells": sum(p["Nx"] * p["Ny"] * p["Nvx"] * p["Nvy"] for p in all_runs),
+                                        "cpu_sample_runs": used},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

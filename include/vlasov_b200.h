@@ -92,6 +92,28 @@ int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int6
                  size_t workspace_bytes, void* stream);
 size_t vp_drift_rho_workspace_bytes(int64_t n_outer, int64_t n_line, int64_t n_inner);
 
+/* Both position drifts of f[nx][ny][nvx][nvy] in one pass over f, the
+ * intermediate on chip: x then y (xfirst = 1) or y then x (xfirst = 0), each
+ * drift as vp_drift with its own table (shift_x/W_x indexed by vx, shift_y/
+ * W_y by vy; W in FP32). Replaces the pairs advect_x_static(axis 0) +
+ * advect_x_static(axis 1) of vlasov_step_gather_free_impl
+ * (vlasov2D2V.py:1063-1064 and :1079-1080); f is the same bits as the two
+ * sweeps give. Only the output rows x_begin .. x_begin + x_count - 1 are
+ * written (the input rows wrap around nx), so a caller can compute the rows
+ * that need fresh neighbour data apart from the others. With xfirst and rho
+ * != NULL the pass also forms the density of its rows,
+ *   rho[x*ny + y] = scale * sum_{vx,vy} out[x,y,vx,vy]   (FP64, deterministic),
+ * for x in the range; workspace: vp_drift_pair_workspace_bytes() bytes
+ * (the density partials; may be NULL without rho).
+ * Needs FP32, 16 <= ny <= 128, nvy a multiple of 32 and 16-byte aligned
+ * buffers; VP_ERR_UNSUPPORTED otherwise (the caller then runs two vp_drift
+ * sweeps). */
+int vp_drift_pair(const void* f_in, void* f_out, int dtype, int64_t nx, int64_t ny, int64_t nvx,
+                  int64_t nvy, int32_t xfirst, int64_t x_begin, int64_t x_count, const int32_t* shift_x,
+                  const void* W_x, const int32_t* shift_y, const void* W_y, double scale, double* rho,
+                  void* workspace, size_t workspace_bytes, void* stream);
+size_t vp_drift_pair_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy);
+
 /* Dirichlet kick along n_line with a field constant over each outer row
  * (the vx or vy kick). Replaces advect_v_static with build_v_tap_weights
  * (vlasov2D2V.py:822-913; vlasov1D1V.py:450-501): outer row o uses the field
@@ -217,8 +239,10 @@ size_t vp_poisson1d_workspace_bytes(int64_t nx);
  * events[2p] is recorded on the stream before phase p, events[2p+1] after
  * it (cudaEvent_t handles created by the caller; both at the same point
  * when a phase does not run). */
-#define VP_PHASE_DRIFT_X1 0  /* 1D1V: the first x drift fused with n */
-#define VP_PHASE_DRIFT_Y1 1  /* y drift fused with rho (2D2V only) */
+#define VP_PHASE_DRIFT_X1 0  /* 1D1V: the first x drift fused with n; 2D2V fused
+                                pair: the x-then-y pass with its density partials */
+#define VP_PHASE_DRIFT_Y1 1  /* y drift fused with rho (2D2V only); fused pair:
+                                the sum of the density partials */
 #define VP_PHASE_FIELD 2     /* Poisson solve */
 #define VP_PHASE_KICK 3      /* vx+vy kick (2D2V), v kick (1D1V) */
 #define VP_PHASE_DRIFT_Y2 4  /* 2D2V only */

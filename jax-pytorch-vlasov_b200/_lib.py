@@ -105,6 +105,9 @@ SIGNATURES = {
     "vp_drift": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I64, P, I32, P, P]),
     "vp_drift_rho": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I64, P, I32, P, D, P, P, SZ, P]),
     "vp_drift_rho_workspace_bytes": (SZ, [I64, I64, I64]),
+    "vp_drift_pair": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, I64, I32, I64, I64, P, P, P, P, D, P, P, SZ,
+                                     P]),
+    "vp_drift_pair_workspace_bytes": (SZ, [I64, I64, I64, I64]),
     "vp_kick": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, P, ctypes.c_int, I64, D, D, I32, P]),
     "vp_kick2d": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, P, P, D, D, D, I32, P, P, P, P]),
     "vp_advect_gather": (ctypes.c_int, [P, P, ctypes.c_int, I64, I64, I64, P, I64, I64, I64, D, D, ctypes.c_int, P]),

@@ -189,6 +189,38 @@ int vp_drift_rho(const void* f_in, void* f_out, int dtype, int64_t n_outer, int6
     return run_rho_finalize(part, n_outer, n_line, tiles, scale, 0.0, rho, S(stream));
 }
 
+size_t vp_drift_pair_workspace_bytes(int64_t nx, int64_t ny, int64_t nvx, int64_t nvy) {
+    if (nx <= 0 || ny <= 0 || nvx <= 0 || nvy <= 0) return 0;
+    return (size_t)nx * (size_t)plane_part_tiles(nvx, nvy) * (size_t)ny * sizeof(double);
+}
+
+int vp_drift_pair(const void* f_in, void* f_out, int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
+                  int32_t xfirst, int64_t x_begin, int64_t x_count, const int32_t* shift_x, const void* W_x,
+                  const int32_t* shift_y, const void* W_y, double scale, double* rho, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+    if (!dtype_ok(dtype)) return set_error(VP_ERR_DTYPE, "vp_drift_pair: unknown dtype");
+    VP_CHECK(f_in && f_out && shift_x && W_x && shift_y && W_y, "vp_drift_pair: null pointer");
+    VP_CHECK(f_in != f_out, "vp_drift_pair: f_out must not alias f_in");
+    VP_CHECK(nx > 0 && ny > 0 && nvx > 0 && nvy > 0, "vp_drift_pair: bad size");
+    VP_CHECK(x_begin >= 0 && x_count > 0 && x_begin + x_count <= nx, "vp_drift_pair: output rows outside [0, nx)");
+    VP_CHECK(!rho || xfirst, "vp_drift_pair: the density comes with the x-then-y order");
+    if (!plane_fits(dtype, nx, ny, nvx, nvy, f_in) || !plane_fits(dtype, nx, ny, nvx, nvy, f_out))
+        return set_error(VP_ERR_UNSUPPORTED,
+                         "vp_drift_pair: needs FP32, 16 <= ny <= 128, nvy % 32 == 0 and 16-byte aligned buffers");
+    double* part = nullptr;
+    if (rho) {
+        if (!workspace || workspace_bytes < vp_drift_pair_workspace_bytes(nx, ny, nvx, nvy))
+            return set_error(VP_ERR_WORKSPACE, "vp_drift_pair: workspace too small");
+        part = static_cast<double*>(workspace);
+    }
+    int tiles = 0;
+    int rc = run_plane(dtype, xfirst != 0, f_in, f_out, nx, ny, nvx, nvy, x_begin, x_count, shift_x, W_x, shift_y,
+                       W_y, part, &tiles, EQ_NONE, nullptr, 0, S(stream));
+    if (rc || !rho) return rc;
+    // the partials are [nx][tiles][ny]: the range's rows are contiguous
+    return run_rho_finalize(part + x_begin * tiles * ny, x_count, ny, tiles, scale, 0.0, rho + x_begin * ny, S(stream));
+}
+
 int vp_kick(const void* f_in, void* f_out, int dtype, int64_t n_outer, int64_t n_line, int64_t n_inner,
             const void* E, int e_dtype, int64_t e_div, double dt, double dv, int32_t window, void* stream) {
     if (!dtype_ok(dtype)) return set_error(VP_ERR_DTYPE, "vp_kick: unknown dtype");
@@ -372,12 +404,15 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         if ((rc = mk.begin(VP_PHASE_DRIFT_X1))) return rc;
         dst = dst_of(i++);
         int tiles = 0;
-        rc = run_plane(d->dtype, true, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y,
+        rc = run_plane(d->dtype, true, src, dst, nx, ny, nvx, nvy, 0, nx, d->shift_x, d->W_x, d->shift_y, d->W_y,
                        want_rho ? w.part : nullptr, &tiles, EQ, d->status, d->test_stall, st);
-        if (!rc && want_rho)
-            rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, eq_on ? d->eq_moment : 0.0, w.rho, st);
         if (rc || (rc = mk.end(VP_PHASE_DRIFT_X1))) return rc;
-        if ((rc = mk.begin(VP_PHASE_DRIFT_Y1)) || (rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
+        // the density partials' sum, timed as its own phase
+        if ((rc = mk.begin(VP_PHASE_DRIFT_Y1))) return rc;
+        if (want_rho &&
+            (rc = run_rho_finalize(w.part, nx, ny, tiles, d->dvx * d->dvy, eq_on ? d->eq_moment : 0.0, w.rho, st)))
+            return rc;
+        if ((rc = mk.end(VP_PHASE_DRIFT_Y1))) return rc;
         src = dst;
     } else {
     // x drift (dt/2)
@@ -448,8 +483,8 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
         if ((rc = mk.begin(VP_PHASE_DRIFT_Y2)) || (rc = mk.end(VP_PHASE_DRIFT_Y2))) return rc;
         if ((rc = mk.begin(VP_PHASE_DRIFT_X2))) return rc;
         dst = dst_of(i++);
-        rc = run_plane(d->dtype, false, src, dst, nx, ny, nvx, nvy, d->shift_x, d->W_x, d->shift_y, d->W_y, nullptr,
-                       nullptr, EQ, d->status, d->test_stall, st);
+        rc = run_plane(d->dtype, false, src, dst, nx, ny, nvx, nvy, 0, nx, d->shift_x, d->W_x, d->shift_y, d->W_y,
+                       nullptr, nullptr, EQ, d->status, d->test_stall, st);
         if (rc || (rc = mk.end(VP_PHASE_DRIFT_X2)) || (rc = mk.begin(VP_PHASE_DIAG))) return rc;
     } else {
     // y drift (dt/2)

@@ -155,9 +155,11 @@ int run_init_product(int dtype, const double* S, const double* V, void* f, int64
 // single-axis sweeps do.
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* in);
 int64_t plane_part_tiles(int64_t nvx, int64_t nvy);
+// Only the output rows x_begin .. x_begin + x_count - 1 are written (their
+// density partials too); the inputs wrap around nx.
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
-              const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
-              const EqSplit* eq, int* status, int stall, cudaStream_t st);
+              int64_t x_begin, int64_t x_count, const int* shift_x, const void* W_x, const int* shift_y,
+              const void* W_y, double* part, int* tiles, const EqSplit* eq, int* status, int stall, cudaStream_t st);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                     int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,

@@ -73,6 +73,7 @@ __host__ __device__ constexpr int stage_floats(int ym) { return ym * CG; }
 struct Args {
     float* out;
     int nx, ny, nvx, nvy;
+    int xb, xc;         // the output rows: xb .. xb + xc - 1 (all: 0, nx)
     int64_t m;          // columns per (x, y) point: nvx * nvy
     int n_cg;           // column groups: m / CG
     const int* shift_x;
@@ -87,8 +88,9 @@ struct Args {
 };
 
 // The rows a CTA loads. Work comes in segments (one group, output rows
-// xa .. xa+n-1), each loading the rows xa - s - 3 + q, q = 0 .. n + 4, of
-// its group (s: the group's x shift). CTA b of G first takes whole lines of
+// xa .. xa+n-1 of the launch's range xb .. xb+xc-1; a line is the whole
+// range), each loading the rows xa - s - 3 + q, q = 0 .. n + 4, of its group
+// (s: the group's x shift; rows wrap around nx). CTA b of G first takes whole lines of
 // the groups b, b + G, b + 2G, ... (neighbouring groups then stream the same
 // x rows at the same time, so HBM sees long runs of each (x, y) point's
 // columns), then an even share of the rows of the n_cg % G groups left.
@@ -101,7 +103,7 @@ struct Seq {
         G = G_;
         full = a.n_cg / G;
         w = 0;
-        const int64_t rest = (int64_t)(a.n_cg - full * G) * a.nx;
+        const int64_t rest = (int64_t)(a.n_cg - full * G) * a.xc;
         t = rest * b / G;
         t1 = rest * (b + 1) / G;
         if (valid()) start(a);
@@ -109,13 +111,14 @@ struct Seq {
     __device__ __forceinline__ void start(const Args& a) {
         if (w < full) {
             cg = w * G + b;
-            xa = 0;
-            n = a.nx;
+            xa = a.xb;
+            n = a.xc;
         } else {
-            cg = full * G + (int)(t / a.nx);
-            xa = (int)(t % a.nx);
+            cg = full * G + (int)(t / a.xc);
+            const int o = (int)(t % a.xc);
+            xa = a.xb + o;
             const int64_t left = t1 - t;
-            n = (int)(left < (int64_t)(a.nx - xa) ? left : (int64_t)(a.nx - xa));
+            n = (int)(left < (int64_t)(a.xc - o) ? left : (int64_t)(a.xc - o));
         }
         const int jx = (int)(((int64_t)cg * CG / a.nvy) % a.nvx);
         r0 = xa - __ldg(a.shift_x + jx) - 3;
@@ -1076,7 +1079,7 @@ static int launch_t(const CUtensorMap& tin, const CUtensorMap& thalo, const CUte
         raised[dev] = 1;
     }
     const int occ = occupancy(kern, block, smem);
-    const int64_t total = (int64_t)a.n_cg * a.nx;
+    const int64_t total = (int64_t)a.n_cg * a.xc;
     const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
     kern<<<(unsigned)grid, block, smem, st>>>(tin, thalo, tout, a);
     return check_launch("k_plane");
@@ -1097,7 +1100,7 @@ static int launch_xrd(const CUtensorMap& tin, const CUtensorMap& thalo, const Ar
     }
     const int occ = occupancy(kern, XRD_THREADS, smem);
     if (occ < 1) return set_error(VP_ERR_UNSUPPORTED, "run_plane: the density pass does not fit an SM");
-    const int64_t total = (int64_t)a.n_cg * a.nx;
+    const int64_t total = (int64_t)a.n_cg * a.xc;
     const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
     kern<<<(unsigned)grid, XRD_THREADS, smem, st>>>(tin, thalo, a);
     return check_launch("k_plane_xrd");
@@ -1119,7 +1122,7 @@ static int launch_xr(const CUtensorMap& tin, const CUtensorMap& thalo, const Arg
         raised[dev] = 1;
     }
     const int occ = occupancy(kern, block, smem);
-    const int64_t total = (int64_t)a.n_cg * a.nx;
+    const int64_t total = (int64_t)a.n_cg * a.xc;
     const int64_t grid = std::min<int64_t>(total, (int64_t)sm_count() * occ);
     kern<<<(unsigned)grid, block, smem, st>>>(tin, thalo, a);
     return check_launch("k_plane_xr");
@@ -1139,14 +1142,18 @@ bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, con
 int64_t plane_part_tiles(int64_t nvx, int64_t nvy) { return nvx * nvy / plane::CG; }
 
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
-              const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part, int* tiles,
-              const EqSplit* eq, int* status, int stall, cudaStream_t st) {
+              int64_t x_begin, int64_t x_count, const int* shift_x, const void* W_x, const int* shift_y,
+              const void* W_y, double* part, int* tiles, const EqSplit* eq, int* status, int stall, cudaStream_t st) {
     using namespace plane;
     if (!plane_fits(dtype, nx, ny, nvx, nvy, in) || !plane_fits(dtype, nx, ny, nvx, nvy, out))
         return set_error(VP_ERR_UNSUPPORTED, "run_plane: layout not fused");
+    if (x_begin < 0 || x_count < 1 || x_begin + x_count > nx)
+        return set_error(VP_ERR_ARG, "run_plane: output rows outside [0, nx)");
     Args a{};
     a.out = static_cast<float*>(out);
     a.nx = (int)nx;
+    a.xb = (int)x_begin;
+    a.xc = (int)x_count;
     a.ny = (int)ny;
     a.nvx = (int)nvx;
     a.nvy = (int)nvy;

@@ -496,33 +496,40 @@ int run_strided(int dtype, const void* in, void* out, int64_t n_outer, int64_t n
 // 32 columns): block (32 lines, 8 slices); slice s adds the tiles
 // t = s (mod 8) with four running sums (t = s, s+8, s+16, s+24 mod 32),
 // then the 8 slices are added in order. Fixed order, so deterministic.
-__global__ void __launch_bounds__(256) k_rho_finalize_wide(const double* __restrict__ part, int n_line, int tiles,
-                                                           double scale, double offset, double* __restrict__ rho) {
-    __shared__ double sl[8][33];
+// The density from many tiles' partials [n_outer][tiles][n_line]: 32 points
+// of a line per block, 16 slices of the tiles per point (slice s adds tiles
+// s, s + 16, ... into 8 accumulators in turn, so that 8 loads are in flight
+// per thread), then the accumulators and the slices in a fixed order.
+constexpr int kFinSlices = 16;
+__global__ void __launch_bounds__(32 * kFinSlices) k_rho_finalize_wide(const double* __restrict__ part, int n_line,
+                                                                      int tiles, double scale, double offset,
+                                                                      double* __restrict__ rho) {
+    __shared__ double sl[kFinSlices][33];
     const int l = blockIdx.x * 32 + threadIdx.x;
     const int64_t o = blockIdx.y;
     const int sidx = threadIdx.y;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (l < n_line) {
         const double* p = part + (o * tiles) * (int64_t)n_line + l;
         int t = sidx;
-        for (; t + 24 < tiles; t += 32) {
-            a0 += p[(int64_t)t * n_line];
-            a1 += p[(int64_t)(t + 8) * n_line];
-            a2 += p[(int64_t)(t + 16) * n_line];
-            a3 += p[(int64_t)(t + 24) * n_line];
+        for (; t + 7 * kFinSlices < tiles; t += 8 * kFinSlices) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = __ldcs(p + (int64_t)(t + k * kFinSlices) * n_line);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] += v[k];
         }
-        if (t < tiles) a0 += p[(int64_t)t * n_line];
-        if (t + 8 < tiles) a1 += p[(int64_t)(t + 8) * n_line];
-        if (t + 16 < tiles) a2 += p[(int64_t)(t + 16) * n_line];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (t + k * kFinSlices < tiles) acc[k] += __ldcs(p + (int64_t)(t + k * kFinSlices) * n_line);
     }
-    sl[sidx][threadIdx.x] = (a0 + a1) + (a2 + a3);
+    sl[sidx][threadIdx.x] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     __syncthreads();
     if (sidx == 0 && l < n_line) {
-        double acc = sl[0][threadIdx.x];
+        double a = sl[0][threadIdx.x];
 #pragma unroll
-        for (int k = 1; k < 8; ++k) acc += sl[k][threadIdx.x];
-        rho[o * n_line + l] = acc * scale + offset;
+        for (int k = 1; k < kFinSlices; ++k) a += sl[k][threadIdx.x];
+        rho[o * n_line + l] = a * scale + offset;
     }
 }
 
@@ -531,7 +538,7 @@ int run_rho_finalize(const double* part, int64_t n_outer, int64_t n_line, int ti
                      cudaStream_t st) {
     if (tiles > 32 && n_outer <= 65535) {
         const dim3 grid((unsigned)((n_line + 31) / 32), (unsigned)n_outer);
-        k_rho_finalize_wide<<<grid, dim3(32, 8), 0, st>>>(part, (int)n_line, tiles, scale, offset, rho);
+        k_rho_finalize_wide<<<grid, dim3(32, kFinSlices), 0, st>>>(part, (int)n_line, tiles, scale, offset, rho);
         return check_launch("k_rho_finalize_wide");
     }
     const int64_t total = n_outer * n_line;

@@ -136,6 +136,32 @@ def drift_rho(f: torch.Tensor, table: DriftTable, axis: int, vel_axis: int, scal
     return out, rho
 
 
+def drift_pair(f: torch.Tensor, tx: DriftTable, ty: DriftTable, xfirst: bool, out: torch.Tensor | None = None,
+               rows: tuple[int, int] | None = None, scale: float | None = None, rho: torch.Tensor | None = None):
+    """Both position drifts of f[Nx][Ny][Nvx][Nvy] in one pass (x then y or
+    y then x; vp_drift_pair). rows = (first, count) restricts the output rows
+    (default all); with xfirst and `scale` the density of those rows goes into
+    rho[Nx, Ny] (float64, allocated if None). Returns (out, rho or None).
+    Raises VlasovError (VP_ERR_UNSUPPORTED) when the layout does not fit."""
+    L.require_cuda(f)
+    out = torch.empty_like(f) if out is None else out
+    Nx, Ny, Nvx, Nvy = f.shape
+    x0, nrows = rows if rows is not None else (0, Nx)
+    ws = None
+    if scale is not None:
+        if not xfirst:
+            raise ValueError("the density comes with the x-then-y order")
+        if rho is None:
+            rho = torch.empty((Nx, Ny), dtype=torch.float64, device=f.device)
+        nb = L.query("vp_drift_pair_workspace_bytes", Nx, Ny, Nvx, Nvy)
+        ws = workspace(f.device, nb, "drift_pair")
+    L.call("vp_drift_pair", L.ptr(f), L.ptr(out), L.dtype_code(f.dtype), Nx, Ny, Nvx, Nvy, 1 if xfirst else 0,
+           int(x0), int(nrows), L.ptr(tx.shift), L.ptr(tx.W), L.ptr(ty.shift), L.ptr(ty.W),
+           float(scale) if scale is not None else 1.0, L.ptr(rho) if scale is not None else None,
+           L.ptr(ws), ws.numel() if ws is not None else 0, L.stream_of(f))
+    return out, (rho if scale is not None else None)
+
+
 def kick(f: torch.Tensor, E: torch.Tensor, dt: float, dv: float, axis: int, window: int = -1,
          out: torch.Tensor | None = None):
     """Dirichlet kick along `axis` with a field E over the leading dims

@@ -20,6 +20,13 @@ the slabs' rho are all-gathered (Nx*Ny float64, 128 KiB at 128^2) and every
 rank solves the small Poisson problem for the whole domain, so the kick of
 every local row (halo rows included) uses the global field.
 
+Where the layout allows (FP32, 16 <= Ny <= 128, Nvy a multiple of 32) each
+pair of position drifts runs as one fused pass over the extended buffer
+(vp_drift_pair), as the one-GPU step does. The halo exchange then overlaps the
+first pass: the rows whose x windows stay inside the rank's own rows are
+computed while the halo rows are in flight, the rows next to the halo after
+they have arrived.
+
 `SlabPlan` is pure host logic; `exchange_halos` / `gather_rho` take a
 torch.distributed process group (NCCL for CUDA tensors, gloo for CPU ones);
 `SlabStepper2D` runs the two halves of a step around the field solve on the
@@ -95,10 +102,13 @@ def _slab(f_ext: torch.Tensor, plan: SlabPlan, r: int) -> torch.Tensor:
     return f_ext[plan.hl:plan.hl + plan.local(r)]
 
 
-def exchange_halos(f_ext: torch.Tensor, plan: SlabPlan, rank: int, group=None) -> None:
-    """Fill the halo rows of this rank's extended buffer from its ring
+def start_halo_exchange(f_ext: torch.Tensor, plan: SlabPlan, rank: int, group=None) -> list:
+    """Start filling the halo rows of this rank's extended buffer from its ring
     neighbours' slab rows (point-to-point over the process group; a single
-    rank copies its own rows)."""
+    rank copies its own rows at once). Returns the requests to wait on; until
+    then the halo rows must not be read nor the slab rows written. With NCCL
+    the transfers run on the library's own stream, so kernels launched on the
+    current stream meanwhile overlap them."""
     slab = _slab(f_ext, plan, rank)
     if plan.ranks == 1:
         # the halo may be wider than the line itself: gather by global row
@@ -106,7 +116,7 @@ def exchange_halos(f_ext: torch.Tensor, plan: SlabPlan, rank: int, group=None) -
         halo = torch.cat([torch.arange(0, plan.hl), torch.arange(plan.hl + n, ext)]).to(f_ext.device)
         rows = torch.as_tensor(plan.global_rows(0), device=f_ext.device)
         f_ext[halo] = slab[rows[halo]]
-        return
+        return []
     left, right = (rank - 1) % plan.ranks, (rank + 1) % plan.ranks
     ops_ = []
     # my last hl rows are the right neighbour's "before" halo, my first hr
@@ -117,8 +127,19 @@ def exchange_halos(f_ext: torch.Tensor, plan: SlabPlan, rank: int, group=None) -
     if plan.hr:
         ops_.append(dist.P2POp(dist.isend, slab[:plan.hr].contiguous(), left, group))
         ops_.append(dist.P2POp(dist.irecv, f_ext[plan.hl + plan.local(rank):], right, group))
-    for req in dist.batch_isend_irecv(ops_):
+    return list(dist.batch_isend_irecv(ops_))
+
+
+def finish_halo_exchange(reqs: list) -> None:
+    """Wait for the requests of start_halo_exchange (with NCCL: the current
+    stream waits for the transfers)."""
+    for req in reqs:
         req.wait()
+
+
+def exchange_halos(f_ext: torch.Tensor, plan: SlabPlan, rank: int, group=None) -> None:
+    """Fill the halo rows of this rank's extended buffer (start and wait)."""
+    finish_halo_exchange(start_halo_exchange(f_ext, plan, rank, group))
 
 
 def gather_rho(rho_slab: torch.Tensor, plan: SlabPlan, group=None) -> torch.Tensor:
@@ -134,13 +155,14 @@ def gather_rho(rho_slab: torch.Tensor, plan: SlabPlan, group=None) -> torch.Tens
 
 
 class SlabStepper2D:
-    """One rank's share of a 2D2V Strang step (the one-sweep-per-axis
-    schedule of vp_step2d: x, y + rho, field, fused kick, y, x), on the
-    extended buffer of `SlabPlan`. The same arguments as engine.Stepper2D,
-    for the whole domain."""
+    """One rank's share of a 2D2V Strang step (the schedule of vp_step2d: x,
+    y + rho, field, fused kick, y, x; each drift pair as one fused pass where
+    the layout allows, else one sweep per axis), on the extended buffer of
+    `SlabPlan`. The same arguments as engine.Stepper2D, for the whole domain;
+    fuse_drifts=False keeps one sweep per axis."""
 
     def __init__(self, plan: SlabPlan, rank: int, Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt,
-                 dtype=torch.float32, device="cuda", window=-1):
+                 dtype=torch.float32, device="cuda", window=-1, fuse_drifts=True):
         if Nx != plan.nx:
             raise ValueError("the plan is for another Nx")
         self.plan, self.rank = plan, rank
@@ -156,6 +178,12 @@ class SlabStepper2D:
         self.ty = ops.DriftTable.from_velocity(vy, self.dt / 2.0, self.dy, dtype, self.device)
         self.kx, self.ky, self.inv_ksq = ops.spectral_2d(Nx, Ny, float(Lx), float(Ly), self.device)
         self.rows = torch.as_tensor(plan.global_rows(rank), device=self.device)
+        # the fused drift pairs (vp_drift_pair's layout conditions)
+        self.fused = bool(fuse_drifts) and dtype == torch.float32 and 16 <= Ny <= 128 and Nvy % 32 == 0
+        # first-pass rows whose x windows stay inside the rank's own rows
+        lo, hi = drift_reach(self.tx.shift.cpu().numpy())
+        a, b = plan.hl + lo, plan.hl + plan.local(rank) - hi
+        self.interior = (a, b - a) if b > a else None
 
     @staticmethod
     def plan_for(Nx, ranks, Lx, Vx_max, Nvx, dt, dtype=torch.float32) -> SlabPlan:
@@ -171,8 +199,29 @@ class SlabStepper2D:
     def first_half(self, f_ext: torch.Tensor):
         """x and y drifts of the extended buffer (its halo filled): the
         drifted buffer and this rank's rho rows."""
+        if self.fused:
+            b, rho = ops.drift_pair(f_ext, self.tx, self.ty, True, scale=self.dvx * self.dvy)
+            return b, _slab(rho, self.plan, self.rank)
         a = ops.drift(f_ext, self.tx, 0, 2)
         b, rho = ops.drift_rho(a, self.ty, 1, 3, self.dvx * self.dvy)
+        return b, _slab(rho, self.plan, self.rank)
+
+    def first_half_overlapped(self, f_ext: torch.Tensor, reqs: list):
+        """first_half while the halo exchange `reqs` is in flight: the interior
+        rows first, then (after the exchange) the rows next to the halo. The
+        same results as first_half after the exchange."""
+        if not self.fused or self.interior is None:
+            finish_halo_exchange(reqs)
+            return self.first_half(f_ext)
+        ext = self.shape[0]
+        i0, n = self.interior
+        scale = self.dvx * self.dvy
+        b, rho = ops.drift_pair(f_ext, self.tx, self.ty, True, rows=(i0, n), scale=scale)
+        finish_halo_exchange(reqs)
+        if i0 > 0:
+            ops.drift_pair(f_ext, self.tx, self.ty, True, out=b, rows=(0, i0), scale=scale, rho=rho)
+        if i0 + n < ext:
+            ops.drift_pair(f_ext, self.tx, self.ty, True, out=b, rows=(i0 + n, ext - i0 - n), scale=scale, rho=rho)
         return b, _slab(rho, self.plan, self.rank)
 
     def field(self, rho_global: torch.Tensor):
@@ -182,15 +231,18 @@ class SlabStepper2D:
     def second_half(self, b: torch.Tensor, Ex: torch.Tensor, Ey: torch.Tensor, out: torch.Tensor | None = None):
         """Kicks with the global field on every local row, then y and x."""
         c = ops.kick2d(b, Ex[self.rows], Ey[self.rows], self.dt, self.dvx, self.dvy, self.window)
+        if self.fused:
+            return ops.drift_pair(c, self.tx, self.ty, False, out=out)[0]
         d = ops.drift(c, self.ty, 1, 3)
         return ops.drift(d, self.tx, 0, 2, out=out)
 
     def step(self, f_ext: torch.Tensor, group=None, out: torch.Tensor | None = None):
-        """One step over the process group: halo exchange, first half, rho
+        """One step over the process group: halo exchange (overlapped with the
+        interior of the first pass where the drifts are fused), first half, rho
         all-gather, field, second half. Returns (f_ext', drho, phi)."""
         L.require_cuda(f_ext)
-        exchange_halos(f_ext, self.plan, self.rank, group)
-        b, rho = self.first_half(f_ext)
+        reqs = start_halo_exchange(f_ext, self.plan, self.rank, group)
+        b, rho = self.first_half_overlapped(f_ext, reqs)
         Ex, Ey, drho, phi = self.field(gather_rho(rho, self.plan, group))
         return self.second_half(b, Ex, Ey, out), drho, phi
 
@@ -215,4 +267,5 @@ def slab_rows(f_ext: torch.Tensor, plan: SlabPlan, r: int) -> torch.Tensor:
     return _slab(f_ext, plan, r)
 
 
-__all__ = ["SlabPlan", "SlabStepper2D", "drift_reach", "exchange_halos", "gather_rho", "scatter", "slab_rows"]
+__all__ = ["SlabPlan", "SlabStepper2D", "drift_reach", "exchange_halos", "finish_halo_exchange", "gather_rho",
+           "scatter", "slab_rows", "start_halo_exchange"]
