@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweeps-only", action="store_true",
-                    help="2D2V: one sweep per axis even where the fused (x, y) plane passes apply")
+                    help="2D2V and the batch: one sweep per axis even where the fused (x, y) plane passes apply")
     ap.add_argument("--split", action="store_true",
                     help="2D2V: store the perturbation of the initial condition's velocity equilibrium "
                          "(g = f - A(vx) B(vy)) with float64-evaluated drift tables")
@@ -684,7 +684,7 @@ def run_batch(a):
     runs = wl.batch_runs()
     diag = 1 if a.diagnostics else 0
     st = vp.BatchStepper2D(runs, dtype=dtype, device=dev, window=1, diagnostics=diag, graph_slots=10,
-                           tiles=None if a.tiles == "default" else "auto")
+                           tiles=None if a.tiles == "default" else "auto", fuse_drifts=not a.sweeps_only)
     if a.tiles == "tune":  # on a scratch state, before the initial condition is set
         at = importlib.import_module("jax-pytorch-vlasov_b200.autotune")
         for r, p in enumerate(runs):
@@ -834,7 +834,9 @@ def run_batch(a):
                        "l2_flush": "not needed: the batch state (all runs) exceeds the L2 several times",
                        "diagnostics_level": diag, "graph": "10 steps per CUDA graph, replayed",
                        "tiles": {k: v for k, v in (st.tiles or {}).items() if k != "run_segments"},
-                       "tiles_source": a.tiles},
+                       "tiles_source": a.tiles,
+                       "fused_runs": int(sum(st.fused)), "fused_cells": int(sum(
+                           math.prod(sh) for sh, fu in zip(st.shapes, st.fused) if fu))},
             "roofline": roof,
             "step_gbs": 5 * sweep_bytes / (ms_step * 1e-3) / 1e9,
             "gpu_launches": int(per_step_launches * K),

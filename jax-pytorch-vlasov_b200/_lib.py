@@ -94,7 +94,8 @@ BATCH_KINDS = 3
 
 
 class BatchTiles(ctypes.Structure):
-    _fields_ = [("block", I32 * BATCH_KINDS), ("ctas_per_sm", I32 * BATCH_KINDS), ("segments", I32 * BATCH_KINDS)]
+    _fields_ = [("block", I32 * BATCH_KINDS), ("ctas_per_sm", I32 * BATCH_KINDS), ("segments", I32 * BATCH_KINDS),
+                ("sweeps_only", I32)]
 
 
 # name -> (restype, argtypes)

@@ -5,11 +5,14 @@
 // plain argument blocks (the same blocks the single-run kernels take) plus
 // per-sweep item offsets; the caller copies the table to the device once.
 // vp_batch2d_step then only launches kernels whose arguments point into the
-// device copy, so a sequence of steps is capturable in a CUDA graph and
-// costs 9 launches per step whatever the number of runs:
-//   x drift (f -> s1), y drift + rho partials (s1 -> s2), rho finalize,
-//   3 Poisson kernels, fused kick (s2 -> s1), y drift (s1 -> s2),
-//   x drift (s2 -> f), diagnostics.
+// device copy, so a sequence of steps is capturable in a CUDA graph. The runs
+// whose layout the fused drift pairs take (FP32, 48 < ny <= 64, nvy a
+// multiple of 32) make three passes over f: x then y with the rho partials
+// (f -> s2), the fused kick (s2 -> s1), y then x (s1 -> f); the others one
+// sweep per axis: x (f -> s1), y + rho partials (s1 -> s2), kick (s2 -> s1),
+// y (s1 -> s2), x (s2 -> f). Each kind of pass is one launch for all runs
+// that take it, plus the rho finalize, 3 Poisson kernels and the
+// diagnostics: at most 12 launches per step whatever the number of runs.
 // Every run's arithmetic is that of vp_step2d (same item bodies, same
 // weights, same reduction order for the default tile shapes).
 #include <algorithm>
@@ -43,14 +46,19 @@ struct BatchHeader {
     int64_t off_pois;  // Pois2dRun[n]
     int64_t off_rfin;  // RhoFinRun[n]
     int64_t off_diag;  // DiagArgs[n]
+    int64_t off_p1, off_p2;  // plane-pass records (x then y, y then x), 64-byte aligned
+    int64_t off_sp;          // int64[n+1]: prefix sums of the plane items
+    int64_t plane_items;     // all runs' plane items (0: no fused runs)
+    int64_t sweep_items;     // all runs' x-drift items (0: every run fused)
     int64_t total_bytes;
 };
 
 size_t al16(size_t b) { return (b + 15) & ~size_t(15); }
+size_t al64(size_t b) { return (b + 63) & ~size_t(63); }
 
 struct Layout {
     int64_t off_x1, off_y1, off_y2, off_x2, off_sx, off_sy1, off_sy2, off_sk, off_kick, off_pois, off_rfin, off_diag,
-        total;
+        off_p1, off_p2, off_sp, total;
 };
 
 Layout layout_for(int n) {
@@ -73,6 +81,12 @@ Layout layout_for(int n) {
     L.off_pois = take(sizeof(Pois2dRun) * n);
     L.off_rfin = take(sizeof(RhoFinRun) * n);
     L.off_diag = take(sizeof(DiagArgs) * n);
+    L.off_sp = take(sizeof(int64_t) * (n + 1));
+    off = al64(off);  // tensor maps inside the plane records need 64-byte alignment
+    L.off_p1 = (int64_t)off;
+    off += al64(plane_run_bytes() * n);
+    L.off_p2 = (int64_t)off;
+    off += al64(plane_run_bytes() * n);
     L.total = (int64_t)off;
     return L;
 }
@@ -145,6 +159,10 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     DiagArgs* dg = at<DiagArgs>(table, L.off_diag);
     int vx_min = 4, ntx_min = 7, vy_min = 4, nty_min = 7, vk_min = 4;
     bool wrap_x = false, wrap_y = false;  // some run sweeps whole lines of a multiple of 8 rows
+    const bool sweeps_only = tiles && tiles->sweeps_only;
+    int64_t* sp = at<int64_t>(table, L.off_sp);
+    std::vector<char> fused(n_runs, 0);
+    sp[0] = 0;
     for (int r = 0; r < n_runs; ++r) {
         const vp_batch2d_run& d = runs[r];
         if (d.nx <= 0 || d.ny <= 0 || d.nvx <= 1 || d.nvy <= 1)
@@ -169,27 +187,49 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         Step2dWs w;
         step2d_layout(d.nx, d.ny, d.nvx, d.nvy, static_cast<char*>(d.workspace), &w);
         const int64_t nx = d.nx, ny = d.ny, nvx = d.nvx, nvy = d.nvy;
+        const bool want_rho = phys || diagnostics;
+        // the fused drift pairs: f -> s2 (x then y, the rho partials), then
+        // s1 -> f (after the kick) or s2 -> f (without it)
+        fused[r] = !sweeps_only && plane_batch_fits(dtype, nx, ny, nvx, nvy, d.f, d.s1, d.s2);
+        int64_t items = 0;
+        if (fused[r]) {
+            int rc = plane_batch_run(static_cast<char*>(table) + L.off_p1 + r * plane_run_bytes(), d.f, d.s2, nx, ny,
+                                     nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, want_rho ? w.part : nullptr,
+                                     &items);
+            if (!rc)
+                rc = plane_batch_run(static_cast<char*>(table) + L.off_p2 + r * plane_run_bytes(), phys ? d.s1 : d.s2,
+                                     d.f, nx, ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, nullptr, &items);
+            if (rc) return rc;
+        }
+        sp[r + 1] = sp[r] + items;
         int v, nt;
         // x drifts: f -> s1 and s2 -> f (with the kicks) or s1 -> f (without)
         strided_batch_args(dtype, d.f, d.s1, 1, nx, ny * nvx * nvy, nvy, nvx, d.shift_spread_x, d.shift_x, d.W_x,
                            nullptr, block[0], &x1[r], &v, &nt);
-        vx_min = std::min(vx_min, v);
-        ntx_min = std::min(ntx_min, nt);
+        if (!fused[r]) {
+            vx_min = std::min(vx_min, v);
+            ntx_min = std::min(ntx_min, nt);
+        }
         void* last_src = phys ? d.s2 : d.s1;
         strided_batch_args(dtype, last_src, d.f, 1, nx, ny * nvx * nvy, nvy, nvx, d.shift_spread_x, d.shift_x,
                            d.W_x, nullptr, block[0], &x2[r], &v, &nt);
-        vx_min = std::min(vx_min, v);
-        ntx_min = std::min(ntx_min, nt);
+        if (!fused[r]) {
+            vx_min = std::min(vx_min, v);
+            ntx_min = std::min(ntx_min, nt);
+        }
         // y drifts: s1 -> s2 (+rho), then s1 -> s2 (kicks) or s2 -> s1 (no kicks)
-        const bool want_rho = phys || diagnostics;
         strided_batch_args(dtype, d.s1, d.s2, nx, ny, nvx * nvy, 1, nvy, d.shift_spread_y, d.shift_y, d.W_y,
                            want_rho ? w.part : nullptr, block[1], &y1[r], &v, &nt);
-        vy_min = std::min(vy_min, v);
-        nty_min = std::min(nty_min, nt);
+        if (!fused[r]) {
+            vy_min = std::min(vy_min, v);
+            nty_min = std::min(nty_min, nt);
+        }
         strided_batch_args(dtype, phys ? d.s1 : d.s2, phys ? d.s2 : d.s1, nx, ny, nvx * nvy, 1, nvy,
                            d.shift_spread_y, d.shift_y, d.W_y, nullptr, block[1], &y2[r], &v, &nt);
-        vy_min = std::min(vy_min, v);
-        nty_min = std::min(nty_min, nt);
+        if (!fused[r]) {
+            vy_min = std::min(vy_min, v);
+            nty_min = std::min(nty_min, nt);
+        }
         if (phys) {
             kick2d_batch_args(dtype, d.s2, d.s1, nx * ny, nvx, nvy, w.ex, w.ey, d.dt, d.dvx, d.dvy, d.window, &kk[r],
                               &v);
@@ -260,6 +300,11 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
             a->items *= a->nseg;
         }
         rf[r].tiles = y1[r].tiles;
+        if (fused[r]) {
+            // no sweeps for this run; its density partials are per group
+            for (StridedArgs* a : {&x1[r], &x2[r], &y1[r], &y2[r]}) a->items = 0;
+            rf[r].tiles = (int)plane_part_tiles(runs[r].nvx, runs[r].nvy);
+        }
         sx[r + 1] = sx[r] + x1[r].items;
         sy1[r + 1] = sy1[r] + y1[r].items;
         sy2[r + 1] = sy2[r] + y2[r].items;
@@ -278,6 +323,11 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     h.grid[1] = grid_for(per_sm[1], std::max(sy1[n_runs], sy2[n_runs]));
     h.grid[2] = grid_for(per_sm[2], std::max<int64_t>(sk[n_runs], 1));
     h.kick_smem = kick_smem;
+    h.plane_items = sp[n_runs];
+    h.sweep_items = sx[n_runs];
+    h.off_p1 = L.off_p1;
+    h.off_p2 = L.off_p2;
+    h.off_sp = L.off_sp;
     h.off_x1 = L.off_x1;
     h.off_y1 = L.off_y1;
     h.off_y2 = L.off_y2;
@@ -314,18 +364,27 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
             return set_cuda_error("cudaEventRecord(timing event)");
         return VP_OK;
     };
-    // x drift (dt/2): f -> s1
-    if ((rc = mark(2 * VP_PHASE_DRIFT_X1))) return rc;
-    rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x1), sx, n,
-                              h.block[0], h.grid[0], 0, st);
-    if (rc || (rc = mark(2 * VP_PHASE_DRIFT_X1 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_Y1))) return rc;
-    // y drift (dt/2) fused with the rho partials: s1 -> s2
     const bool want_rho = h.phys || h.diag;
-    rc = launch_strided_batch(h.dtype, h.vec_y, h.nt_y, want_rho, h.wrap_y && !want_rho,
-                              at<StridedArgs>(table_dev, h.off_y1), sy1, n, h.block[1], h.grid[1], h.max_ny, st);
-    if (rc) return rc;
+    const bool sweeps = h.sweep_items > 0;
+    const int64_t* sp = at<int64_t>(table_dev, h.off_sp);
+    // the fused runs: x then y (dt/2 each) with the rho partials, f -> s2;
+    // the others: x drift (dt/2), f -> s1
+    if ((rc = mark(2 * VP_PHASE_DRIFT_X1))) return rc;
+    if ((rc = launch_plane_batch(true, want_rho, at<char>(table_dev, h.off_p1), sp, n, h.plane_items, st))) return rc;
+    if (sweeps) {
+        rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x1), sx,
+                                  n, h.block[0], h.grid[0], 0, st);
+        if (rc) return rc;
+    }
+    if ((rc = mark(2 * VP_PHASE_DRIFT_X1 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_Y1))) return rc;
+    // y drift (dt/2) fused with the rho partials: s1 -> s2
+    if (sweeps) {
+        rc = launch_strided_batch(h.dtype, h.vec_y, h.nt_y, want_rho, h.wrap_y && !want_rho,
+                                  at<StridedArgs>(table_dev, h.off_y1), sy1, n, h.block[1], h.grid[1], h.max_ny, st);
+        if (rc) return rc;
+    }
     if (h.phys) {
-        if ((rc = launch_rho_finalize_batch(at<RhoFinRun>(table_dev, h.off_rfin), n, h.max_points, st))) return rc;
+        if ((rc = launch_rho_finalize_batch(at<RhoFinRun>(table_dev, h.off_rfin), n, h.max_nx, h.max_ny, st))) return rc;
     }
     if ((rc = mark(2 * VP_PHASE_DRIFT_Y1 + 1)) || (rc = mark(2 * VP_PHASE_FIELD))) return rc;
     if (h.phys) {
@@ -341,13 +400,20 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     }
     if ((rc = mark(2 * VP_PHASE_KICK + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_Y2))) return rc;
     // y drift (dt/2)
-    rc = launch_strided_batch(h.dtype, h.vec_y, h.nt_y, false, h.wrap_y, at<StridedArgs>(table_dev, h.off_y2), sy2, n,
-                              h.block[1], h.grid[1], 0, st);
-    if (rc || (rc = mark(2 * VP_PHASE_DRIFT_Y2 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_X2))) return rc;
-    // x drift (dt/2) back into f
-    rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x2), sx, n,
-                              h.block[0], h.grid[0], 0, st);
-    if (rc || (rc = mark(2 * VP_PHASE_DRIFT_X2 + 1)) || (rc = mark(2 * VP_PHASE_DIAG))) return rc;
+    if (sweeps) {
+        rc = launch_strided_batch(h.dtype, h.vec_y, h.nt_y, false, h.wrap_y, at<StridedArgs>(table_dev, h.off_y2), sy2,
+                                  n, h.block[1], h.grid[1], 0, st);
+        if (rc) return rc;
+    }
+    if ((rc = mark(2 * VP_PHASE_DRIFT_Y2 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_X2))) return rc;
+    // the fused runs: y then x back into f; the others: x drift back into f
+    if ((rc = launch_plane_batch(false, false, at<char>(table_dev, h.off_p2), sp, n, h.plane_items, st))) return rc;
+    if (sweeps) {
+        rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x2), sx,
+                                  n, h.block[0], h.grid[0], 0, st);
+        if (rc) return rc;
+    }
+    if ((rc = mark(2 * VP_PHASE_DRIFT_X2 + 1)) || (rc = mark(2 * VP_PHASE_DIAG))) return rc;
     if (h.diag && (rc = launch_diag_finalize_batch(at<DiagArgs>(table_dev, h.off_diag), n, slot, st))) return rc;
     return mark(2 * VP_PHASE_DIAG + 1);
 }

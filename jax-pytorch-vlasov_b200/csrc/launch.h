@@ -160,6 +160,19 @@ int64_t plane_part_tiles(int64_t nvx, int64_t nvy);
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
               int64_t x_begin, int64_t x_count, const int* shift_x, const void* W_x, const int* shift_y,
               const void* W_y, double* part, int* tiles, const EqSplit* eq, int* status, int stall, cudaStream_t st);
+// Batched drift pairs (runs of up to 64 rows, FP32, nvy % 32 == 0, aligned):
+// one record of plane_run_bytes() per run in the device table (64-byte
+// aligned), filled on the host by plane_batch_run (in -> out; part: the
+// density partials [nx][nvx*nvy/32][ny] of the x-first pass, or NULL), items
+// = the run's groups of 32 columns; start[r] the prefix sums of the items.
+size_t plane_run_bytes();
+bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* a, const void* b,
+                      const void* c);
+int plane_batch_run(void* record, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
+                    const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part,
+                    int64_t* items);
+int launch_plane_batch(bool xfirst, bool rho, const void* runs, const int64_t* start, int n_runs, int64_t items,
+                       cudaStream_t st);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                     int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,
@@ -176,7 +189,7 @@ void strided_batch_finish(StridedArgs* a, int vec, int block);
 int strided_batch_pref_vec(int dtype);
 int launch_strided_batch(int dtype, int vec, int nt, bool rho, bool wrap, const StridedArgs* runs,
                          const int64_t* start, int n_runs, int block, int grid_cap, int max_line, cudaStream_t st);
-int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int64_t max_points, cudaStream_t st);
+int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int max_outer, int max_line, cudaStream_t st);
 int kick2d_batch_args(int dtype, const void* in, void* out, int64_t n_planes, int64_t nvx, int64_t nvy,
                       const double* Ex, const double* Ey, double dt, double dvx, double dvy, int window,
                       Kick2dArgs* a, int* vec);

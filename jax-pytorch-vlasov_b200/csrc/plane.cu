@@ -50,6 +50,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 
 #include "common.cuh"
@@ -1029,6 +1030,343 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
     }
 }
 
+// ---- many runs in one launch ------------------------------------------------
+// The batched form of k_plane for runs of up to 64 rows (the 64-run batch of
+// uneven grids): one persistent launch per drift pair for every run whose
+// layout fits, each CTA walking whole lines (one group of 32 columns over all
+// x) of the runs in order. Each run's tensor maps live in the batch's device
+// table next to its arguments. The arithmetic of every element is that of
+// k_plane (same FMA chains, FP32 intermediate), so f is bit-identical to the
+// run stepped alone; outputs leave by direct stores, and the x-first pass
+// stages its rows only for the FP64 density sums (four threads per y row,
+// the order of k_plane's). Blocks have 8 warps; the warps past a run's rows
+// compute nothing that is stored.
+struct alignas(64) PlaneRun {
+    CUtensorMap tin;    // [nx*ny][m] FP32, box {32, ny}
+    CUtensorMap thalo;  // box {32, HALO}: y rows 0..15 of an x row, after row ny
+    Args a;
+};
+
+// Whole lines of the batch's items, item g = (run r, group g - start[r]),
+// for CTA b of G: items b, b + G, ...; loads q = 0 .. nx + 4 of the group's
+// rows -s - 3 + q (mod nx), s the group's x shift.
+struct BSeq {
+    int64_t g, total, stride;
+    int r, cg, nx, ny, q, r0;
+    __device__ __forceinline__ void init(const PlaneRun* runs, const int64_t* start, int n_runs, int64_t b,
+                                         int64_t G) {
+        g = b;
+        stride = G;
+        total = start[n_runs];
+        r = 0;
+        if (valid()) begin(runs, start, n_runs);
+    }
+    __device__ __forceinline__ void begin(const PlaneRun* runs, const int64_t* start, int n_runs) {
+        while (r + 1 < n_runs && start[r + 1] <= g) ++r;
+        const Args& a = runs[r].a;
+        cg = (int)(g - start[r]);
+        nx = a.nx;
+        ny = a.ny;
+        const int jx = (int)(((int64_t)cg * CG / a.nvy) % a.nvx);
+        r0 = -__ldg(a.shift_x + jx) - 3;
+        q = 0;
+    }
+    __device__ __forceinline__ bool valid() const { return g < total; }
+    __device__ __forceinline__ int row() const {
+        const int v = (r0 + q) % nx;
+        return v < 0 ? v + nx : v;
+    }
+    __device__ __forceinline__ void next(const PlaneRun* runs, const int64_t* start, int n_runs) {
+        if (++q == nx + 5) {
+            g += stride;
+            if (valid()) begin(runs, start, n_runs);
+        }
+    }
+};
+
+struct BProducer {
+    BSeq seq;
+    long long issued;
+    int fenced;  // the last run whose tensor maps this CTA has acquired
+};
+
+__host__ __device__ constexpr size_t batch_smem_bytes(bool xfirst, bool rho) {
+    return (size_t)(DEPTH * buf_floats(YMAX / 2) + (rho ? 2 * stage_floats(YMAX / 2) : 0) +
+                    (xfirst ? 2 * buf_floats(YMAX / 2) : 0)) * 4 +
+           DEPTH * 8 + sizeof(BProducer);
+}
+
+template <bool XFIRST, bool RHO>
+__global__ void __launch_bounds__(YMAX / 2 / YT * 32, 2)
+    k_plane_batch(const PlaneRun* __restrict__ runs, const int64_t* __restrict__ start, int n_runs) {
+    static_assert(!RHO || XFIRST, "the density comes with the x-first order");
+    constexpr int YM = YMAX / 2, BUF = buf_floats(YM), STG = stage_floats(YM);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* slabs = reinterpret_cast<float*>(smem);    // [DEPTH][BUF]
+    float* stage = slabs + DEPTH * BUF;                // [2][STG] (the density's staged rows)
+    float* planes = stage + (RHO ? 2 * STG : 0);       // [2][BUF] (x first)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(planes + (XFIRST ? 2 * BUF : 0));
+    BProducer* prod = reinterpret_cast<BProducer*>(bars + DEPTH);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int y0 = warp * YT;
+    BSeq cons;
+    cons.init(runs, start, n_runs, blockIdx.x, gridDim.x);
+    if (!cons.valid()) return;
+    const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
+    auto issue = [&](int d, const BSeq& s) {
+        const PlaneRun* pr = runs + s.r;
+        if (prod->fenced != s.r) {
+            // the run's tensor maps reached global memory by a copy from the host
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pr->tin) : "memory");
+            if constexpr (!XFIRST)
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pr->thalo) : "memory");
+            prod->fenced = s.r;
+        }
+        const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
+        const int rr = s.row() * s.ny;
+        expect_bytes(bar, (uint32_t)((s.ny + (XFIRST ? 0 : HALO)) * CG * 4));
+        tma_load(&pr->tin, dst, bar, s.cg * CG, rr);
+        if constexpr (!XFIRST) tma_load(&pr->thalo, dst + (uint32_t)(s.ny * CG * 4), bar, s.cg * CG, rr);
+    };
+    if (tid == 0) {
+        prod->fenced = -1;
+        for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        BSeq p = cons;
+        long long n = 0;
+        for (; n < DEPTH && p.valid(); ++n) {
+            issue((int)n, p);
+            p.next(runs, start, n_runs);
+        }
+        prod->seq = p;
+        prod->issued = n;
+    }
+    __syncthreads();
+
+    float2 win[YT / 2][6];
+#pragma unroll
+    for (int p = 0; p < YT / 2; ++p)
+#pragma unroll
+        for (int s = 0; s < 6; ++s) win[p][s] = make_float2(0.f, 0.f);
+    float2 wx[6], wy[6];
+    int yoff = 0, ny = cons.ny, n_cg = 0;
+    float* out = nullptr;
+    double* part = nullptr;
+    int64_t m = 0;
+    uint32_t parity = 0;
+    long long L = 0;
+    bool failed = false, okacc = true;
+    bool pend = false;  // x first: a row waiting for its y drift
+    int pend_x = 0, pend_cg = 0;
+    bool rho_on = false;  // x first: a staged row waiting for its density
+    int rho_x = 0, rho_cg = 0, rho_ny = 0, rho_ncg = 0;
+    double* rho_part = nullptr;
+
+    // the weights, y window and run of the consumer's current group
+    auto tables = [&]() {
+        const Args& a = runs[cons.r].a;
+        out = a.out;
+        m = a.m;
+        ny = cons.ny;
+        part = a.part;
+        n_cg = a.n_cg;
+        const int jx = (int)(((int64_t)cons.cg * CG / a.nvy) % a.nvx);
+        const int jy = (int)(((int64_t)cons.cg * CG) % a.nvy) + lane;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
+            wx[j] = make_float2(u, u);
+            wy[j] = make_float2(v, v);
+        }
+        int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
+        if (r < 0) r += ny;
+        yoff = r * CG + lane;
+    };
+    tables();
+
+    // x first: y drift of the pending row from plane PL; stored, and staged
+    // in PL for its density
+    auto y_pending = [&](auto pl) {
+        constexpr int PL = decltype(pl)::value;
+        float2 o[YT / 2];
+        y_drift<false>(planes + PL * BUF + yoff, wy, 0.f, o);
+        if (pend) {
+            float* dst = out + ((int64_t)pend_x * ny + y0) * m + (int64_t)pend_cg * CG + lane;
+#pragma unroll
+            for (int p = 0; p < YT / 2; ++p) {
+                const int y = y0 + 2 * p;
+                if (y < ny) dst[(int64_t)(2 * p) * m] = o[p].x;
+                if (y + 1 < ny) dst[(int64_t)(2 * p + 1) * m] = o[p].y;
+            }
+        }
+        if constexpr (RHO) {
+            float* st = stage + PL * STG;
+#pragma unroll
+            for (int p = 0; p < YT / 2; ++p) {
+                const int y = y0 + 2 * p;
+                if (y < ny) st[y * CG + lane] = o[p].x;
+                if (y + 1 < ny) st[(y + 1) * CG + lane] = o[p].y;
+            }
+        }
+    };
+    // x first: density partials of the row staged in SP (thread: y row
+    // tid / 4, columns 8 (tid % 4) .. + 7; the sums of k_plane's order)
+    const int rrow = tid >> 2, rq = tid & 3;
+    auto rho_row = [&](auto sp) {
+        constexpr int SP = decltype(sp)::value;
+        const float4* src = reinterpret_cast<const float4*>(stage + SP * STG + rrow * CG) + 2 * rq;
+        const int odd = rrow & 1;
+        const float4 u = src[odd], v = src[1 - odd];
+        const double s = (((double)u.x + (double)u.y) + ((double)u.z + (double)u.w)) +
+                         (((double)v.x + (double)v.y) + ((double)v.z + (double)v.w));
+        double t = s + __shfl_xor_sync(0xffffffffu, s, 1);
+        t += __shfl_xor_sync(0xffffffffu, t, 2);
+        if (rho_on && rq == 0 && rrow < rho_ny) rho_part[((int64_t)rho_x * rho_ncg + rho_cg) * rho_ny + rrow] = t;
+    };
+
+    auto body = [&](auto step) -> bool {
+        constexpr int P = decltype(step)::value;
+        if constexpr (XFIRST) {
+            if constexpr (RHO) rho_row(Step<P & 1>{});
+            y_pending(Step<(P + 1) & 1>{});
+        }
+        const bool ok = wait_phase(bar0 + 8 * P, parity);
+        const bool emit = cons.q >= 5;
+        const float* sl = slabs + P * BUF;
+        float2 nv[YT / 2];
+        if constexpr (XFIRST) {
+            // x drift of the new row into plane P & 1 (read one step later)
+#pragma unroll
+            for (int p = 0; p < YT / 2; ++p)
+                nv[p] = make_float2(sl[(y0 + 2 * p) * CG + lane], sl[(y0 + 2 * p + 1) * CG + lane]);
+            float* pl = planes + (P & 1) * BUF;
+#pragma unroll
+            for (int p = 0; p < YT / 2; ++p) {
+                const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                      win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                const int y = y0 + 2 * p;
+                if (y < ny) pl[y * CG + lane] = o.x;
+                if (y + 1 < ny) pl[(y + 1) * CG + lane] = o.y;
+                if (y0 < HALO) {  // warp-uniform: the rows copied after row ny
+                    pl[(ny + y) * CG + lane] = o.x;
+                    pl[(ny + y + 1) * CG + lane] = o.y;
+                }
+            }
+        } else {
+            // y drift of the new row from its slab, then the x drift
+            y_drift<false>(sl + yoff, wy, 0.f, nv);
+            if (emit) {
+                float* dst = out + ((int64_t)(cons.q - 5) * ny + y0) * m + (int64_t)cons.cg * CG + lane;
+#pragma unroll
+                for (int p = 0; p < YT / 2; ++p) {
+                    const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                          win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                    const int y = y0 + 2 * p;
+                    if (y < ny) dst[(int64_t)(2 * p) * m] = o.x;
+                    if (y + 1 < ny) dst[(int64_t)(2 * p + 1) * m] = o.y;
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < YT / 2; ++p) win[p][P] = nv[p];
+        okacc = okacc && ok;
+        if (XFIRST || (P & 1)) {
+            // x first: every row (its plane and staged row change hands);
+            // y first: every second row (slabs P-1 and P are free)
+            if (__syncthreads_or(!okacc)) {
+                failed = true;
+                return false;
+            }
+            if (tid == 0) {
+                BSeq& p = prod->seq;
+#pragma unroll
+                for (int d = XFIRST ? P : P - 1; d <= P; ++d)
+                    if (p.valid()) {
+                        issue(d, p);
+                        p.next(runs, start, n_runs);
+                        prod->issued += 1;
+                    }
+            }
+        }
+        if (P == DEPTH - 1) parity ^= 1u;
+        ++L;
+        if constexpr (XFIRST) {
+            // the row y_pending staged this step belongs to the consumer's run
+            rho_on = pend;
+            rho_x = pend_x;
+            rho_cg = pend_cg;
+            rho_ny = ny;
+            rho_ncg = n_cg;
+            rho_part = part;
+            pend = emit;
+            pend_x = cons.q - 5;
+            pend_cg = cons.cg;
+        }
+        cons.next(runs, start, n_runs);
+        // a new group: its tables after the pending row of the last one went
+        // through (x first: one step into the group; y first: before its first row)
+        if (cons.valid() && cons.q == (XFIRST ? 1 : 0)) tables();
+        return cons.valid();
+    };
+
+    while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
+           body(Step<5>{})) {
+    }
+    if constexpr (!XFIRST) {
+        // a wait on a last, even row has had no barrier vote yet
+        if (!failed && __syncthreads_or(!okacc)) failed = true;
+    } else if (!failed) {
+        // the rows still in the pipeline: the density of the row staged at
+        // the last step, then the last row (its plane is complete)
+        const int last = (int)((L - 1) % DEPTH);
+        if constexpr (RHO) {
+            if (last & 1)
+                rho_row(Step<0>{});
+            else
+                rho_row(Step<1>{});
+        }
+        if (pend) {
+            if (last & 1)
+                y_pending(Step<1>{});
+            else
+                y_pending(Step<0>{});
+            if constexpr (RHO) {
+                __syncthreads();
+                rho_on = true;
+                rho_x = pend_x;
+                rho_cg = pend_cg;
+                rho_ny = ny;
+                rho_ncg = n_cg;
+                rho_part = part;
+                if (last & 1)
+                    rho_row(Step<1>{});
+                else
+                    rho_row(Step<0>{});
+            }
+        }
+    }
+    if (failed) {
+        // the whole share reads NaN, then the loads in flight land
+        __syncthreads();
+        BSeq z;
+        z.init(runs, start, n_runs, blockIdx.x, gridDim.x);
+        while (z.valid()) {
+            if (z.q >= 5) {
+                const Args& za = runs[z.r].a;
+                const int x = z.q - 5;
+                for (int i = 0; i < YT && y0 + i < z.ny; ++i) {
+                    za.out[((int64_t)x * z.ny + y0 + i) * za.m + (int64_t)z.cg * CG + lane] = NAN;
+                    if (RHO && lane == 0) za.part[((int64_t)x * za.n_cg + z.cg) * z.ny + y0 + i] = (double)NAN;
+                }
+            }
+            z.next(runs, start, n_runs);
+        }
+        if (tid == 0)
+            for (long long k = L; k < prod->issued; ++k)
+                wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+    }
+}
+
 // cuTensorMapEncodeTiled from the driver, looked up once
 static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -1128,7 +1466,81 @@ static int launch_xr(const CUtensorMap& tin, const CUtensorMap& thalo, const Arg
     return check_launch("k_plane_xr");
 }
 
+template <bool XFIRST, bool RHO>
+static int launch_batch_t(const PlaneRun* runs, const int64_t* start, int n_runs, int64_t items, cudaStream_t st) {
+    auto kern = k_plane_batch<XFIRST, RHO>;
+    constexpr size_t smem = batch_smem_bytes(XFIRST, RHO);
+    constexpr int block = YMAX / 2 / YT * 32;
+    static int raised[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(VP_ERR_CUDA, "plane batch: device index out of range");
+    if (!raised[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return set_cuda_error("cudaFuncSetAttribute(k_plane_batch)");
+        raised[dev] = 1;
+    }
+    const int occ = occupancy(kern, block, smem);
+    if (occ < 1) return set_error(VP_ERR_UNSUPPORTED, "plane batch: the kernel does not fit an SM");
+    const int64_t grid = std::min<int64_t>(items, (int64_t)sm_count() * occ);
+    kern<<<(unsigned)grid, block, smem, st>>>(runs, start, n_runs);
+    return check_launch("k_plane_batch");
+}
+
 }  // namespace plane
+
+size_t plane_run_bytes() { return sizeof(plane::PlaneRun); }
+
+// Runs of 49..64 rows. Measured on B200 (batches of one run size, FP32): the
+// fused pairs beat the sweeps for 64-row runs (64^4: 1.575 against 1.839 ms a
+// step) but not below (48 rows: 1.740 against 1.584; 16 rows: 2.4x slower):
+// a smaller run's TMA row boxes keep too few bytes in flight in the 6-slab
+// ring, and most of the block's warps have no rows.
+bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* a, const void* b,
+                      const void* c) {
+    return plane_fits(dtype, nx, ny, nvx, nvy, a) && plane_fits(dtype, nx, ny, nvx, nvy, b) &&
+           plane_fits(dtype, nx, ny, nvx, nvy, c) && ny > 48 && ny <= plane::YMAX / 2;
+}
+
+int plane_batch_run(void* record, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
+                    const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part,
+                    int64_t* items) {
+    using namespace plane;
+    // encoded in an aligned local record, then copied into the (host) table
+    PlaneRun rec;
+    std::memset(static_cast<void*>(&rec), 0, sizeof(PlaneRun));
+    PlaneRun* pr = &rec;
+    Args& a = pr->a;
+    a.out = static_cast<float*>(out);
+    a.nx = (int)nx;
+    a.ny = (int)ny;
+    a.nvx = (int)nvx;
+    a.nvy = (int)nvy;
+    a.xb = 0;
+    a.xc = (int)nx;
+    a.m = nvx * nvy;
+    a.n_cg = (int)(a.m / CG);
+    a.shift_x = shift_x;
+    a.W_x = static_cast<const float*>(W_x);
+    a.shift_y = shift_y;
+    a.W_y = static_cast<const float*>(W_y);
+    a.part = part;
+    if (!make_map(&pr->tin, in, a.m, nx * ny, (int)ny) || !make_map(&pr->thalo, in, a.m, nx * ny, HALO))
+        return set_error(VP_ERR_CUDA, "plane batch: cuTensorMapEncodeTiled failed");
+    std::memcpy(record, &rec, sizeof(PlaneRun));
+    *items = a.n_cg;
+    return VP_OK;
+}
+
+int launch_plane_batch(bool xfirst, bool rho, const void* runs, const int64_t* start, int n_runs, int64_t items,
+                       cudaStream_t st) {
+    using namespace plane;
+    if (items <= 0) return VP_OK;
+    const PlaneRun* pr = static_cast<const PlaneRun*>(runs);
+    if (!xfirst) return launch_batch_t<false, false>(pr, start, n_runs, items, st);
+    return rho ? launch_batch_t<true, true>(pr, start, n_runs, items, st)
+               : launch_batch_t<true, false>(pr, start, n_runs, items, st);
+}
 
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* f) {
     using namespace plane;

@@ -1034,15 +1034,49 @@ int run_kick2d(int dtype, const void* in, void* out, int64_t n_planes, int64_t n
 // many runs per launch (the batched step): argument blocks of every run live
 // in a device table; one launch per sweep covers the items of all runs
 // ---------------------------------------------------------------------------
-__global__ void k_rho_finalize_batch(const RhoFinRun* __restrict__ runs) {
-    const RhoFinRun a = runs[blockIdx.y];
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n_outer * a.n_line) return;
-    const int64_t o = i / a.n_line;
-    const int l = (int)(i % a.n_line);
-    double acc = 0.0;
-    for (int t = 0; t < a.tiles; ++t) acc += a.part[(o * a.tiles + t) * (int64_t)a.n_line + l];
-    a.rho[i] = acc * a.scale + a.offset;
+// The density of every run of a batch: block (line chunk, outer row o, run);
+// each run's partials are summed in the order the single-run step uses for
+// its tile count (k_rho_finalize_wide above 32 tiles, k_rho_finalize else),
+// so a run of a batch has the density of the same run stepped alone.
+__global__ void __launch_bounds__(32 * kFinSlices) k_rho_finalize_batch(const RhoFinRun* __restrict__ runs) {
+    __shared__ double sl[kFinSlices][33];
+    const RhoFinRun a = runs[blockIdx.z];
+    const int64_t o = blockIdx.y;
+    const int l = blockIdx.x * 32 + threadIdx.x;
+    if (o >= a.n_outer || blockIdx.x * 32 >= a.n_line) return;  // uniform over the block
+    const int sidx = threadIdx.y;
+    const bool ok = l < a.n_line;
+    const double* p = a.part + (o * a.tiles) * (int64_t)a.n_line + l;
+    if (a.tiles <= 32) {
+        if (sidx == 0 && ok) {
+            double acc = 0.0;
+            for (int t = 0; t < a.tiles; ++t) acc += p[(int64_t)t * a.n_line];
+            a.rho[o * a.n_line + l] = acc * a.scale + a.offset;
+        }
+        return;
+    }
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (ok) {
+        int t = sidx;
+        for (; t + 7 * kFinSlices < a.tiles; t += 8 * kFinSlices) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = __ldcs(p + (int64_t)(t + k * kFinSlices) * a.n_line);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] += v[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (t + k * kFinSlices < a.tiles) acc[k] += __ldcs(p + (int64_t)(t + k * kFinSlices) * a.n_line);
+    }
+    sl[sidx][threadIdx.x] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    __syncthreads();
+    if (sidx == 0 && ok) {
+        double s = sl[0][threadIdx.x];
+#pragma unroll
+        for (int k = 1; k < kFinSlices; ++k) s += sl[k][threadIdx.x];
+        a.rho[o * a.n_line + l] = s * a.scale + a.offset;
+    }
 }
 
 int strided_batch_args(int dtype, const void* in, void* out, int64_t n_outer, int64_t n_line, int64_t n_inner,
@@ -1122,9 +1156,9 @@ int launch_strided_batch(int dtype, int vec, int nt, bool rho, bool wrap, const 
     return launch_sb_d<false, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, st);
 }
 
-int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int64_t max_points, cudaStream_t st) {
-    const dim3 grid((unsigned)((max_points + 255) / 256), (unsigned)n_runs);
-    k_rho_finalize_batch<<<grid, 256, 0, st>>>(runs);
+int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int max_outer, int max_line, cudaStream_t st) {
+    const dim3 grid((unsigned)((max_line + 31) / 32), (unsigned)max_outer, (unsigned)n_runs);
+    k_rho_finalize_batch<<<grid, dim3(32, kFinSlices), 0, st>>>(runs);
     return check_launch("k_rho_finalize_batch");
 }
 

@@ -306,8 +306,11 @@ class Stepper1D(_Stepper):
 class BatchStepper2D:
     """Independent 2D2V runs of uneven sizes and parameters advanced in
     lockstep: vp_batch2d_step launches one kernel per substep for all runs
-    (9 launches per step whatever their number) and the state of run r is
-    advanced in place in self.f[r]. Each run's step is vp_step2d's.
+    (at most 12 launches per step whatever their number) and the state of run
+    r is advanced in place in self.f[r]. Each run's step is vp_step2d's: the
+    runs in `fused` (FP32, 48 < Ny <= 64, Nvy a multiple of 32) take their
+    drift pairs as fused passes, bit-identical to a Stepper2D with the fused
+    passes; the others one sweep per axis (fuse_drifts=False: all of them).
 
     runs: sequence of dicts with Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt
     (other keys are ignored). tiles: None (defaults), "auto" (the autotuner's
@@ -318,10 +321,11 @@ class BatchStepper2D:
     """
 
     def __init__(self, runs, dtype=torch.float32, device="cuda", physics_mode=True, window=-1, diagnostics=1,
-                 tiles=None, precise_tables=False, graph_slots=10):
+                 tiles=None, precise_tables=False, graph_slots=10, fuse_drifts=True):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise ValueError("BatchStepper2D runs on a CUDA device only")
+        self.fuse_drifts = bool(fuse_drifts)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.dtype = dtype
@@ -340,6 +344,10 @@ class BatchStepper2D:
         for p in self.params:
             shape = (int(p["Nx"]), int(p["Ny"]), int(p["Nvx"]), int(p["Nvy"]))
             self.shapes.append(shape)
+        # the rule of vp_batch2d_plan (the arenas keep every buffer 256-byte aligned)
+        self.fused = [self.fuse_drifts and dtype == torch.float32 and 48 < s[1] <= 64 and s[3] % 32 == 0
+                      for s in self.shapes]
+        for p, shape in zip(self.params, self.shapes):
             offs.append(fbytes)
             fbytes += al(esz * shape[0] * shape[1] * shape[2] * shape[3])
             wsoffs.append(wsbytes)
@@ -410,12 +418,13 @@ class BatchStepper2D:
         for r in range(n):
             sx, sy = (seg[r] if seg is not None else (0, 0))
             self._runs_c[r].segments_x, self._runs_c[r].segments_y = int(sx), int(sy)
-        if tiles is not None:
+        if tiles is not None or not self.fuse_drifts:
             t = L.BatchTiles()
             for key in ("block", "ctas_per_sm", "segments"):
-                vals = tiles.get(key, (0, 0, 0))
+                vals = (tiles or {}).get(key, (0, 0, 0))
                 for i in range(L.BATCH_KINDS):
                     getattr(t, key)[i] = int(vals[i])
+            t.sweeps_only = 0 if self.fuse_drifts else 1
         nb = L.query("vp_batch2d_table_bytes", n)
         table = ctypes.create_string_buffer(nb)
         L.call("vp_batch2d_plan", L.dtype_code(self.dtype), 1 if self.physics_mode else 0, self.diagnostics,

@@ -1,7 +1,9 @@
 """Batched uneven runs (vp_batch2d_*): every run of a batch follows the
 single-run step exactly. With the default tile shapes the batch reproduces
-Stepper2D bit for bit (same item bodies, same reduction order); other tile
-shapes only reorder the FP64 charge sums."""
+Stepper2D bit for bit (same item bodies, same reduction order): the runs whose
+drift pairs the batch fuses against a Stepper2D with the fused passes, the
+others against one sweep per axis; other tile shapes only reorder the FP64
+charge sums."""
 import math
 
 import numpy as np
@@ -14,8 +16,8 @@ pytestmark = pytest.mark.gpu
 
 RUNS = [
     dict(Nx=16, Ny=24, Nvx=32, Nvy=48, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=6.0, dt=0.1),
-    dict(Nx=32, Ny=16, Nvx=48, Nvy=32, Lx=10 * math.pi, Ly=6 * math.pi, Vx_max=8.0, Vy_max=7.0, dt=0.05),
-    dict(Nx=24, Ny=24, Nvx=64, Nvy=64, Lx=2 * math.pi / 0.7, Ly=2 * math.pi / 0.7, Vx_max=7.5, Vy_max=7.5,
+    dict(Nx=32, Ny=56, Nvx=48, Nvy=32, Lx=10 * math.pi, Ly=6 * math.pi, Vx_max=8.0, Vy_max=7.0, dt=0.05),
+    dict(Nx=24, Ny=64, Nvx=64, Nvy=64, Lx=2 * math.pi / 0.7, Ly=2 * math.pi / 0.7, Vx_max=7.5, Vy_max=7.5,
          dt=0.05),
     dict(Nx=8, Ny=8, Nvx=16, Nvy=12, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=5.0, dt=0.3),
     dict(Nx=12, Ny=40, Nvx=20, Nvy=24, Lx=8.0, Ly=9.0, Vx_max=5.0, Vy_max=6.0, dt=0.2),
@@ -28,21 +30,24 @@ def _ic(vp, p, r, dtype):
                                    p["Vy_max"], 0.05, 2 * math.pi / p["Lx"], 1.5, dtype=dtype)
 
 
-def _single(vp, p, dtype):
-    # the batch runs one sweep per axis: so does the single run it is held to
-    # bit for bit (the fused plane passes sum the density in another order)
+def _single(vp, p, dtype, fused):
+    # the same drift passes as the batch's run: fused pairs or one sweep per
+    # axis (the two sum the density in different orders)
     return vp.Stepper2D(p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"], p["Vx_max"], p["Vy_max"], p["dt"],
-                        dtype=dtype, window=-1, diagnostics=1, fuse_drifts=False)
+                        dtype=dtype, window=-1, diagnostics=1, fuse_drifts=fused)
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
 def test_batch_equals_single_runs(vp, dtype):
     b = vp.BatchStepper2D(RUNS, dtype=dtype, window=-1, diagnostics=1)
+    assert b.fused == ([False, True, True, False, False] if dtype == torch.float32 else [False] * len(RUNS))
     ref = []
     for r, p in enumerate(RUNS):
         f0 = _ic(vp, p, r, dtype)
         b.set_state(r, f0)
-        ref.append((_single(vp, p, dtype), f0.clone()))
+        st = _single(vp, p, dtype, b.fused[r])
+        assert st.passes(st.empty_f(), st.empty_f())[1] == b.fused[r]
+        ref.append((st, f0.clone()))
     hist = []
     for s in range(3):
         b.step(0)
@@ -53,6 +58,32 @@ def test_batch_equals_single_runs(vp, dtype):
             assert torch.equal(b.drho[r], st.drho) and torch.equal(b.phi[r], st.phi)
             d = hist[-1][r].cpu().numpy()
             np.testing.assert_array_equal(d[[0, 1, 5]], st.diag.cpu().numpy()[[0, 1, 5]])
+
+
+@pytest.mark.parametrize("physics", [True, False])
+def test_batch_fused_and_sweeps(vp, physics):
+    """The fused drift pairs of a batch against one sweep per axis: the same
+    f to FP32 rounding of the density's summation order, the same density."""
+    dtype = torch.float32
+    a = vp.BatchStepper2D(RUNS, dtype=dtype, physics_mode=physics, diagnostics=1 if physics else 0)
+    b = vp.BatchStepper2D(RUNS, dtype=dtype, physics_mode=physics, diagnostics=1 if physics else 0,
+                          fuse_drifts=False)
+    assert any(a.fused) and not any(b.fused)
+    for r, p in enumerate(RUNS):
+        f0 = _ic(vp, p, r, dtype)
+        a.set_state(r, f0)
+        b.set_state(r, f0)
+    for _ in range(3):
+        a.step(0)
+        b.step(0)
+    torch.cuda.synchronize()
+    for r in range(len(RUNS)):
+        if physics:
+            np.testing.assert_allclose(a.drho[r].cpu().numpy(), b.drho[r].cpu().numpy(), rtol=0, atol=1e-9)
+            scale = b.f[r].abs().max().item()
+            assert (a.f[r] - b.f[r]).abs().max().item() <= 1e-5 * scale
+        else:
+            assert torch.equal(a.f[r], b.f[r])  # drifts only: the same bits
 
 
 def test_batch_tile_shapes(vp):
@@ -131,8 +162,8 @@ def test_batch_seeded_draws(vp):
     for r, p in enumerate(runs):
         b.set_state(r, vp.workloads.initial_2d(p["kind"], p["Nx"], p["Ny"], p["Nvx"], p["Nvy"], p["Lx"], p["Ly"],
                                                p["Vx_max"], p["Vy_max"], p["eps"], p["k"], p["v0"]))
-    pick = [0, 17, 40, 63]
-    singles = {r: (_single(vp, runs[r], torch.float32), b.f[r].clone()) for r in pick}
+    pick = [0, 17, 40, 63] + [r for r in range(len(runs)) if runs[r]["Nvy"] % 32][:2]  # fused and not
+    singles = {r: (_single(vp, runs[r], torch.float32, b.fused[r]), b.f[r].clone()) for r in pick}
     h = torch.zeros((2, len(runs), 8), dtype=torch.float64, device="cuda")
     b.run(2, history=h, graph=False)
     for r, (st, f) in singles.items():
