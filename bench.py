@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
     ap.add_argument("--dtype", choices=["float32", "bfloat16", "float64"], default=None)
     ap.add_argument("--size", type=int, default=None, help="override N of a 2D2V workload (N^4 grid)")
+    ap.add_argument("--grid", default=None,
+                    help="override the grid of a 2D2V workload: NX,NY,NVX,NVY (small cases for profiling)")
     ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -90,6 +92,7 @@ def parse():
     ap.add_argument("--tiles", choices=["default", "auto", "tune"], default="auto",
                     help="batched workload: default tile shapes, the autotuner's cache, or tune now")
     a = ap.parse_args()
+    a.grid_override = a.grid
     wl = WORKLOADS[a.workload]
     a.kind, a.grid, a.L, a.vmax, a.dt, a.ic, a.icp, dflt, a.desc = wl
     a.dtype = a.dtype or dflt
@@ -102,6 +105,13 @@ def parse():
             raise SystemExit("--size applies to 2D2V workloads")
         a.grid = (a.size,) * 4
         a.desc = a.desc.replace("128^4", f"{a.size}^4")
+    if a.grid_override:
+        if a.kind != "2d":
+            raise SystemExit("--grid applies to 2D2V workloads")
+        a.grid = tuple(int(v) for v in a.grid_override.split(","))
+        if len(a.grid) != 4 or a.grid[2] != a.grid[3] or a.grid[0] < 1 or a.grid[1] < 1:
+            raise SystemExit("--grid takes NX,NY,NV,NV (equal velocity sizes)")
+        a.desc = a.desc.replace("128^4", "x".join(map(str, a.grid)))
     return a
 
 
@@ -310,11 +320,12 @@ def _initial_f(a, dev, dtype, rank, torch):
         ops = importlib.import_module("jax-pytorch-vlasov_b200.ops")
         return ops.init_product(1.0 + eps * torch.cos(a.icp[1] * x), torch.exp(-0.5 * v * v) / math.sqrt(2 * math.pi),
                                 dtype)
-    n, _, nv, _ = a.grid
-    x = torch.linspace(0, a.L, n + 1, dtype=gdt, device=dev)[:-1]
+    nx, ny, nv, _ = a.grid
+    x = torch.linspace(0, a.L, nx + 1, dtype=gdt, device=dev)[:-1]
+    y = torch.linspace(0, a.L, ny + 1, dtype=gdt, device=dev)[:-1]
     v = torch.linspace(-a.vmax, a.vmax, nv, dtype=gdt, device=dev)
     k = a.icp[1]
-    sp = 1.0 + eps * (torch.cos(k * x)[:, None] + torch.cos(k * x)[None, :])
+    sp = 1.0 + eps * (torch.cos(k * x)[:, None] + torch.cos(k * y)[None, :])
     M = lambda u: torch.exp(-0.5 * u * u) / math.sqrt(2 * math.pi)  # noqa: E731
     if a.ic == "landau":
         fv = M(v)[:, None] * M(v)[None, :]

@@ -245,6 +245,8 @@ class LearnedStepper2D:
         nb = L.query("vp_poisson2d_workspace_bytes", Nx, Ny)
         self.ws = torch.empty(nb, dtype=torch.uint8, device=b.device)
         self._graphs = {}
+        # the fused drift pairs take the layout (vp_drift_pair's conditions)
+        self._pairs = b.passes(b.empty_f(), b.empty_f())[1]
 
     def _drift(self, f, axis, out):
         b = self.base
@@ -263,22 +265,31 @@ class LearnedStepper2D:
 
     def step(self, f_in, f_out, energy=None):
         """One step f_in -> f_out (distinct buffers); energy: optional float64
-        [2] = {field energy, mass} of the mid-step field."""
+        [2] = {field energy, mass} of the mid-step field. Without a drift
+        network the position drifts go in pairs through the fused passes
+        (the first one forms the density) where the layout allows."""
         b = self.base
         st = L.stream_of(f_in)
-        self._drift(f_in, 0, self.t1)
-        self._drift(self.t1, 1, self.t2)
         Nx, Ny, Nvx, Nvy = self.shape
-        L.call("vp_rho", L.ptr(self.t2), L.VP_F32, Nx * Ny, Nvx * Nvy, float(b.dvx), float(b.dvy), L.ptr(self.rho),
-               L.VP_F64, st)
+        fused = self.drift_net is None and self._pairs
+        if fused:
+            ops.drift_pair(f_in, b.tx, b.ty, True, out=self.t2, scale=b.dvx * b.dvy, rho=self.rho)
+        else:
+            self._drift(f_in, 0, self.t1)
+            self._drift(self.t1, 1, self.t2)
+            L.call("vp_rho", L.ptr(self.t2), L.VP_F32, Nx * Ny, Nvx * Nvy, float(b.dvx), float(b.dvy),
+                   L.ptr(self.rho), L.VP_F64, st)
         e = self.energy if energy is None else energy
         L.call("vp_poisson2d", L.ptr(self.rho), Nx, Ny, L.ptr(b.kx), L.ptr(b.ky), L.ptr(b.inv_ksq), float(b.dx),
                float(b.dy), L.ptr(b.ex), L.ptr(b.ey), L.ptr(b.drho), L.ptr(b.phi), L.ptr(e), L.ptr(self.ws),
                self.ws.numel(), st)
         self._kick(self.t2, b.ex, 2, self.t1)
         self._kick(self.t1, b.ey, 3, self.t2)
-        self._drift(self.t2, 1, self.t1)
-        self._drift(self.t1, 0, f_out)
+        if fused:
+            ops.drift_pair(self.t2, b.tx, b.ty, False, out=f_out)
+        else:
+            self._drift(self.t2, 1, self.t1)
+            self._drift(self.t1, 0, f_out)
         return f_out
 
     def run(self, f, nsteps: int, history=None, graph: bool = True, chunk: int = 10):

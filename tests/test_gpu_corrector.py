@@ -159,13 +159,17 @@ def test_training_lowers_loss(vp):
     assert losses[-1] < 0.8 * losses[0], (losses[0], losses[-1])
 
 
-def test_learned_step_with_zero_nets_is_plain_step(vp):
+@pytest.mark.parametrize("with_drift_net", [True, False])
+def test_learned_step_with_zero_nets_is_plain_step(vp, with_drift_net):
     """With zero output layers the learned stepper is the plain step (up to
-    FP32 summation order: separate kicks instead of the fused one)."""
+    FP32 summation order: separate kicks instead of the fused one). Without a
+    drift network its position drifts are the fused pairs."""
     C = vp.corrector
-    n = 16
+    n = 32  # the fused pairs take 32^4 (nvy a multiple of 32)
     L_ = 4 * math.pi
-    ls = C.LearnedStepper2D(C.Corrector("cuda"), n, n, n, n, L_, L_, 6.0, 6.0, 0.1, drift_net=C.Corrector("cuda"))
+    ls = C.LearnedStepper2D(C.Corrector("cuda"), n, n, n, n, L_, L_, 6.0, 6.0, 0.1,
+                            drift_net=C.Corrector("cuda") if with_drift_net else None)
+    assert ls._pairs
     st = vp.Stepper2D(n, n, n, n, L_, L_, 6.0, 6.0, 0.1, dtype=torch.float32, window=-1, precise_tables=True)
     f = vp.workloads.initial_2d("landau", n, n, n, n, L_, L_, 6.0, 6.0, 0.05, 0.5)
     h = torch.zeros((12, 2), dtype=torch.float64, device="cuda")
