@@ -434,8 +434,13 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
  *   h1 = relu(W1 x), h2 = relu(W2 [h1, 1, 0...]), o = W3 [h2, 1, 0...]
  *   out = sum_k (W[k][j] + o_k - mean(o_0..o_5)) f_k
  * with f_k the stencil values of vp_drift, j the table column of the cell
- * and alpha[j] its fractional shift. Matrix products run on tcgen05 tensor
- * cores with BF16 operands and FP32 accumulation.
+ * and alpha[j] its fractional shift. When n_line and n_inner are both powers
+ * of two the correction is projected line by line,
+ *   out_l -= mean over the line of (out_l - sum_k W[k][j] f_k),
+ * so that every line (o, c) keeps the plain sweep's sum (the drift conserves
+ * it, the kick changes it only by what leaves the velocity range); the
+ * training passes differentiate through the projection. Matrix products run
+ * on tcgen05 tensor cores with BF16 operands and FP32 accumulation.
  * net: bf16 row-major, packed W1 [64][16] (column 7 = bias), W2 [64][80]
  * (column 64 = bias), W3 [16][80] (rows 6..15 zero), then the transposed
  * copies W3T [64][16] (W3T[h][o] = W3[o][h]) and W2T [64][64]

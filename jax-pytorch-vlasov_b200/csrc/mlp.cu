@@ -10,6 +10,15 @@
 //   o  = W3 [h2, 1, 0]         W3: [16][80]  (rows >= 6 zero)
 //   dw = o[0:6] - mean(o[0:6])        (the weights keep summing to one)
 //   out = sum_k (w_k + dw_k) f_k
+// When the line length n and n_inner are powers of two the correction is
+// projected, line by line, to zero sum:
+//   out_l -= mean_l (out_l - plain_l),  plain_l = sum_k w_k f_k
+// so each line's sum changes exactly as in the plain sweep (the periodic
+// drift keeps it, the kick loses what leaves the velocity range). The tiles
+// of a CTA then run in super-tiles of P tiles that hold whole lines (a lane
+// keeps to one line in all P tiles); the line sums are reduced at the end of
+// the super-tile and subtracted from the outputs it wrote, which are still
+// in L2.
 // x, h1, h2 and the weights are BF16 operands of tcgen05.mma (kind::f16,
 // FP32 accumulators in tensor memory); dw and the output are FP32.
 //
@@ -29,14 +38,19 @@
 // Training (TRAIN = true) adds, per tile, the residual against a target,
 //   r = (out - target) * inv_scale,  loss += sum r^2,
 // the backward deltas on tensor cores
-//   do  = P (2 r inv_scale f)           (P: the zero-mean projection)
+//   do  = P (gy f),  gy = 2 r inv_scale (less its line mean when projected)
+//                                       (P: the zero-mean projection)
 //   dz2 = (do  W3)[0:64] * [z2 > 0]     (MMA with W3 transposed)
 //   dz1 = (dz2 W2)[0:64] * [z1 > 0]     (MMA with W2 transposed)
 // and the weight gradients accumulated in tensor memory over all tiles of
 // the CTA (reduction over cells = the MMA K):
 //   [dW2; dW1] = [dz2^T; dz1^T] [h1', x]      (one M=128, N=96 chain)
 //   dW3^T      = h2'^T do                     (M=128, N=16)
-// added to the global FP32 gradient once per CTA.
+// added to the global FP32 gradient once per CTA. A projected training
+// sweep runs the forward layers twice per super-tile: the first pass sums
+// (out - plain) and (plain - target) over each line, the second uses their
+// means: out' = out - mean(out - plain) and, since mean(out') = mean(plain),
+//   mean_l(gy) = 2 inv_scale^2 (mean(plain) - mean(target)).
 #include <stdint.h>
 
 #include <algorithm>
@@ -163,7 +177,7 @@ struct CellData {
 struct Smem {
     uint32_t x, h1, h2, w1, w2, w3, w3t, w2t;  // both modes
     uint32_t dO, dz2, aw, bw, h2t, doT;        // training only
-    uint32_t bar, tslot, loss, total;
+    uint32_t bar, tslot, loss, line, total;
 };
 
 __host__ __device__ constexpr uint32_t al128(uint32_t b) { return (b + 127u) & ~127u; }
@@ -198,6 +212,7 @@ __host__ __device__ constexpr Smem plan(bool train) {
     s.bar = take(8);
     s.tslot = take(4);
     s.loss = take(sub * TM * 8);
+    s.line = take(2 * TM * 4);  // line sums of the projection
     s.total = o;
     return s;
 }
@@ -231,6 +246,11 @@ struct MlpSweepArgs {
     double* loss;     // training: sum of r^2
     float inv_scale;  // training: residual scale
     int64_t cells;    // n_outer * n_line * n_inner
+    // line projection (set by run_mlp_sweep): with nb = 2^st_lg, super-tile
+    // st holds the tiles (st / nb) * per_st * nb + k * nb + st % nb,
+    // k < per_st; in each tile q lanes, qstride apart, belong to one line
+    // (q, qstride powers of two)
+    int proj, per_st, q, qstride, st_lg;
     int* status;
 };
 
@@ -246,11 +266,12 @@ __device__ void load_matrix(unsigned char* sm, uint32_t dst, const __nv_bfloat16
 }
 
 template <bool TRAIN, bool KICK>
-__global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __grid_constant__ SweepArgs a) {
+__global__ void __launch_bounds__(TM * subtiles(TRAIN), TRAIN ? 1 : 4) k_mlp_sweep(const __grid_constant__ SweepArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     constexpr Smem S = plan(TRAIN);
     constexpr int SUB = subtiles(TRAIN);
     constexpr int NT = TM * SUB;
+    static_assert(SUB == 1, "the super-tile loop takes one tile per item");
     constexpr uint32_t TD3 = TRAIN ? T_D3 : T_D1;  // inference: layer 3 reuses layer 1's columns
     const int t = threadIdx.x;
     const int u = t / TM;        // this thread's tile of the CTA
@@ -326,10 +347,10 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
     const int n = a.n_line;
     // stencil of a cell: f_k = in[o, l - s - (k - 2), c], taken mod n (drift)
     // or zero outside [0, n) (kick)
-    auto gather = [&](int64_t tile0) {
+    auto gather = [&](int64_t tile) {
         CellData d;
-        d.cell = (tile0 + u) * TM + tl;  // = (o * n + l) * n_inner + c
-        d.act = tile0 < tiles && d.cell < a.cells;
+        d.cell = (tile + u) * TM + tl;  // = (o * n + l) * n_inner + c
+        d.act = tile < tiles && d.cell < a.cells;
         d.al = 0.0f;
 #pragma unroll
         for (int k = 0; k < 6; ++k) d.f[k] = d.w[k] = 0.0f;
@@ -368,9 +389,41 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
         return d;
     };
 
-    const int64_t step = (int64_t)gridDim.x * SUB;
-    CellData nxt = gather((int64_t)blockIdx.x * SUB);
-    for (int64_t tile0 = (int64_t)blockIdx.x * SUB; tile0 < tiles && ok; tile0 += step) {
+    // super-tiles: P tiles holding whole lines (one tile without projection);
+    // training with projection passes over them twice (line sums, then the
+    // forward + backward pass)
+    const int P = a.per_st;
+    const int npass = (TRAIN && a.proj) ? 2 : 1;
+    const int items = npass * P;
+    const int64_t n_super = tiles / P;
+    auto tile_of = [&](int64_t st, int k) -> int64_t {
+        return (((st >> a.st_lg) * P + k) << a.st_lg) + (st & ((1ll << a.st_lg) - 1));
+    };
+    float* lred = reinterpret_cast<float*>(sm + S.line);
+    // a line's lanes: within a warp they are combined by shuffles (offsets
+    // qstride, 2 qstride, ... < 32), across warps through shared memory
+    // (cnt partials, xs apart, from gx)
+    const int qspan = a.q * a.qstride;
+    const int xs = max(a.qstride, 32);
+    const int cnt = qspan / xs;
+    const int gx = (tl / qspan) * qspan + tl % xs;
+    const float inv_n = 1.0f / (float)n;  // exact: n is a power of two when projecting
+    float lsum_c = 0.0f, lsum_d = 0.0f;   // this lane's share of its line's sums
+    float mc = 0.0f, md = 0.0f;           // line means of (out - plain), (plain - target)
+
+    int64_t st = blockIdx.x;
+    int j = 0;
+    CellData nxt = gather(st < n_super ? tile_of(st, 0) : tiles);
+    while (st < n_super && ok) {
+        const int pass = j / P, k_st = j - (j / P) * P;
+        int64_t st2 = st;
+        int j2 = j + 1;
+        if (j2 == items) {
+            st2 += gridDim.x;
+            j2 = 0;
+        }
+        const int64_t tile2 = st2 < n_super ? tile_of(st2, j2 % P) : tiles;
+        const bool last_pass = pass == npass - 1;
         const CellData cur = nxt;
         const bool act = cur.act;
         const int64_t cell = cur.cell;
@@ -400,7 +453,7 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
                       for (int v = 0; v < SUB; ++v)
                           gemm(tm + v * 128 + T_D1, base + S.x + v * XS, base + S.w1, K1, HID, false);
                   },
-                  [&] { nxt = gather(tile0 + step); })))
+                  [&] { nxt = gather(tile2); })))
             break;
         uint32_t m1[2] = {0u, 0u}, m2[2] = {0u, 0u};  // relu masks of z1, z2
 #pragma unroll
@@ -457,74 +510,117 @@ __global__ void __launch_bounds__(TM * subtiles(TRAIN), 1) k_mlp_sweep(const __g
 #pragma unroll
         for (int k = 0; k < 6; ++k) mean += ov[k];
         mean *= (1.0f / 6.0f);
-        float y = 0.0f;
+        float y = 0.0f, yp = 0.0f;
 #pragma unroll
         for (int k = 0; k < 6; ++k) y = fmaf(w[k] + (ov[k] - mean), f[k], y);
-        if (!TRAIN) {
-            if (act) a.out[cell] = y;
-            continue;
-        }
-        // ---- training: residual, deltas, weight gradients ----
-        const float tg = act ? a.target[cell] : 0.0f;
-        const float r = act ? (y - tg) * a.inv_scale : 0.0f;
-        loss_acc += (double)r * r;
-        const float gy = 2.0f * r * a.inv_scale;  // dL/dy
-        float g6[6], gm = 0.0f;
+        if (a.proj) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            g6[k] = gy * f[k];
-            gm += g6[k];
+            for (int k = 0; k < 6; ++k) yp = fmaf(w[k], f[k], yp);
         }
-        gm *= (1.0f / 6.0f);
-        {
-            float dv8[8];
+        if (!TRAIN) {
+            if (act) {
+                a.out[cell] = y;
+                lsum_c += y - yp;
+            }
+        } else if (!last_pass) {
+            if (act) {
+                const float tg = a.target[cell];
+                lsum_c += y - yp;
+                lsum_d += yp - tg;
+            }
+        } else {
+            // ---- training: residual, deltas, weight gradients ----
+            const float tg = act ? a.target[cell] : 0.0f;
+            const float r = act ? (y - mc - tg) * a.inv_scale : 0.0f;
+            loss_acc += (double)r * r;
+            const float gy = act ? 2.0f * (r - md * a.inv_scale) * a.inv_scale : 0.0f;  // dL/dy, less its line mean
+            float g6[6], gm = 0.0f;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                dv8[k] = act ? g6[k] - gm : 0.0f;
-                st_bf16(sm, S.doT + kmaj(k, t, KW), dv8[k]);
+                g6[k] = gy * f[k];
+                gm += g6[k];
             }
-            dv8[6] = dv8[7] = 0.0f;
-            st8_bf16(sm, S.dO + kmaj(t, 0, NO), dv8);
-        }
-        // dh2 = do W3 (B = W3^T [64][16])
-        if (!(ok = run([&] { gemm(tm + T_G2, base + S.dO, base + S.w3t, NO, HID, false); }))) break;
+            gm *= (1.0f / 6.0f);
+            {
+                float dv8[8];
 #pragma unroll
-        for (int q = 0; q < HID / 16; ++q) {
-            float v[16];
-            tmem_ld16(lane_base + T_G2 + q * 16, v);
-            tmem_wait_ld();
-            float dz[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int h = q * 16 + i;
-                dz[i] = act && ((m2[h >> 5] >> (h & 31)) & 1u) ? v[i] : 0.0f;
-                st_bf16(sm, S.aw + kmaj(h, t, KW), dz[i]);
+                for (int k = 0; k < 6; ++k) {
+                    dv8[k] = act ? g6[k] - gm : 0.0f;
+                    st_bf16(sm, S.doT + kmaj(k, t, KW), dv8[k]);
+                }
+                dv8[6] = dv8[7] = 0.0f;
+                st8_bf16(sm, S.dO + kmaj(t, 0, NO), dv8);
             }
-            st8_bf16(sm, S.dz2 + kmaj(t, q * 16, HID), dz);
-            st8_bf16(sm, S.dz2 + kmaj(t, q * 16 + 8, HID), dz + 8);
+            // dh2 = do W3 (B = W3^T [64][16])
+            if (!(ok = run([&] { gemm(tm + T_G2, base + S.dO, base + S.w3t, NO, HID, false); }))) break;
+#pragma unroll
+            for (int q = 0; q < HID / 16; ++q) {
+                float v[16];
+                tmem_ld16(lane_base + T_G2 + q * 16, v);
+                tmem_wait_ld();
+                float dz[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int h = q * 16 + i;
+                    dz[i] = act && ((m2[h >> 5] >> (h & 31)) & 1u) ? v[i] : 0.0f;
+                    st_bf16(sm, S.aw + kmaj(h, t, KW), dz[i]);
+                }
+                st8_bf16(sm, S.dz2 + kmaj(t, q * 16, HID), dz);
+                st8_bf16(sm, S.dz2 + kmaj(t, q * 16 + 8, HID), dz + 8);
+            }
+            // dh1 = dz2 W2 (B = W2^T [64][64])
+            if (!(ok = run([&] { gemm(tm + T_G1, base + S.dz2, base + S.w2t, HID, HID, false); }))) break;
+#pragma unroll
+            for (int q = 0; q < HID / 16; ++q) {
+                float v[16];
+                tmem_ld16(lane_base + T_G1 + q * 16, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int h = q * 16 + i;
+                    const float d = (m1[h >> 5] >> (h & 31)) & 1u ? v[i] : 0.0f;
+                    st_bf16(sm, S.aw + kmaj(HID + h, t, KW), act ? d : 0.0f);
+                }
+            }
+            // weight gradients over this tile's cells (K = the 128 cells)
+            const bool acc_w = wacc;
+            if (!(ok = run([&] {
+                      gemm(tm + T_WA, base + S.aw, base + S.bw, KW, 96, acc_w);
+                      gemm(tm + T_WB, base + S.h2t, base + S.doT, KW, NO, acc_w);
+                  })))
+                break;
+            wacc = true;
         }
-        // dh1 = dz2 W2 (B = W2^T [64][64])
-        if (!(ok = run([&] { gemm(tm + T_G1, base + S.dz2, base + S.w2t, HID, HID, false); }))) break;
-#pragma unroll
-        for (int q = 0; q < HID / 16; ++q) {
-            float v[16];
-            tmem_ld16(lane_base + T_G1 + q * 16, v);
-            tmem_wait_ld();
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int h = q * 16 + i;
-                const float d = (m1[h >> 5] >> (h & 31)) & 1u ? v[i] : 0.0f;
-                st_bf16(sm, S.aw + kmaj(HID + h, t, KW), act ? d : 0.0f);
+        // end of the super-tile's first pass: line means, then (inference)
+        // the outputs it wrote are moved onto the plain sweep's line sums
+        if (a.proj && pass == 0 && k_st == P - 1) {
+            for (int off = a.qstride; off < 32 && off < qspan; off <<= 1) {
+                lsum_c += __shfl_xor_sync(0xffffffffu, lsum_c, off);
+                lsum_d += __shfl_xor_sync(0xffffffffu, lsum_d, off);
+            }
+            if (cnt > 1) {
+                lred[tl] = lsum_c;
+                lred[TM + tl] = lsum_d;
+                __syncthreads();
+                lsum_c = lsum_d = 0.0f;
+                for (int m = 0; m < cnt; ++m) {
+                    lsum_c += lred[gx + m * xs];
+                    lsum_d += lred[TM + gx + m * xs];
+                }
+                __syncthreads();
+            }
+            mc = lsum_c * inv_n;
+            md = lsum_d * inv_n;
+            lsum_c = lsum_d = 0.0f;
+            if (!TRAIN) {
+                for (int k = 0; k < P; ++k) {
+                    const int64_t c2 = tile_of(st, k) * TM + tl;
+                    if (c2 < a.cells) a.out[c2] -= mc;
+                }
             }
         }
-        // weight gradients over this tile's cells (K = the 128 cells)
-        const bool acc_w = wacc;
-        if (!(ok = run([&] {
-                  gemm(tm + T_WA, base + S.aw, base + S.bw, KW, 96, acc_w);
-                  gemm(tm + T_WB, base + S.h2t, base + S.doT, KW, NO, acc_w);
-              })))
-            break;
-        wacc = true;
+        st = st2;
+        j = j2;
     }
 
     if (TRAIN && ok && wacc) {
@@ -583,6 +679,31 @@ int run_mlp_sweep(bool train, bool kick, const MlpSweepArgs& args, cudaStream_t 
     MlpSweepArgs a = args;
     a.cells = a.n_outer * a.n_line * a.n_inner;
     const int64_t tiles = (a.cells + mlp::TM - 1) / mlp::TM;
+    // line projection when n_line and n_inner are powers of two; a line
+    // (o, c) of n cells n_inner apart occupies
+    //   n_inner >= TM:      one lane in each of n tiles (n_inner / TM tiles apart)
+    //   n * n_inner >= TM:  TM / n_inner lanes in each of n * n_inner / TM consecutive tiles
+    //   n * n_inner <  TM:  n lanes of one tile
+    auto pow2 = [](int64_t v) { return v > 0 && (v & (v - 1)) == 0; };
+    const int64_t n = a.n_line, ni = a.n_inner;
+    a.proj = pow2(n) && pow2(ni) ? 1 : 0;
+    a.per_st = 1;
+    a.q = 1;
+    a.qstride = 1;
+    a.st_lg = 0;
+    if (a.proj) {
+        if (ni >= mlp::TM) {
+            a.per_st = (int)n;
+            while ((mlp::TM << a.st_lg) < ni) a.st_lg++;
+        } else if (n * ni >= mlp::TM) {
+            a.q = (int)(mlp::TM / ni);
+            a.qstride = (int)ni;
+            a.per_st = (int)(n * ni / mlp::TM);
+        } else {
+            a.q = (int)n;
+            a.qstride = (int)ni;
+        }
+    }
     // inference asks for at least 48 KB so that no more than four CTAs (4 x 128
     // tensor-memory columns) share an SM
     const size_t smem = train ? mlp_smem_bytes(true) : std::max<size_t>(mlp_smem_bytes(false), 48 * 1024);
@@ -593,8 +714,8 @@ int run_mlp_sweep(bool train, bool kick, const MlpSweepArgs& args, cudaStream_t 
     // training holds all 512 tensor-memory columns: one CTA per SM;
     // inference holds 128: four CTAs per SM
     const int64_t per_sm = train ? 1 : 4;
-    const int64_t sub = mlp::subtiles(train);
-    const int64_t grid = std::min<int64_t>((tiles + sub - 1) / sub, (int64_t)sm_count() * per_sm);
+    const int64_t n_super = tiles / a.per_st;  // super-tiles (tiles without projection)
+    const int64_t grid = std::min<int64_t>(n_super, (int64_t)sm_count() * per_sm);
     kern<<<(unsigned)std::max<int64_t>(grid, 1), mlp::TM * mlp::subtiles(train), smem, st>>>(a);
     return check_launch("k_mlp_sweep");
 }

@@ -10,6 +10,10 @@ vlasov2D2V.py:210-285, and this corrects those weights):
   z2 = W2 [h1, 1, 0],   h2 = bf16(relu(z2))
   o  = W3 [h2, 1, 0]
   y  = sum_k (w_k + o_k - mean(o_0..5)) f_k
+and, when the line length n and the stride n_inner of the swept lines are
+powers of two, the line projection
+  y_l -= mean_l (y_l - p_l),  p_l = sum_k w_k f_k  (the plain sweep)
+that keeps each line's sum equal to the plain sweep's.
 BF16 values are rounded to nearest even exactly as the device does; the
 matrix products are summed in float64 here (FP32 on the device), so the two
 agree to accumulation round-off, not bit for bit.
@@ -97,8 +101,36 @@ def drift_cells(f: np.ndarray, shift, W, alpha, axis: int, vel_axis: int):
     return F.reshape(6, -1).T, np.asarray(W, np.float32)[:, j].T, np.asarray(alpha, np.float32)[j]
 
 
-def forward_cells(F, w, al, W1, W2, W3):
-    """The corrected sweep of cells with stencils F, weights w, fractions al."""
+def lines_of(shape, axis: int):
+    """(n_outer, n, n_inner) of the lines swept along axis when the corrected
+    sweep projects them (n and n_inner powers of two), else None."""
+    n_outer = int(np.prod(shape[:axis]))
+    n, n_inner = int(shape[axis]), int(np.prod(shape[axis + 1:]))
+
+    def pow2(v):
+        return v > 0 and (v & (v - 1)) == 0
+
+    return (n_outer, n, n_inner) if pow2(n) and pow2(n_inner) else None
+
+
+def line_mean(v, lines) -> np.ndarray:
+    """Per cell (memory order), the float32 mean of v over the cell's line."""
+    n_outer, n, n_inner = lines
+    m = (np.asarray(v, np.float64).reshape(n_outer, n, n_inner).sum(axis=1) / n).astype(np.float32)
+    return np.broadcast_to(m[:, None, :], (n_outer, n, n_inner)).reshape(-1)
+
+
+def plain_cells(F, w) -> np.ndarray:
+    """The plain sweep sum_k w_k f_k (fused multiply-adds in k order)."""
+    y = np.zeros(F.shape[0], np.float32)
+    for k in range(6):
+        y = (w[:, k].astype(np.float64) * F[:, k].astype(np.float64) + y.astype(np.float64)).astype(np.float32)
+    return y
+
+
+def forward_cells(F, w, al, W1, W2, W3, lines=None):
+    """The corrected sweep of cells with stencils F, weights w, fractions al;
+    lines (from lines_of) turns on the line projection."""
     s = np.abs(F).max(axis=1)
     inv = np.where(s > 0, np.float32(1.0) / np.where(s > 0, s, 1).astype(np.float32), np.float32(0.0))
     inv = inv.astype(np.float32)
@@ -122,16 +154,21 @@ def forward_cells(F, w, al, W1, W2, W3):
     for k in range(6):  # fused multiply-add: exact product, one rounding
         a = (w[:, k] + (o[:, k] - mean)).astype(np.float32)
         y = (a.astype(np.float64) * F[:, k].astype(np.float64) + y.astype(np.float64)).astype(np.float32)
+    if lines is not None:
+        y = (y - line_mean(y - plain_cells(F, w), lines)).astype(np.float32)
     cache = dict(F=F, x=x, z1=z1, h1=h1, z2=z2, h2=h2, o=o, W1b=W1b, W2b=W2b, W3b=W3b)
     return y, cache
 
 
-def train_cells(F, w, al, target, W1, W2, W3, inv_scale):
-    """(sum r^2, dW1, dW2, dW3) of r = (y - target) * inv_scale."""
-    y, c = forward_cells(F, w, al, W1, W2, W3)
+def train_cells(F, w, al, target, W1, W2, W3, inv_scale, lines=None):
+    """(sum r^2, dW1, dW2, dW3) of r = (y - target) * inv_scale; with the
+    line projection dL/dy loses its line mean (the projection's transpose)."""
+    y, c = forward_cells(F, w, al, W1, W2, W3, lines)
     r = ((y - np.asarray(target, np.float32).reshape(-1)) * np.float32(inv_scale)).astype(np.float32)
     loss = float(np.sum(r.astype(np.float64) ** 2))
     gy = (np.float32(2.0) * r * np.float32(inv_scale)).astype(np.float32)
+    if lines is not None:
+        gy = (gy - line_mean(gy, lines)).astype(np.float32)
     g = gy[:, None] * c["F"]
     gm = g.sum(axis=1, dtype=np.float32) * np.float32(1.0 / 6.0)
     N = g.shape[0]
@@ -149,10 +186,12 @@ def train_cells(F, w, al, target, W1, W2, W3, inv_scale):
 
 def forward(f, shift, W, alpha, axis, vel_axis, W1, W2, W3):
     """Corrected drift of f (float32) and the intermediates of every cell."""
-    y, cache = forward_cells(*drift_cells(f, shift, W, alpha, axis, vel_axis), W1, W2, W3)
+    y, cache = forward_cells(*drift_cells(f, shift, W, alpha, axis, vel_axis), W1, W2, W3,
+                             lines_of(np.shape(f), axis))
     return y.reshape(np.shape(f)), cache
 
 
 def train_grad(f, target, shift, W, alpha, axis, vel_axis, W1, W2, W3, inv_scale):
     """(sum r^2, dW1, dW2, dW3) of the corrected drift against target."""
-    return train_cells(*drift_cells(f, shift, W, alpha, axis, vel_axis), target, W1, W2, W3, inv_scale)
+    return train_cells(*drift_cells(f, shift, W, alpha, axis, vel_axis), target, W1, W2, W3, inv_scale,
+                       lines_of(np.shape(f), axis))

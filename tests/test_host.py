@@ -166,3 +166,39 @@ def test_corrector_packing_matches_oracle(vp):
     ref = OC.pack_net(net.W1.numpy(), net.W2.numpy(), net.W3.numpy())
     np.testing.assert_array_equal(bits, ref)
     assert bits.size == C.NET_ELEMS
+
+
+def test_corrector_oracle_line_projection():
+    """The oracle's line projection: power-of-two lines keep the plain
+    sweep's sums, the projected dL/dy has zero line sums, and other line
+    lengths are left unprojected."""
+    from oracle import corrector as OC
+
+    rng = np.random.default_rng(3)
+    shape = (3, 8, 4)
+    lines = OC.lines_of(shape, 1)
+    assert lines == (3, 8, 4) and OC.lines_of((3, 6, 4), 1) is None and OC.lines_of((3, 8, 5), 1) is None
+    N = int(np.prod(shape))
+    F = rng.random((N, 6), dtype=np.float32)
+    w = rng.standard_normal((N, 6)).astype(np.float32) * np.float32(0.2)
+    al = rng.random(N, dtype=np.float32)
+    W1 = rng.standard_normal((OC.HID, OC.K1)).astype(np.float32) * np.float32(0.3)
+    W2 = rng.standard_normal((OC.HID, OC.K2)).astype(np.float32) * np.float32(0.1)
+    W3 = rng.standard_normal((OC.NO, OC.K2)).astype(np.float32) * np.float32(0.1)
+    W3[6:] = 0
+    y, _ = OC.forward_cells(F, w, al, W1, W2, W3, lines=lines)
+    yu, _ = OC.forward_cells(F, w, al, W1, W2, W3)
+    p = OC.plain_cells(F, w)
+    ls = lambda v: np.asarray(v, np.float64).reshape(shape).sum(axis=1)  # noqa: E731
+    np.testing.assert_allclose(ls(y), ls(p), rtol=0, atol=1e-5)
+    assert np.abs(ls(yu) - ls(p)).max() > 1e-3
+    # the projection's transpose: with residuals of zero line mean the
+    # projected loss and gradients are the unprojected ones of the same
+    # residuals (sum_l (gy_l - mean gy) dy_l = sum_l gy_l dy_l)
+    target = y + rng.standard_normal(N).astype(np.float32) * np.float32(0.01)
+    target = (target - OC.line_mean(target - y, lines)).astype(np.float32)
+    a = OC.train_cells(F, w, al, target, W1, W2, W3, 1.0, lines=lines)
+    b = OC.train_cells(F, w, al, (target + (yu - y)).astype(np.float32), W1, W2, W3, 1.0)
+    assert abs(a[0] - b[0]) <= 1e-4 * a[0]
+    for ga, gb in zip(a[1:], b[1:]):
+        assert np.linalg.norm(ga - gb) <= 2e-2 * np.linalg.norm(gb)
