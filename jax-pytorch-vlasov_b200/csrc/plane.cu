@@ -97,7 +97,7 @@ struct Args {
 // columns), then an even share of the rows of the n_cg % G groups left.
 struct Seq {
     int w, full, b, G;  // whole-line rounds: done, total; this CTA; CTAs
-    int64_t t, t1;      // share of the remaining lines' rows
+    int t, t1;          // share of the remaining lines' rows (n_cg * xc < 2^31)
     int cg, xa, n, q, r0;
     __device__ __forceinline__ void init(const Args& a, int b_, int G_) {
         b = b_;
@@ -105,8 +105,8 @@ struct Seq {
         full = a.n_cg / G;
         w = 0;
         const int64_t rest = (int64_t)(a.n_cg - full * G) * a.xc;
-        t = rest * b / G;
-        t1 = rest * (b + 1) / G;
+        t = (int)(rest * b / G);
+        t1 = (int)(rest * (b + 1) / G);
         if (valid()) start(a);
     }
     __device__ __forceinline__ void start(const Args& a) {
@@ -115,13 +115,12 @@ struct Seq {
             xa = a.xb;
             n = a.xc;
         } else {
-            cg = full * G + (int)(t / a.xc);
-            const int o = (int)(t % a.xc);
+            cg = full * G + t / a.xc;
+            const int o = t % a.xc;
             xa = a.xb + o;
-            const int64_t left = t1 - t;
-            n = (int)(left < (int64_t)(a.xc - o) ? left : (int64_t)(a.xc - o));
+            n = min(t1 - t, a.xc - o);
         }
-        const int jx = (int)(((int64_t)cg * CG / a.nvy) % a.nvx);
+        const int jx = (cg * CG / a.nvy) % a.nvx;
         r0 = xa - __ldg(a.shift_x + jx) - 3;
         q = 0;
     }
@@ -131,7 +130,7 @@ struct Seq {
         return r < 0 ? r + nx : r;
     }
     __device__ __forceinline__ void next(const Args& a) {
-        if (++q == n + 5) {
+        if (__builtin_expect(++q == n + 5, 0)) {
             if (w < full)
                 ++w;
             else
@@ -881,8 +880,8 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
         float bx = 0.f, by = 0.f;
         int yoff = 0;
         auto tables = [&]() {
-            const int jx = (int)(((int64_t)cons.cg * CG / a.nvy) % a.nvx);
-            const int jy = (int)(((int64_t)cons.cg * CG) % a.nvy) + lane;
+            const int jx = (cons.cg * CG / a.nvy) % a.nvx;
+            const int jy = (cons.cg * CG) % a.nvy + lane;
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
                 const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
@@ -959,7 +958,7 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             if (P == DEPTH - 1) parity ^= 1u;
             ++L;
             cons.next(a);
-            if (cons.valid() && cons.q == 0) tables();
+            if (__builtin_expect(cons.q == 0, 0) && cons.valid()) tables();
             return cons.valid();
         };
         while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
@@ -1547,6 +1546,7 @@ bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, con
     if (dtype != VP_F32) return false;
     if (ny < YMIN || ny > YMAX || nvy % CG != 0 || nvx < 1 || nx < 1) return false;
     if ((int64_t)nx * ny >= (1ll << 31) || nvx * nvy >= (1ll << 31)) return false;
+    if (nvx * nvy / CG * nx >= (1ll << 31)) return false;  // column groups x rows: 32-bit work counters
     if (reinterpret_cast<uintptr_t>(f) % 16 != 0) return false;
     return encoder() != nullptr;
 }
