@@ -746,18 +746,25 @@ def run_batch(a):
     value = world * cells * K / (ms_max / 1e3)
     ms_step = ms_max / K
     sweep_bytes = 2.0 * esz * cells
+    fused_cells = sum(math.prod(sh) for sh, fu in zip(st.shapes, st.fused) if fu)
+    # the x phases and the kick move every run's f once; the y phases only
+    # the runs on single-axis sweeps (the fused runs' y drifts ride in the x
+    # phases' plane passes)
+    phase_bytes = {"drift_x1": sweep_bytes, "drift_y1_rho": 2.0 * esz * (cells - fused_cells),
+                   "kick_vx_vy": sweep_bytes, "drift_y2": 2.0 * esz * (cells - fused_cells), "drift_x2": sweep_bytes}
     peak, peak_kind = measured_peak()
     ph = {p: sum(row[2 * j].elapsed_time(row[2 * j + 1]) for row in evs) / n_ev for j, p in enumerate(PHASES)}
-    groups = {"drift_x": ph["drift_x1"] + ph["drift_x2"], "drift_y_rho": ph["drift_y1_rho"],
-              "kick_vx_vy": ph["kick_vx_vy"], "drift_y": ph["drift_y2"]}
-    dom = max(groups, key=groups.get)
-    dom_ms = groups[dom] / (2 if dom == "drift_x" else 1)
-    achieved = sweep_bytes / (dom_ms * 1e-3) / 1e9
-    roof = {"bound": "hbm", "kernel": dom + " (batched, all runs)", "achieved": achieved, "peak": peak,
+    dom = max(phase_bytes, key=lambda p: ph[p])
+    achieved = phase_bytes[dom] / (ph[dom] * 1e-3) / 1e9
+    dom_name = {"drift_x1": "x1 phase: x-then-y plane pass of the fused runs, x sweep of the others",
+                "drift_x2": "x2 phase: y-then-x plane pass of the fused runs, x sweep of the others",
+                "kick_vx_vy": "fused vx+vy kick", "drift_y1_rho": "y drift + rho partials (swept runs)",
+                "drift_y2": "y drift (swept runs)"}[dom]
+    roof = {"bound": "hbm", "kernel": dom_name + " (batched)", "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": ncu_traffic(f"batch_{dom}_{a.dtype}"), "algorithmic_bytes_per_launch": sweep_bytes}
-    phase_gbs = {p: (sweep_bytes / (ph[p] * 1e-3) / 1e9 if ph[p] > 0 and p not in ("field", "diag") else None)
-                 for p in PHASES}
+            "traffic": ncu_traffic(f"batch_{dom}_{a.dtype}"), "algorithmic_bytes_per_launch": phase_bytes[dom]}
+    phase_gbs = {p: (phase_bytes[p] / (ph[p] * 1e-3) / 1e9 if p in phase_bytes and ph[p] > 0 and phase_bytes[p] > 0
+                     else None) for p in PHASES}
     h = hist.cpu()
     finite = bool(torch.isfinite(h[:, :, :2]).all())
 
@@ -846,10 +853,9 @@ def run_batch(a):
                        "diagnostics_level": diag, "graph": "10 steps per CUDA graph, replayed",
                        "tiles": {k: v for k, v in (st.tiles or {}).items() if k != "run_segments"},
                        "tiles_source": a.tiles,
-                       "fused_runs": int(sum(st.fused)), "fused_cells": int(sum(
-                           math.prod(sh) for sh, fu in zip(st.shapes, st.fused) if fu))},
+                       "fused_runs": int(sum(st.fused)), "fused_cells": int(fused_cells)},
             "roofline": roof,
-            "step_gbs": 5 * sweep_bytes / (ms_step * 1e-3) / 1e9,
+            "step_gbs": sum(phase_bytes.values()) / (ms_step * 1e-3) / 1e9,
             "gpu_launches": int(per_step_launches * K),
             "e2e": e2e,
             "cpu_baseline": cpu,

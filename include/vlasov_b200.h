@@ -371,14 +371,15 @@ size_t vp_step1d_workspace_bytes(int64_t nx, int64_t nv);
  *
  * Usage: fill one vp_batch2d_run per run; vp_batch2d_plan writes a table of
  * vp_batch2d_table_bytes(n) bytes into host memory; copy it unchanged to a
- * device buffer aligned to 64 bytes (it holds the TMA descriptors of the
- * fused runs); then every vp_batch2d_step(table, table_dev, slot, stream)
- * advances all runs by one step. The step only launches kernels (no copies,
- * no allocation), so a sequence of steps can be captured in a CUDA graph.
+ * device buffer aligned to 64 bytes; then every vp_batch2d_step(table,
+ * table_dev, slot, stream) advances all runs by one step. The step only
+ * launches kernels (no copies, no allocation), so a sequence of steps can be
+ * captured in a CUDA graph; it reads the host table too (the fused runs' TMA
+ * descriptors go to the kernels as parameters), which must stay as planned.
  * Each run's state is advanced in place: f -> s2 -> s1 -> f for the runs
- * whose drift pairs are fused (FP32, 48 < ny <= 64, nvy % 32 == 0, 16-byte
- * aligned buffers, unless vp_batch_tiles.sweeps_only), else
- * f -> s1 -> s2 -> s1 -> s2 -> f. */
+ * whose drift pairs are fused (FP32, 32 <= ny <= 64 with ny % 8 == 0,
+ * nvy % 32 == 0, 16-byte aligned buffers, unless vp_batch_tiles.sweeps_only),
+ * else f -> s1 -> s2 -> s1 -> s2 -> f. */
 typedef struct vp_batch2d_run {
     int32_t nx, ny, nvx, nvy;
     double dt, dx, dy, dvx, dvy;
@@ -414,7 +415,8 @@ typedef struct vp_batch_tiles {
     int32_t ctas_per_sm[VP_BATCH_KINDS]; /* persistent CTAs per SM, <= the occupancy limit */
     int32_t segments[VP_BATCH_KINDS];    /* CTAs per line of the drifts: 1, 2 or 4 (ignored for the kick) */
     int32_t sweeps_only;                 /* 1: one sweep per axis for every run, even those the fused
-                                            drift pairs take (FP32, 48 < ny <= 64, nvy % 32 == 0) */
+                                            drift pairs take (FP32, 32 <= ny <= 64, ny % 8 == 0,
+                                            nvy % 32 == 0) */
 } vp_batch_tiles;
 
 size_t vp_batch2d_table_bytes(int32_t n_runs);

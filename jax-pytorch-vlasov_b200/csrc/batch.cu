@@ -5,9 +5,11 @@
 // plain argument blocks (the same blocks the single-run kernels take) plus
 // per-sweep item offsets; the caller copies the table to the device once.
 // vp_batch2d_step then only launches kernels whose arguments point into the
-// device copy, so a sequence of steps is capturable in a CUDA graph. The runs
-// whose layout the fused drift pairs take (FP32, 48 < ny <= 64, nvy a
-// multiple of 32) make three passes over f: x then y with the rho partials
+// device copy (the fused runs' tensor maps are copied from the host table
+// into the plane kernels' parameters), so a sequence of steps is capturable
+// in a CUDA graph. The runs whose layout the fused drift pairs take (FP32,
+// 32 <= ny <= 64 a multiple of 8, nvy a multiple of 32; several column
+// groups of a run per CTA) make three passes over f: x then y with the rho partials
 // (f -> s2), the fused kick (s2 -> s1), y then x (s1 -> f); the others one
 // sweep per axis: x (f -> s1), y + rho partials (s1 -> s2), kick (s2 -> s1),
 // y (s1 -> s2), x (s2 -> f). Each kind of pass is one launch for all runs
@@ -46,9 +48,10 @@ struct BatchHeader {
     int64_t off_pois;  // Pois2dRun[n]
     int64_t off_rfin;  // RhoFinRun[n]
     int64_t off_diag;  // DiagArgs[n]
-    int64_t off_p1, off_p2;  // plane-pass records (x then y, y then x), 64-byte aligned
-    int64_t off_sp;          // int64[n+1]: prefix sums of the plane items
-    int64_t plane_items;     // all runs' plane items (0: no fused runs)
+    int64_t off_p1, off_p2;    // plane-pass records (x then y, y then x), 64-byte aligned
+    int64_t off_sp1, off_sp2;  // int64[n+1]: prefix sums of the two passes' plane items
+    int64_t plane_items1, plane_items2;  // all runs' plane items (0: no fused runs)
+    int32_t p1_slab_rows, p2_slab_rows;  // the largest ring slab of the fused runs
     int64_t sweep_items;     // all runs' x-drift items (0: every run fused)
     int64_t total_bytes;
 };
@@ -58,7 +61,7 @@ size_t al64(size_t b) { return (b + 63) & ~size_t(63); }
 
 struct Layout {
     int64_t off_x1, off_y1, off_y2, off_x2, off_sx, off_sy1, off_sy2, off_sk, off_kick, off_pois, off_rfin, off_diag,
-        off_p1, off_p2, off_sp, total;
+        off_p1, off_p2, off_sp1, off_sp2, total;
 };
 
 Layout layout_for(int n) {
@@ -81,7 +84,8 @@ Layout layout_for(int n) {
     L.off_pois = take(sizeof(Pois2dRun) * n);
     L.off_rfin = take(sizeof(RhoFinRun) * n);
     L.off_diag = take(sizeof(DiagArgs) * n);
-    L.off_sp = take(sizeof(int64_t) * (n + 1));
+    L.off_sp1 = take(sizeof(int64_t) * (n + 1));
+    L.off_sp2 = take(sizeof(int64_t) * (n + 1));
     off = al64(off);  // tensor maps inside the plane records need 64-byte alignment
     L.off_p1 = (int64_t)off;
     off += al64(plane_run_bytes() * n);
@@ -160,9 +164,11 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     int vx_min = 4, ntx_min = 7, vy_min = 4, nty_min = 7, vk_min = 4;
     bool wrap_x = false, wrap_y = false;  // some run sweeps whole lines of a multiple of 8 rows
     const bool sweeps_only = tiles && tiles->sweeps_only;
-    int64_t* sp = at<int64_t>(table, L.off_sp);
+    int64_t* sp1 = at<int64_t>(table, L.off_sp1);
+    int64_t* sp2 = at<int64_t>(table, L.off_sp2);
     std::vector<char> fused(n_runs, 0);
-    sp[0] = 0;
+    sp1[0] = sp2[0] = 0;
+    int slab1 = 0, slab2 = 0;
     for (int r = 0; r < n_runs; ++r) {
         const vp_batch2d_run& d = runs[r];
         if (d.nx <= 0 || d.ny <= 0 || d.nvx <= 1 || d.nvy <= 1)
@@ -191,17 +197,22 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         // the fused drift pairs: f -> s2 (x then y, the rho partials), then
         // s1 -> f (after the kick) or s2 -> f (without it)
         fused[r] = !sweeps_only && plane_batch_fits(dtype, nx, ny, nvx, nvy, d.f, d.s1, d.s2);
-        int64_t items = 0;
+        int64_t items1 = 0, items2 = 0;
         if (fused[r]) {
-            int rc = plane_batch_run(static_cast<char*>(table) + L.off_p1 + r * plane_run_bytes(), d.f, d.s2, nx, ny,
-                                     nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, want_rho ? w.part : nullptr,
-                                     &items);
+            int rows1 = 0, rows2 = 0;
+            int rc = plane_batch_run(static_cast<char*>(table) + L.off_p1 + r * plane_run_bytes(), true, d.f, d.s2, nx,
+                                     ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, want_rho ? w.part : nullptr,
+                                     &items1, &rows1);
             if (!rc)
-                rc = plane_batch_run(static_cast<char*>(table) + L.off_p2 + r * plane_run_bytes(), phys ? d.s1 : d.s2,
-                                     d.f, nx, ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, nullptr, &items);
+                rc = plane_batch_run(static_cast<char*>(table) + L.off_p2 + r * plane_run_bytes(), false,
+                                     phys ? d.s1 : d.s2, d.f, nx, ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y,
+                                     nullptr, &items2, &rows2);
             if (rc) return rc;
+            slab1 = std::max(slab1, rows1);
+            slab2 = std::max(slab2, rows2);
         }
-        sp[r + 1] = sp[r] + items;
+        sp1[r + 1] = sp1[r] + items1;
+        sp2[r + 1] = sp2[r] + items2;
         int v, nt;
         // x drifts: f -> s1 and s2 -> f (with the kicks) or s1 -> f (without)
         strided_batch_args(dtype, d.f, d.s1, 1, nx, ny * nvx * nvy, nvy, nvx, d.shift_spread_x, d.shift_x, d.W_x,
@@ -323,11 +334,15 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     h.grid[1] = grid_for(per_sm[1], std::max(sy1[n_runs], sy2[n_runs]));
     h.grid[2] = grid_for(per_sm[2], std::max<int64_t>(sk[n_runs], 1));
     h.kick_smem = kick_smem;
-    h.plane_items = sp[n_runs];
+    h.plane_items1 = sp1[n_runs];
+    h.plane_items2 = sp2[n_runs];
+    h.p1_slab_rows = slab1;
+    h.p2_slab_rows = slab2;
     h.sweep_items = sx[n_runs];
     h.off_p1 = L.off_p1;
     h.off_p2 = L.off_p2;
-    h.off_sp = L.off_sp;
+    h.off_sp1 = L.off_sp1;
+    h.off_sp2 = L.off_sp2;
     h.off_x1 = L.off_x1;
     h.off_y1 = L.off_y1;
     h.off_y2 = L.off_y2;
@@ -366,11 +381,14 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     };
     const bool want_rho = h.phys || h.diag;
     const bool sweeps = h.sweep_items > 0;
-    const int64_t* sp = at<int64_t>(table_dev, h.off_sp);
+    const int64_t* sp1 = at<int64_t>(table_dev, h.off_sp1);
+    const int64_t* sp2 = at<int64_t>(table_dev, h.off_sp2);
     // the fused runs: x then y (dt/2 each) with the rho partials, f -> s2;
     // the others: x drift (dt/2), f -> s1
     if ((rc = mark(2 * VP_PHASE_DRIFT_X1))) return rc;
-    if ((rc = launch_plane_batch(true, want_rho, at<char>(table_dev, h.off_p1), sp, n, h.plane_items, st))) return rc;
+    rc = launch_plane_batch(true, want_rho, at<char>(table_dev, h.off_p1), at<char>(table, h.off_p1), sp1,
+                            at<int64_t>(table, h.off_sp1), n, h.plane_items1, h.p1_slab_rows, st);
+    if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x1), sx,
                                   n, h.block[0], h.grid[0], 0, st);
@@ -407,7 +425,9 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     }
     if ((rc = mark(2 * VP_PHASE_DRIFT_Y2 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_X2))) return rc;
     // the fused runs: y then x back into f; the others: x drift back into f
-    if ((rc = launch_plane_batch(false, false, at<char>(table_dev, h.off_p2), sp, n, h.plane_items, st))) return rc;
+    rc = launch_plane_batch(false, false, at<char>(table_dev, h.off_p2), at<char>(table, h.off_p2), sp2,
+                            at<int64_t>(table, h.off_sp2), n, h.plane_items2, h.p2_slab_rows, st);
+    if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x2), sx,
                                   n, h.block[0], h.grid[0], 0, st);

@@ -160,19 +160,24 @@ int64_t plane_part_tiles(int64_t nvx, int64_t nvy);
 int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
               int64_t x_begin, int64_t x_count, const int* shift_x, const void* W_x, const int* shift_y,
               const void* W_y, double* part, int* tiles, const EqSplit* eq, int* status, int stall, cudaStream_t st);
-// Batched drift pairs (runs of up to 64 rows, FP32, nvy % 32 == 0, aligned):
-// one record of plane_run_bytes() per run in the device table (64-byte
-// aligned), filled on the host by plane_batch_run (in -> out; part: the
-// density partials [nx][nvx*nvy/32][ny] of the x-first pass, or NULL), items
-// = the run's groups of 32 columns; start[r] the prefix sums of the items.
+// Batched drift pairs (runs of up to 64 rows, a multiple of 8, FP32,
+// nvy % 32 == 0, aligned): one record of plane_run_bytes() per run and pass
+// in the device table (64-byte aligned), filled on the host by
+// plane_batch_run (in -> out; part: the density partials
+// [nx][nvx*nvy/32][ny] of the x-first pass, or NULL); items = the run's
+// items (x first: packs of groups of 32 columns; y first: groups), start[r]
+// the prefix sums of the items; slab_rows the rows of one ring slab of the
+// run, the launch takes the largest over its runs.
 size_t plane_run_bytes();
 bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* a, const void* b,
                       const void* c);
-int plane_batch_run(void* record, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
-                    const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part,
-                    int64_t* items);
-int launch_plane_batch(bool xfirst, bool rho, const void* runs, const int64_t* start, int n_runs, int64_t items,
-                       cudaStream_t st);
+int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx,
+                    int64_t nvy, const int* shift_x, const void* W_x, const int* shift_y, const void* W_y,
+                    double* part, int64_t* items, int* slab_rows);
+// runs_host / start_host: the host copies of the records and prefix sums
+// (the x-first pass takes the runs' tensor maps as a kernel parameter)
+int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs_host, const int64_t* start,
+                       const int64_t* start_host, int n_runs, int64_t items, int slab_rows, cudaStream_t st);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                     int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,

@@ -50,6 +50,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <cmath>
 
@@ -1030,114 +1031,496 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
 }
 
 // ---- many runs in one launch ------------------------------------------------
-// The batched form of k_plane for runs of up to 64 rows (the 64-run batch of
-// uneven grids): one persistent launch per drift pair for every run whose
-// layout fits, each CTA walking whole lines (one group of 32 columns over all
-// x) of the runs in order. Each run's tensor maps live in the batch's device
-// table next to its arguments. The arithmetic of every element is that of
-// k_plane (same FMA chains, FP32 intermediate), so f is bit-identical to the
-// run stepped alone; outputs leave by direct stores, and the x-first pass
-// stages its rows only for the FP64 density sums (four threads per y row,
-// the order of k_plane's). Blocks have 8 warps; the warps past a run's rows
-// compute nothing that is stored.
+// The batched drift pairs for runs of up to 64 rows (the 64-run batch of
+// uneven grids): one persistent launch per pair for every run whose layout
+// fits, each CTA walking whole lines (column groups over all x) of the runs
+// in order, several groups of one run at a time. The runs' arguments live in
+// the batch's device table; their tensor maps go to the kernel as a
+// parameter (up to XB_MAXR runs a launch), so that TMA reads its
+// descriptors from the parameter space as in the single-run kernels (with
+// the maps in the device table the same kernels ran at about half the
+// speed). The arithmetic of every element is that of the single-run passes
+// (same FMA chains, FP32 intermediate), so f is bit-identical to the run
+// stepped alone.
 struct alignas(64) PlaneRun {
     CUtensorMap tin;    // [nx*ny][m] FP32, box {32, ny}
-    CUtensorMap thalo;  // box {32, HALO}: y rows 0..15 of an x row, after row ny
+    CUtensorMap thalo;  // box {32, halo rows}: y rows 0.. of an x row, after row ny
     Args a;
+    int k_pack;         // column groups stepped together by one CTA
+    int slab_rows;      // rows of one ring slab: k_pack boxes of ny + halo rows
 };
 
-// Whole lines of the batch's items, item g = (run r, group g - start[r]),
-// for CTA b of G: items b, b + G, ...; loads q = 0 .. nx + 4 of the group's
-// rows -s - 3 + q (mod nx), s the group's x shift.
-struct BSeq {
-    int64_t g, total, stride;
-    int r, cg, nx, ny, q, r0;
-    __device__ __forceinline__ void init(const PlaneRun* runs, const int64_t* start, int n_runs, int64_t b,
-                                         int64_t G) {
-        g = b;
+// ---- many runs, x then y, register window ---------------------------------
+// The batched x-first pass in the form of k_plane_xrd: 8 drift warps of 16 y
+// rows with the 21-row x window in registers, and a warpgroup of 4 density
+// warps (the FP64 row sums of the staged output, one thread a row, in
+// k_plane_xrd's order; its first thread issues the TMA loads). A CTA steps a
+// pack of K column groups of one run through x together, K = 8 / ceil(ny /
+// 16) (two groups of up to 64 rows, four of up to 32): warp w works on group
+// w / wpg, rows 16 (w % wpg) .. +15. Each step loads K boxes of ny + 20 rows,
+// one per group (the groups of a pack lie in different vx, so their x rows
+// differ). The K ny <= 128 output rows of a step are staged for the density
+// warps without padding, 16-byte chunks swizzled by row (chunk ^ row % 8;
+// ny is a multiple of 8, so a warp's rows start on a multiple of 8). Every
+// element takes k_plane_xrd's FMA chains and every density partial its sum
+// order, so f and rho are bit-identical to the run stepped alone.
+constexpr int XB_SROWS = 128;  // staged rows per slot
+// packs per ny: up to 32 rows four groups of ny + 20 rows, up to 64 two
+constexpr int xb_pack(int ny) { return XRD_CW / ((ny + YT2 - 1) / YT2); }
+constexpr int XB_MAX_SLAB_ROWS = 4 * (32 + HALO2);
+struct PackMeta {
+    int x, r, cg0, kv, ny, valid, pad0, pad1;
+};
+
+// Whole lines of the batch's packs, pack g = (run r, groups k_pack (g -
+// start[r]) ..), for CTA b of G: packs b, b + G, ...; step q = 0 .. nx + 4
+// loads, for each group k of the pack, x row r0_k + q (mod nx).
+struct PSeq {
+    int g, total, stride;
+    int r, K, kv, cg0, nx, ny, q;
+    __device__ __forceinline__ void init(const PlaneRun* runs, const int64_t* start, int n_runs, int b, int G) {
+        g = (int)start[0] + b;  // start[] holds the prefix sums of the whole batch
         stride = G;
-        total = start[n_runs];
+        total = (int)start[n_runs];
         r = 0;
         if (valid()) begin(runs, start, n_runs);
     }
     __device__ __forceinline__ void begin(const PlaneRun* runs, const int64_t* start, int n_runs) {
         while (r + 1 < n_runs && start[r + 1] <= g) ++r;
-        const Args& a = runs[r].a;
-        cg = (int)(g - start[r]);
-        nx = a.nx;
-        ny = a.ny;
-        const int jx = (int)(((int64_t)cg * CG / a.nvy) % a.nvx);
-        r0 = -__ldg(a.shift_x + jx) - 3;
+        const PlaneRun& pr = runs[r];
+        K = pr.k_pack;
+        cg0 = (g - (int)start[r]) * K;
+        kv = min(K, pr.a.n_cg - cg0);
+        nx = pr.a.nx;
+        ny = pr.a.ny;
         q = 0;
     }
     __device__ __forceinline__ bool valid() const { return g < total; }
-    __device__ __forceinline__ int row() const {
-        const int v = (r0 + q) % nx;
-        return v < 0 ? v + nx : v;
+    // the next step of the pack; false at its end (then next_pack)
+    __device__ __forceinline__ bool step_on() { return ++q < nx + 5; }
+    __device__ __forceinline__ void next_pack(const PlaneRun* runs, const int64_t* start, int n_runs) {
+        g += stride;
+        if (valid()) begin(runs, start, n_runs);
     }
     __device__ __forceinline__ void next(const PlaneRun* runs, const int64_t* start, int n_runs) {
-        if (++q == nx + 5) {
-            g += stride;
-            if (valid()) begin(runs, start, n_runs);
-        }
+        if (!step_on()) next_pack(runs, start, n_runs);
     }
 };
 
-struct BProducer {
-    BSeq seq;
-    long long issued;
-    int fenced;  // the last run whose tensor maps this CTA has acquired
-};
-
-__host__ __device__ constexpr size_t batch_smem_bytes(bool xfirst, bool rho) {
-    return (size_t)(DEPTH * buf_floats(YMAX / 2) + (rho ? 2 * stage_floats(YMAX / 2) : 0) +
-                    (xfirst ? 2 * buf_floats(YMAX / 2) : 0)) * 4 +
-           DEPTH * 8 + sizeof(BProducer);
+// body(Step<P>) for P = p0, p0 + 1, ... around the ring until it returns
+// false; the step it stopped at. One copy of each unrolled step: a pack's
+// end leaves the loop instead of being handled inside every step.
+template <typename Body>
+__device__ __forceinline__ int run_steps(Body& body, int p0) {
+    for (;;) {
+        switch (p0) {
+            case 0:
+                if (!body(Step<0>{})) return 0;
+                [[fallthrough]];
+            case 1:
+                if (!body(Step<1>{})) return 1;
+                [[fallthrough]];
+            case 2:
+                if (!body(Step<2>{})) return 2;
+                [[fallthrough]];
+            case 3:
+                if (!body(Step<3>{})) return 3;
+                [[fallthrough]];
+            case 4:
+                if (!body(Step<4>{})) return 4;
+                [[fallthrough]];
+            default:
+                if (!body(Step<5>{})) return 5;
+        }
+        p0 = 0;
+    }
 }
 
-template <bool XFIRST, bool RHO>
-__global__ void __launch_bounds__(YMAX / 2 / YT * 32, 2)
-    k_plane_batch(const PlaneRun* __restrict__ runs, const int64_t* __restrict__ start, int n_runs) {
-    static_assert(!RHO || XFIRST, "the density comes with the x-first order");
-    constexpr int YM = YMAX / 2, BUF = buf_floats(YM), STG = stage_floats(YM);
+struct XBProducer {
+    PSeq seq;
+    int r0[4];  // the current pack's groups: -(x shift) - 3
+    long long issued;  // loads issued (steps)
+};
+
+// the tensor maps of up to XB_MAXR runs as a kernel parameter (16 KB): TMA
+// reads its descriptors from the parameter space, as the single-run kernels
+// do; batches of more runs launch once per XB_MAXR runs
+constexpr int XB_MAXR = 64;
+struct XBMaps {
+    CUtensorMap tin[XB_MAXR];
+    CUtensorMap thalo[XB_MAXR];
+};
+
+__host__ __device__ constexpr size_t xrd_batch_smem_bytes(int slab_rows) {
+    return (size_t)(DEPTH * slab_rows * CG + DSLOTS * XB_SROWS * CG) * 4 + DSLOTS * sizeof(PackMeta) + DEPTH * 8 +
+           sizeof(XBProducer);
+}
+
+template <bool RHO>
+__global__ void __launch_bounds__(XRD_THREADS, 1)
+    k_plane_xrd_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
+                      const int64_t* __restrict__ start, int n_runs, int slab_floats) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    float* slabs = reinterpret_cast<float*>(smem);    // [DEPTH][BUF]
-    float* stage = slabs + DEPTH * BUF;                // [2][STG] (the density's staged rows)
-    float* planes = stage + (RHO ? 2 * STG : 0);       // [2][BUF] (x first)
-    uint64_t* bars = reinterpret_cast<uint64_t*>(planes + (XFIRST ? 2 * BUF : 0));
-    BProducer* prod = reinterpret_cast<BProducer*>(bars + DEPTH);
+    float* slabs = reinterpret_cast<float*>(smem);                 // [DEPTH][slab_floats]
+    float* stage = slabs + DEPTH * slab_floats;                     // [DSLOTS][XB_SROWS][CG], swizzled
+    PackMeta* meta = reinterpret_cast<PackMeta*>(stage + DSLOTS * XB_SROWS * CG);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(meta + DSLOTS);
+    XBProducer* prod = reinterpret_cast<XBProducer*>(bars + DEPTH);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int y0 = warp * YT;
-    BSeq cons;
-    cons.init(runs, start, n_runs, blockIdx.x, gridDim.x);
+    const bool drift = warp < XRD_CW;
+    constexpr int PTID = XRD_CW * 32;  // producer: the first density thread
+    const int dy = tid - PTID;         // density thread: its staged row
+    PSeq cons;
+    cons.init(runs, start, n_runs, (int)blockIdx.x, (int)gridDim.x);
     if (!cons.valid()) return;
     const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
-    auto issue = [&](int d, const BSeq& s) {
-        const PlaneRun* pr = runs + s.r;
-        if (prod->fenced != s.r) {
-            // the run's tensor maps reached global memory by a copy from the host
-            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pr->tin) : "memory");
-            if constexpr (!XFIRST)
-                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&pr->thalo) : "memory");
-            prod->fenced = s.r;
-        }
-        const uint32_t dst = slab0 + (uint32_t)(d * BUF * 4), bar = bar0 + 8 * d;
-        const int rr = s.row() * s.ny;
-        expect_bytes(bar, (uint32_t)((s.ny + (XFIRST ? 0 : HALO)) * CG * 4));
-        tma_load(&pr->tin, dst, bar, s.cg * CG, rr);
-        if constexpr (!XFIRST) tma_load(&pr->thalo, dst + (uint32_t)(s.ny * CG * 4), bar, s.cg * CG, rr);
+    const uint32_t slab_bytes = (uint32_t)slab_floats * 4u;
+    // producer (thread PTID): its sequence and its pack's x-row offsets live in
+    // its registers; across the role split they pass through shared memory
+    XBProducer pr{};
+    auto pack_rows = [&]() {
+        const Args& a = runs[pr.seq.r].a;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < pr.seq.kv) {
+                const int jx = ((pr.seq.cg0 + k) * CG / a.nvy) % a.nvx;
+                pr.r0[k] = -__ldg(a.shift_x + jx) - 3;
+            }
     };
-    if (tid == 0) {
-        prod->fenced = -1;
+    // the loads of the producer's current step into slab d
+    auto issue = [&](int d) {
+        const PSeq& ps = pr.seq;
+        const CUtensorMap* tin = &maps.tin[ps.r];
+        const CUtensorMap* thalo = &maps.thalo[ps.r];
+        const uint32_t box = (uint32_t)((ps.ny + HALO2) * CG * 4), bar = bar0 + 8 * d;
+        expect_bytes(bar, box * (uint32_t)ps.kv);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < ps.kv) {
+                int v = (pr.r0[k] + ps.q) % ps.nx;
+                if (v < 0) v += ps.nx;
+                const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)k * box;
+                tma_load(tin, dst, bar, (ps.cg0 + k) * CG, v * ps.ny);
+                tma_load(thalo, dst + (uint32_t)(ps.ny * CG * 4), bar, (ps.cg0 + k) * CG, v * ps.ny);
+            }
+        pr.issued += 1;
+    };
+    auto advance = [&]() {
+        if (!pr.seq.step_on()) {
+            pr.seq.next_pack(runs, start, n_runs);
+            if (pr.seq.valid()) pack_rows();
+        }
+    };
+    if (tid == PTID) {
         for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        BSeq p = cons;
-        long long n = 0;
-        for (; n < DEPTH && p.valid(); ++n) {
-            issue((int)n, p);
-            p.next(runs, start, n_runs);
+        pr.seq = cons;
+        pr.issued = 0;
+        pack_rows();
+        for (int n = 0; n < DEPTH && pr.seq.valid(); ++n) {
+            issue(n);
+            advance();
         }
-        prod->seq = p;
+        *prod = pr;
+    }
+    if (tid < DSLOTS) meta[tid].valid = 0;
+    __syncthreads();
+
+    uint32_t parity = 0;
+    long long L = 0;
+    bool failed = false, okacc = true;
+    int pp = 0;  // which pair of staging slots the current two rows use
+
+    // density threads: sum the staged rows of slot pair q in FP64 (fixed
+    // order); the run's partials and the thread's (group, row) are cached
+    int c_r = -1, c_ny = -1, c_ncg = 0, kd = 0, yd = 0;
+    double* c_part = nullptr;
+    auto density = [&](int q) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            const int slot = 2 * q + h;
+            const PackMeta m = meta[slot];
+            if (m.valid && dy < m.kv * m.ny) {
+                if (m.r != c_r) {
+                    c_r = m.r;
+                    c_part = runs[m.r].a.part;
+                    c_ncg = runs[m.r].a.n_cg;
+                }
+                if (m.ny != c_ny) {
+                    c_ny = m.ny;
+                    kd = dy / m.ny;
+                    yd = dy - kd * m.ny;
+                }
+                const float4* rw = reinterpret_cast<const float4*>(stage + ((size_t)slot * XB_SROWS + dy) * CG);
+                const int sw = dy & 7;
+                double t[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {  // two halves of 16 columns, each a fixed tree
+                    const float4 u0 = rw[(4 * k) ^ sw], u1 = rw[(4 * k + 1) ^ sw], u2 = rw[(4 * k + 2) ^ sw],
+                                 u3 = rw[(4 * k + 3) ^ sw];
+                    t[k] = ((((double)u0.x + (double)u0.y) + ((double)u0.z + (double)u0.w)) +
+                            (((double)u1.x + (double)u1.y) + ((double)u1.z + (double)u1.w))) +
+                           ((((double)u2.x + (double)u2.y) + ((double)u2.z + (double)u2.w)) +
+                            (((double)u3.x + (double)u3.y) + ((double)u3.z + (double)u3.w)));
+                }
+                c_part[((int64_t)m.x * c_ncg + m.cg0 + kd) * m.ny + yd] = t[0] + t[1];
+            }
+        }
+    };
+
+    // the register budget of each role holds inside its own branch
+    if (drift) {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 216;" ::: "memory");
+        float2 win[WR / 2][6];  // rows 0..19 of the window, in pairs
+        float wl[6];            // row 20
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+#pragma unroll
+            for (int p = 0; p < WR / 2; ++p) win[p][s] = make_float2(0.f, 0.f);
+            wl[s] = 0.f;
+        }
+        float2 wx[6], wy[6];
+        int yoff = 0, y0 = 0, kg = 0, ny = 0;
+        bool act = false;  // this warp has rows of a valid group of the pack
+        float* outp = nullptr;
+        int64_t m = 0;
+        auto tables = [&]() {
+            const Args& a = runs[cons.r].a;
+            ny = cons.ny;
+            const int wpg = (ny + YT2 - 1) / YT2;
+            kg = warp / wpg;
+            y0 = (warp - kg * wpg) * YT2;
+            act = kg < cons.kv;
+            outp = a.out;
+            m = a.m;
+            if (act) {
+                const int cg = cons.cg0 + kg;
+                const int jx = (cg * CG / a.nvy) % a.nvx;
+                const int jy = (cg * CG) % a.nvy + lane;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
+                    wx[j] = make_float2(u, u);
+                    wy[j] = make_float2(v, v);
+                }
+                int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
+                if (r < 0) r += ny;
+                yoff = kg * (ny + HALO2) * CG + r * CG + lane;
+            }
+        };
+        tables();
+
+        auto body = [&](auto step) -> bool {
+            constexpr int P = decltype(step)::value;
+            bool ok = true;
+            const bool emit = cons.q >= 5;
+            const int slot = 2 * pp + (P & 1);
+            const int x = cons.q - 5;
+            if (act) {
+                ok = wait_phase(bar0 + 8 * P, parity);
+                const float* sl = slabs + P * slab_floats + yoff;
+#pragma unroll
+                for (int p = 0; p < WR / 2; ++p) win[p][P] = make_float2(sl[(2 * p) * CG], sl[(2 * p + 1) * CG]);
+                wl[P] = sl[(WR - 1) * CG];
+                if (emit) {
+                    float xd[WR];
+#pragma unroll
+                    for (int p = 0; p < WR / 2; ++p) {
+                        const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                              win[p][(P + 4) % 6], win[p][(P + 5) % 6], win[p][P]);
+                        xd[2 * p] = o.x;
+                        xd[2 * p + 1] = o.y;
+                    }
+                    xd[WR - 1] = tap1(wx, wl[(P + 1) % 6], wl[(P + 2) % 6], wl[(P + 3) % 6], wl[(P + 4) % 6],
+                                      wl[(P + 5) % 6], wl[P]);
+                    float o16[YT2];
+#pragma unroll
+                    for (int p = 0; p < YT2 / 2; ++p) {
+                        const int i = 2 * p;
+                        const float2 o = taps(wy, make_float2(xd[i], xd[i + 1]), make_float2(xd[i + 1], xd[i + 2]),
+                                              make_float2(xd[i + 2], xd[i + 3]), make_float2(xd[i + 3], xd[i + 4]),
+                                              make_float2(xd[i + 4], xd[i + 5]), make_float2(xd[i + 5], xd[i + 6]));
+                        o16[i] = o.x;
+                        o16[i + 1] = o.y;
+                    }
+                    float* dst = outp + ((int64_t)x * ny + y0) * m + (int64_t)(cons.cg0 + kg) * CG + lane;
+                    float* st = stage + ((size_t)slot * XB_SROWS + kg * ny + y0) * CG;
+                    (void)st;
+                    if (y0 + YT2 <= ny) {  // warp-uniform: all 16 rows are real
+#pragma unroll
+                        for (int e = 0; e < YT2; ++e) {
+                            dst[(int64_t)e * m] = o16[e];
+                            if constexpr (RHO) st[e * CG + (lane ^ ((e & 7) << 2))] = o16[e];
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < YT2; ++e)
+                            if (y0 + e < ny) {
+                                dst[(int64_t)e * m] = o16[e];
+                                if constexpr (RHO) st[e * CG + (lane ^ ((e & 7) << 2))] = o16[e];
+                            }
+                    }
+                }
+            }
+            if (tid == 0) {
+                meta[slot] = PackMeta{x, cons.r, cons.cg0, cons.kv, cons.ny, emit ? 1 : 0, 0, 0};
+                if (!(P & 1)) meta[slot + 1].valid = 0;  // a pair may end after one row
+            }
+            okacc = okacc && ok;
+            if (P & 1) {
+                if (__syncthreads_or(!okacc)) {
+                    failed = true;
+                    return false;
+                }
+                pp ^= 1;
+            }
+            if (P == DEPTH - 1) parity ^= 1u;
+            ++L;
+            return cons.step_on();
+        };
+        for (int p0 = 0;;) {
+            const int pe = run_steps(body, p0);
+            if (failed) break;
+            cons.next_pack(runs, start, n_runs);
+            if (!cons.valid()) break;
+            tables();
+            p0 = (pe + 1) % DEPTH;
+        }
+        // a wait on a last, even row has had no barrier vote yet
+        if (!failed && __syncthreads_or(!okacc)) failed = true;
+        if (failed) {
+            // the whole share reads NaN (after this barrier no store of a
+            // row lands any more)
+            __syncthreads();
+            PSeq z;
+            z.init(runs, start, n_runs, (int)blockIdx.x, (int)gridDim.x);
+            while (z.valid()) {
+                const int wpg = (z.ny + YT2 - 1) / YT2;
+                const int zk = warp / wpg, zy0 = (warp - zk * wpg) * YT2;
+                if (z.q >= 5 && zk < z.kv) {
+                    const Args& za = runs[z.r].a;
+                    const int x = z.q - 5;
+                    for (int i = 0; i < YT2 && zy0 + i < z.ny; ++i) {
+                        za.out[((int64_t)x * z.ny + zy0 + i) * za.m + (int64_t)(z.cg0 + zk) * CG + lane] = NAN;
+                        if (RHO && lane == 0)
+                            za.part[((int64_t)x * za.n_cg + z.cg0 + zk) * z.ny + zy0 + i] = (double)NAN;
+                    }
+                }
+                z.next(runs, start, n_runs);
+            }
+        }
+    } else {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 72;" ::: "memory");
+        if (tid == PTID) pr = *prod;
+        // the density warpgroup: the same steps and barriers, no waits
+        auto body = [&](auto step) -> bool {
+            constexpr int P = decltype(step)::value;
+            if (P & 1) {
+                if (__syncthreads_or(0)) {
+                    failed = true;
+                    return false;
+                }
+                if (tid == PTID) {  // slabs P-1 and P are free
+#pragma unroll
+                    for (int d = P - 1; d <= P; ++d)
+                        if (pr.seq.valid()) {
+                            issue(d);
+                            advance();
+                        }
+                }
+                if constexpr (RHO) density(pp);
+                pp ^= 1;
+            }
+            if (P == DEPTH - 1) parity ^= 1u;
+            ++L;
+            return cons.step_on();
+        };
+        for (int p0 = 0;;) {
+            const int pe = run_steps(body, p0);
+            if (failed) break;
+            cons.next_pack(runs, start, n_runs);
+            if (!cons.valid()) break;
+            p0 = (pe + 1) % DEPTH;
+        }
+        // the drift warps' last vote (the same barrier, reached from their branch)
+        if (!failed && __syncthreads_or(0)) failed = true;
+        if constexpr (RHO)
+            if (!failed && (L & 1)) density(pp);  // the last, single row
+        if (failed) {
+            __syncthreads();  // pairs with the drift warps' barrier before their NaN fill
+            if (tid == PTID) {
+                // the loads in flight land before the block leaves
+                for (long long k = L; k < pr.issued; ++k)
+                    wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
+            }
+        }
+    }
+}
+
+// ---- many runs, y then x ---------------------------------------------------
+// The batched y-first pass in the form of k_plane<0>: 8 warps of 8 y rows, each
+// thread's y drift from 13 rows of the slab, then the 6-row x window of
+// y-drifted rows in registers; two CTAs per SM. A CTA steps a pack of K =
+// 8 / ceil(ny / 8) column groups of one run through x together (two groups
+// of up to 32 rows, else one), warp w on group w / wpg, rows 8 (w % wpg) ..
+// +7; each step loads K boxes of ny + 16 rows. The first thread issues the
+// loads, two slabs after every second row's block barrier.
+constexpr int YB_MAX_SLAB_ROWS = 2 * (32 + HALO);
+constexpr int yb_pack(int ny) { return 8 / ((ny + YT - 1) / YT); }
+
+__host__ __device__ constexpr size_t yx_batch_smem_bytes(int slab_rows) {
+    return (size_t)DEPTH * slab_rows * CG * 4 + DEPTH * 8 + sizeof(XBProducer);
+}
+
+__global__ void __launch_bounds__(8 * 32, 2)
+    k_plane_yx_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
+                     const int64_t* __restrict__ start, int n_runs, int slab_floats) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][slab_floats]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(slabs + DEPTH * slab_floats);
+    XBProducer* prod = reinterpret_cast<XBProducer*>(bars + DEPTH);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    PSeq cons;
+    cons.init(runs, start, n_runs, (int)blockIdx.x, (int)gridDim.x);
+    if (!cons.valid()) return;
+    const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
+    const uint32_t slab_bytes = (uint32_t)slab_floats * 4u;
+    auto pack_rows = [&]() {
+        const PSeq& s = prod->seq;
+        const Args& a = runs[s.r].a;
+        for (int k = 0; k < s.kv; ++k) {
+            const int jx = ((s.cg0 + k) * CG / a.nvy) % a.nvx;
+            prod->r0[k] = -__ldg(a.shift_x + jx) - 3;
+        }
+    };
+    auto issue = [&](int d) {
+        const PSeq& s = prod->seq;
+        const CUtensorMap* tin = &maps.tin[s.r];
+        const CUtensorMap* thalo = &maps.thalo[s.r];
+        const uint32_t box = (uint32_t)((s.ny + HALO) * CG * 4), bar = bar0 + 8 * d;
+        expect_bytes(bar, box * (uint32_t)s.kv);
+        for (int k = 0; k < s.kv; ++k) {
+            int v = (prod->r0[k] + s.q) % s.nx;
+            if (v < 0) v += s.nx;
+            const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)k * box;
+            tma_load(tin, dst, bar, (s.cg0 + k) * CG, v * s.ny);
+            tma_load(thalo, dst + (uint32_t)(s.ny * CG * 4), bar, (s.cg0 + k) * CG, v * s.ny);
+        }
+    };
+    auto advance = [&]() {
+        prod->seq.next(runs, start, n_runs);
+        if (prod->seq.valid() && prod->seq.q == 0) pack_rows();
+    };
+    if (tid == 0) {
+        for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        prod->seq = cons;
+        pack_rows();
+        long long n = 0;
+        for (; n < DEPTH && prod->seq.valid(); ++n) {
+            issue((int)n);
+            advance();
+        }
         prod->issued = n;
     }
     __syncthreads();
@@ -1148,215 +1531,116 @@ __global__ void __launch_bounds__(YMAX / 2 / YT * 32, 2)
 #pragma unroll
         for (int s = 0; s < 6; ++s) win[p][s] = make_float2(0.f, 0.f);
     float2 wx[6], wy[6];
-    int yoff = 0, ny = cons.ny, n_cg = 0;
-    float* out = nullptr;
-    double* part = nullptr;
+    int yoff = 0, y0 = 0, kg = 0, ny = 0;
+    bool act = false;
+    float* outp = nullptr;
     int64_t m = 0;
     uint32_t parity = 0;
     long long L = 0;
     bool failed = false, okacc = true;
-    bool pend = false;  // x first: a row waiting for its y drift
-    int pend_x = 0, pend_cg = 0;
-    bool rho_on = false;  // x first: a staged row waiting for its density
-    int rho_x = 0, rho_cg = 0, rho_ny = 0, rho_ncg = 0;
-    double* rho_part = nullptr;
-
-    // the weights, y window and run of the consumer's current group
     auto tables = [&]() {
         const Args& a = runs[cons.r].a;
-        out = a.out;
-        m = a.m;
         ny = cons.ny;
-        part = a.part;
-        n_cg = a.n_cg;
-        const int jx = (int)(((int64_t)cons.cg * CG / a.nvy) % a.nvx);
-        const int jy = (int)(((int64_t)cons.cg * CG) % a.nvy) + lane;
+        const int wpg = (ny + YT - 1) / YT;
+        kg = warp / wpg;
+        y0 = (warp - kg * wpg) * YT;
+        act = kg < cons.kv;
+        outp = a.out;
+        m = a.m;
+        if (act) {
+            const int cg = cons.cg0 + kg;
+            const int jx = (cg * CG / a.nvy) % a.nvx;
+            const int jy = (cg * CG) % a.nvy + lane;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
-            wx[j] = make_float2(u, u);
-            wy[j] = make_float2(v, v);
+            for (int j = 0; j < 6; ++j) {
+                const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
+                wx[j] = make_float2(u, u);
+                wy[j] = make_float2(v, v);
+            }
+            int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
+            if (r < 0) r += ny;
+            yoff = kg * (ny + HALO) * CG + r * CG + lane;
         }
-        int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
-        if (r < 0) r += ny;
-        yoff = r * CG + lane;
     };
     tables();
 
-    // x first: y drift of the pending row from plane PL; stored, and staged
-    // in PL for its density
-    auto y_pending = [&](auto pl) {
-        constexpr int PL = decltype(pl)::value;
-        float2 o[YT / 2];
-        y_drift<false>(planes + PL * BUF + yoff, wy, 0.f, o);
-        if (pend) {
-            float* dst = out + ((int64_t)pend_x * ny + y0) * m + (int64_t)pend_cg * CG + lane;
-#pragma unroll
-            for (int p = 0; p < YT / 2; ++p) {
-                const int y = y0 + 2 * p;
-                if (y < ny) dst[(int64_t)(2 * p) * m] = o[p].x;
-                if (y + 1 < ny) dst[(int64_t)(2 * p + 1) * m] = o[p].y;
-            }
-        }
-        if constexpr (RHO) {
-            float* st = stage + PL * STG;
-#pragma unroll
-            for (int p = 0; p < YT / 2; ++p) {
-                const int y = y0 + 2 * p;
-                if (y < ny) st[y * CG + lane] = o[p].x;
-                if (y + 1 < ny) st[(y + 1) * CG + lane] = o[p].y;
-            }
-        }
-    };
-    // x first: density partials of the row staged in SP (thread: y row
-    // tid / 4, columns 8 (tid % 4) .. + 7; the sums of k_plane's order)
-    const int rrow = tid >> 2, rq = tid & 3;
-    auto rho_row = [&](auto sp) {
-        constexpr int SP = decltype(sp)::value;
-        const float4* src = reinterpret_cast<const float4*>(stage + SP * STG + rrow * CG) + 2 * rq;
-        const int odd = rrow & 1;
-        const float4 u = src[odd], v = src[1 - odd];
-        const double s = (((double)u.x + (double)u.y) + ((double)u.z + (double)u.w)) +
-                         (((double)v.x + (double)v.y) + ((double)v.z + (double)v.w));
-        double t = s + __shfl_xor_sync(0xffffffffu, s, 1);
-        t += __shfl_xor_sync(0xffffffffu, t, 2);
-        if (rho_on && rq == 0 && rrow < rho_ny) rho_part[((int64_t)rho_x * rho_ncg + rho_cg) * rho_ny + rrow] = t;
-    };
-
     auto body = [&](auto step) -> bool {
         constexpr int P = decltype(step)::value;
-        if constexpr (XFIRST) {
-            if constexpr (RHO) rho_row(Step<P & 1>{});
-            y_pending(Step<(P + 1) & 1>{});
-        }
-        const bool ok = wait_phase(bar0 + 8 * P, parity);
-        const bool emit = cons.q >= 5;
-        const float* sl = slabs + P * BUF;
-        float2 nv[YT / 2];
-        if constexpr (XFIRST) {
-            // x drift of the new row into plane P & 1 (read one step later)
+        bool ok = true;
+        if (act) {
+            ok = wait_phase(bar0 + 8 * P, parity);
+            float2 nv[YT / 2];
+            y_drift<false>(slabs + P * slab_floats + yoff, wy, 0.f, nv);
+            if (cons.q >= 5) {
+                float* dst = outp + ((int64_t)(cons.q - 5) * ny + y0) * m + (int64_t)(cons.cg0 + kg) * CG + lane;
+                float2 o[YT / 2];
 #pragma unroll
-            for (int p = 0; p < YT / 2; ++p)
-                nv[p] = make_float2(sl[(y0 + 2 * p) * CG + lane], sl[(y0 + 2 * p + 1) * CG + lane]);
-            float* pl = planes + (P & 1) * BUF;
+                for (int p = 0; p < YT / 2; ++p)
+                    o[p] = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
+                                win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
+                if (y0 + YT <= ny) {  // warp-uniform: all 8 rows are real
 #pragma unroll
-            for (int p = 0; p < YT / 2; ++p) {
-                const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
-                                      win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
-                const int y = y0 + 2 * p;
-                if (y < ny) pl[y * CG + lane] = o.x;
-                if (y + 1 < ny) pl[(y + 1) * CG + lane] = o.y;
-                if (y0 < HALO) {  // warp-uniform: the rows copied after row ny
-                    pl[(ny + y) * CG + lane] = o.x;
-                    pl[(ny + y + 1) * CG + lane] = o.y;
+                    for (int p = 0; p < YT / 2; ++p) {
+                        dst[(int64_t)(2 * p) * m] = o[p].x;
+                        dst[(int64_t)(2 * p + 1) * m] = o[p].y;
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < YT / 2; ++p) {
+                        const int y = y0 + 2 * p;
+                        if (y < ny) dst[(int64_t)(2 * p) * m] = o[p].x;
+                        if (y + 1 < ny) dst[(int64_t)(2 * p + 1) * m] = o[p].y;
+                    }
                 }
             }
-        } else {
-            // y drift of the new row from its slab, then the x drift
-            y_drift<false>(sl + yoff, wy, 0.f, nv);
-            if (emit) {
-                float* dst = out + ((int64_t)(cons.q - 5) * ny + y0) * m + (int64_t)cons.cg * CG + lane;
 #pragma unroll
-                for (int p = 0; p < YT / 2; ++p) {
-                    const float2 o = taps(wx, win[p][(P + 1) % 6], win[p][(P + 2) % 6], win[p][(P + 3) % 6],
-                                          win[p][(P + 4) % 6], win[p][(P + 5) % 6], nv[p]);
-                    const int y = y0 + 2 * p;
-                    if (y < ny) dst[(int64_t)(2 * p) * m] = o.x;
-                    if (y + 1 < ny) dst[(int64_t)(2 * p + 1) * m] = o.y;
-                }
-            }
+            for (int p = 0; p < YT / 2; ++p) win[p][P] = nv[p];
         }
-#pragma unroll
-        for (int p = 0; p < YT / 2; ++p) win[p][P] = nv[p];
         okacc = okacc && ok;
-        if (XFIRST || (P & 1)) {
-            // x first: every row (its plane and staged row change hands);
-            // y first: every second row (slabs P-1 and P are free)
+        if (P & 1) {
+            // slabs P-1 and P are free
             if (__syncthreads_or(!okacc)) {
                 failed = true;
                 return false;
             }
             if (tid == 0) {
-                BSeq& p = prod->seq;
 #pragma unroll
-                for (int d = XFIRST ? P : P - 1; d <= P; ++d)
-                    if (p.valid()) {
-                        issue(d, p);
-                        p.next(runs, start, n_runs);
+                for (int d = P - 1; d <= P; ++d)
+                    if (prod->seq.valid()) {
+                        issue(d);
+                        advance();
                         prod->issued += 1;
                     }
             }
         }
         if (P == DEPTH - 1) parity ^= 1u;
         ++L;
-        if constexpr (XFIRST) {
-            // the row y_pending staged this step belongs to the consumer's run
-            rho_on = pend;
-            rho_x = pend_x;
-            rho_cg = pend_cg;
-            rho_ny = ny;
-            rho_ncg = n_cg;
-            rho_part = part;
-            pend = emit;
-            pend_x = cons.q - 5;
-            pend_cg = cons.cg;
-        }
-        cons.next(runs, start, n_runs);
-        // a new group: its tables after the pending row of the last one went
-        // through (x first: one step into the group; y first: before its first row)
-        if (cons.valid() && cons.q == (XFIRST ? 1 : 0)) tables();
-        return cons.valid();
+        return cons.step_on();
     };
 
-    while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
-           body(Step<5>{})) {
+    for (int p0 = 0;;) {
+        const int pe = run_steps(body, p0);
+        if (failed) break;
+        cons.next_pack(runs, start, n_runs);
+        if (!cons.valid()) break;
+        tables();
+        p0 = (pe + 1) % DEPTH;
     }
-    if constexpr (!XFIRST) {
-        // a wait on a last, even row has had no barrier vote yet
-        if (!failed && __syncthreads_or(!okacc)) failed = true;
-    } else if (!failed) {
-        // the rows still in the pipeline: the density of the row staged at
-        // the last step, then the last row (its plane is complete)
-        const int last = (int)((L - 1) % DEPTH);
-        if constexpr (RHO) {
-            if (last & 1)
-                rho_row(Step<0>{});
-            else
-                rho_row(Step<1>{});
-        }
-        if (pend) {
-            if (last & 1)
-                y_pending(Step<1>{});
-            else
-                y_pending(Step<0>{});
-            if constexpr (RHO) {
-                __syncthreads();
-                rho_on = true;
-                rho_x = pend_x;
-                rho_cg = pend_cg;
-                rho_ny = ny;
-                rho_ncg = n_cg;
-                rho_part = part;
-                if (last & 1)
-                    rho_row(Step<1>{});
-                else
-                    rho_row(Step<0>{});
-            }
-        }
-    }
+    // a wait on a last, even row has had no barrier vote yet
+    if (!failed && __syncthreads_or(!okacc)) failed = true;
     if (failed) {
         // the whole share reads NaN, then the loads in flight land
         __syncthreads();
-        BSeq z;
-        z.init(runs, start, n_runs, blockIdx.x, gridDim.x);
+        PSeq z;
+        z.init(runs, start, n_runs, (int)blockIdx.x, (int)gridDim.x);
         while (z.valid()) {
-            if (z.q >= 5) {
+            const int wpg = (z.ny + YT - 1) / YT;
+            const int zk = warp / wpg, zy0 = (warp - zk * wpg) * YT;
+            if (z.q >= 5 && zk < z.kv) {
                 const Args& za = runs[z.r].a;
                 const int x = z.q - 5;
-                for (int i = 0; i < YT && y0 + i < z.ny; ++i) {
-                    za.out[((int64_t)x * z.ny + y0 + i) * za.m + (int64_t)z.cg * CG + lane] = NAN;
-                    if (RHO && lane == 0) za.part[((int64_t)x * za.n_cg + z.cg) * z.ny + y0 + i] = (double)NAN;
-                }
+                for (int i = 0; i < YT && zy0 + i < z.ny; ++i)
+                    za.out[((int64_t)x * z.ny + zy0 + i) * za.m + (int64_t)(z.cg0 + zk) * CG + lane] = NAN;
             }
             z.next(runs, start, n_runs);
         }
@@ -1465,45 +1749,91 @@ static int launch_xr(const CUtensorMap& tin, const CUtensorMap& thalo, const Arg
     return check_launch("k_plane_xr");
 }
 
-template <bool XFIRST, bool RHO>
-static int launch_batch_t(const PlaneRun* runs, const int64_t* start, int n_runs, int64_t items, cudaStream_t st) {
-    auto kern = k_plane_batch<XFIRST, RHO>;
-    constexpr size_t smem = batch_smem_bytes(XFIRST, RHO);
-    constexpr int block = YMAX / 2 / YT * 32;
+
+// the parameter copies of the runs' tensor maps, launched per XB_MAXR runs
+template <typename Kern>
+static int launch_runs(Kern kern, int block, size_t smem, const PlaneRun* runs, const PlaneRun* runs_host,
+                       const int64_t* start, const int64_t* start_host, int n_runs, int per_sm, int slab_rows,
+                       cudaStream_t st, const char* name) {
+    XBMaps maps;  // host staging of the parameter (the launch copies it)
+    std::memset(static_cast<void*>(&maps), 0, sizeof(maps));
+    const char* hb = reinterpret_cast<const char*>(runs_host);  // the host table need not be 64-byte aligned
+    for (int r0 = 0; r0 < n_runs; r0 += XB_MAXR) {
+        const int nr = std::min(XB_MAXR, n_runs - r0);
+        const int64_t items = start_host[r0 + nr] - start_host[r0];
+        if (items <= 0) continue;
+        for (int i = 0; i < nr; ++i) {
+            const char* rec = hb + (size_t)(r0 + i) * sizeof(PlaneRun);
+            std::memcpy(static_cast<void*>(&maps.tin[i]), rec + offsetof(PlaneRun, tin), sizeof(CUtensorMap));
+            std::memcpy(static_cast<void*>(&maps.thalo[i]), rec + offsetof(PlaneRun, thalo), sizeof(CUtensorMap));
+        }
+        const int64_t grid = std::min<int64_t>(items, (int64_t)sm_count() * per_sm);
+        kern<<<(unsigned)grid, block, smem, st>>>(maps, runs + r0, start + r0, nr, slab_rows * CG);
+        int rc = check_launch(name);
+        if (rc) return rc;
+    }
+    return VP_OK;
+}
+
+static int launch_yx_batch(const PlaneRun* runs, const PlaneRun* runs_host, const int64_t* start,
+                           const int64_t* start_host, int n_runs, int slab_rows, cudaStream_t st) {
+    auto kern = k_plane_yx_batch;
+    const size_t smem = yx_batch_smem_bytes(slab_rows);
     static int raised[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return set_error(VP_ERR_CUDA, "plane batch: device index out of range");
     if (!raised[dev]) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return set_cuda_error("cudaFuncSetAttribute(k_plane_batch)");
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)yx_batch_smem_bytes(YB_MAX_SLAB_ROWS)) != cudaSuccess)
+            return set_cuda_error("cudaFuncSetAttribute(k_plane_yx_batch)");
         raised[dev] = 1;
     }
-    const int occ = occupancy(kern, block, smem);
+    if (slab_rows < 1 || slab_rows > YB_MAX_SLAB_ROWS) return set_error(VP_ERR_ARG, "plane batch: bad slab rows");
+    const int occ = occupancy(kern, 8 * 32, smem);
     if (occ < 1) return set_error(VP_ERR_UNSUPPORTED, "plane batch: the kernel does not fit an SM");
-    const int64_t grid = std::min<int64_t>(items, (int64_t)sm_count() * occ);
-    kern<<<(unsigned)grid, block, smem, st>>>(runs, start, n_runs);
-    return check_launch("k_plane_batch");
+    return launch_runs(kern, 8 * 32, smem, runs, runs_host, start, start_host, n_runs, occ, slab_rows, st,
+                       "k_plane_yx_batch");
+}
+
+template <bool RHO>
+static int launch_xrd_batch_t(const PlaneRun* runs, const PlaneRun* runs_host, const int64_t* start,
+                              const int64_t* start_host, int n_runs, int slab_rows, cudaStream_t st) {
+    auto kern = k_plane_xrd_batch<RHO>;
+    const size_t smem = xrd_batch_smem_bytes(slab_rows);
+    static int raised[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(VP_ERR_CUDA, "plane batch: device index out of range");
+    if (!raised[dev]) {
+        // once, for the largest layout any batch can ask for
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)xrd_batch_smem_bytes(XB_MAX_SLAB_ROWS)) != cudaSuccess)
+            return set_cuda_error("cudaFuncSetAttribute(k_plane_xrd_batch)");
+        raised[dev] = 1;
+    }
+    if (slab_rows < 1 || slab_rows > XB_MAX_SLAB_ROWS) return set_error(VP_ERR_ARG, "plane batch: bad slab rows");
+    return launch_runs(kern, XRD_THREADS, smem, runs, runs_host, start, start_host, n_runs, 1, slab_rows, st,
+                       "k_plane_xrd_batch");
 }
 
 }  // namespace plane
 
 size_t plane_run_bytes() { return sizeof(plane::PlaneRun); }
 
-// Runs of 49..64 rows. Measured on B200 (batches of one run size, FP32): the
-// fused pairs beat the sweeps for 64-row runs (64^4: 1.575 against 1.839 ms a
-// step) but not below (48 rows: 1.740 against 1.584; 16 rows: 2.4x slower):
-// a smaller run's TMA row boxes keep too few bytes in flight in the 6-slab
-// ring, and most of the block's warps have no rows.
+// Runs of 32..64 rows, a multiple of 8 (the packs of the x-first pass stage
+// whole 8-row swizzle blocks). The packed passes take 20..64 rows; below 32
+// they lose to the sweeps (24^4 batches: 1.565 against 1.135 ms a step), the
+// x window's 5 warm-up rows of every line adding a fifth to the loads.
 bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* a, const void* b,
                       const void* c) {
     return plane_fits(dtype, nx, ny, nvx, nvy, a) && plane_fits(dtype, nx, ny, nvx, nvy, b) &&
-           plane_fits(dtype, nx, ny, nvx, nvy, c) && ny > 48 && ny <= plane::YMAX / 2;
+           plane_fits(dtype, nx, ny, nvx, nvy, c) && ny >= 32 && ny <= plane::YMAX / 2 && ny % 8 == 0;
 }
 
-int plane_batch_run(void* record, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy,
-                    const int* shift_x, const void* W_x, const int* shift_y, const void* W_y, double* part,
-                    int64_t* items) {
+int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx,
+                    int64_t nvy, const int* shift_x, const void* W_x, const int* shift_y, const void* W_y,
+                    double* part, int64_t* items, int* slab_rows) {
     using namespace plane;
     // encoded in an aligned local record, then copied into the (host) table
     PlaneRun rec;
@@ -1524,21 +1854,30 @@ int plane_batch_run(void* record, const void* in, void* out, int64_t nx, int64_t
     a.shift_y = shift_y;
     a.W_y = static_cast<const float*>(W_y);
     a.part = part;
-    if (!make_map(&pr->tin, in, a.m, nx * ny, (int)ny) || !make_map(&pr->thalo, in, a.m, nx * ny, HALO))
+    // x first: packs of xb_pack(ny) groups, boxes of ny + 20 rows; y first:
+    // packs of yb_pack(ny) groups, boxes of ny + 16 rows
+    const int halo = xfirst ? HALO2 : HALO;
+    pr->k_pack = xfirst ? xb_pack((int)ny) : yb_pack((int)ny);
+    pr->slab_rows = pr->k_pack * ((int)ny + halo);
+    if (ny < HALO2 || ny % 8 != 0 || pr->slab_rows > (xfirst ? XB_MAX_SLAB_ROWS : YB_MAX_SLAB_ROWS))
+        return set_error(VP_ERR_UNSUPPORTED, "plane batch: rows outside the packed layouts");
+    if (!make_map(&pr->tin, in, a.m, nx * ny, (int)ny) || !make_map(&pr->thalo, in, a.m, nx * ny, halo))
         return set_error(VP_ERR_CUDA, "plane batch: cuTensorMapEncodeTiled failed");
     std::memcpy(record, &rec, sizeof(PlaneRun));
-    *items = a.n_cg;
+    *items = (a.n_cg + pr->k_pack - 1) / pr->k_pack;
+    *slab_rows = pr->slab_rows;
     return VP_OK;
 }
 
-int launch_plane_batch(bool xfirst, bool rho, const void* runs, const int64_t* start, int n_runs, int64_t items,
-                       cudaStream_t st) {
+int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs_host, const int64_t* start,
+                       const int64_t* start_host, int n_runs, int64_t items, int slab_rows, cudaStream_t st) {
     using namespace plane;
     if (items <= 0) return VP_OK;
     const PlaneRun* pr = static_cast<const PlaneRun*>(runs);
-    if (!xfirst) return launch_batch_t<false, false>(pr, start, n_runs, items, st);
-    return rho ? launch_batch_t<true, true>(pr, start, n_runs, items, st)
-               : launch_batch_t<true, false>(pr, start, n_runs, items, st);
+    const PlaneRun* ph = static_cast<const PlaneRun*>(runs_host);
+    if (!xfirst) return launch_yx_batch(pr, ph, start, start_host, n_runs, slab_rows, st);
+    return rho ? launch_xrd_batch_t<true>(pr, ph, start, start_host, n_runs, slab_rows, st)
+               : launch_xrd_batch_t<false>(pr, ph, start, start_host, n_runs, slab_rows, st);
 }
 
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* f) {

@@ -308,9 +308,10 @@ class BatchStepper2D:
     lockstep: vp_batch2d_step launches one kernel per substep for all runs
     (at most 12 launches per step whatever their number) and the state of run
     r is advanced in place in self.f[r]. Each run's step is vp_step2d's: the
-    runs in `fused` (FP32, 48 < Ny <= 64, Nvy a multiple of 32) take their
-    drift pairs as fused passes, bit-identical to a Stepper2D with the fused
-    passes; the others one sweep per axis (fuse_drifts=False: all of them).
+    runs in `fused` (FP32, 32 <= Ny <= 64 a multiple of 8, Nvy a multiple of
+    32) take their drift pairs as fused passes, bit-identical to a Stepper2D
+    with the fused passes; the others one sweep per axis (fuse_drifts=False:
+    all of them).
 
     runs: sequence of dicts with Nx, Ny, Nvx, Nvy, Lx, Ly, Vx_max, Vy_max, dt
     (other keys are ignored). tiles: None (defaults), "auto" (the autotuner's
@@ -345,8 +346,8 @@ class BatchStepper2D:
             shape = (int(p["Nx"]), int(p["Ny"]), int(p["Nvx"]), int(p["Nvy"]))
             self.shapes.append(shape)
         # the rule of vp_batch2d_plan (the arenas keep every buffer 256-byte aligned)
-        self.fused = [self.fuse_drifts and dtype == torch.float32 and 48 < s[1] <= 64 and s[3] % 32 == 0
-                      for s in self.shapes]
+        self.fused = [self.fuse_drifts and dtype == torch.float32 and 32 <= s[1] <= 64 and s[1] % 8 == 0
+                      and s[3] % 32 == 0 for s in self.shapes]
         for p, shape in zip(self.params, self.shapes):
             offs.append(fbytes)
             fbytes += al(esz * shape[0] * shape[1] * shape[2] * shape[3])
