@@ -139,6 +139,15 @@ struct Seq {
             if (valid()) start(a);
         }
     }
+    // the next row of the segment; false at its end (then next_seg)
+    __device__ __forceinline__ bool step_on() { return ++q < n + 5; }
+    __device__ __forceinline__ void next_seg(const Args& a) {
+        if (w < full)
+            ++w;
+        else
+            t += n;
+        if (valid()) start(a);
+    }
 };
 
 // producer state in shared memory (only thread 0 touches it)
@@ -223,6 +232,35 @@ __device__ __forceinline__ float split_bias(double feq, const float2 (&w)[6]) {
 #pragma unroll
     for (int j = 0; j < 6; ++j) s += (double)w[j].x;
     return (float)(feq * s);
+}
+
+// body(Step<P>) for P = p0, p0 + 1, ... around the ring until it returns
+// false; the step it stopped at. One copy of each unrolled step: a pack's
+// end leaves the loop instead of being handled inside every step.
+template <typename Body>
+__device__ __forceinline__ int run_steps(Body& body, int p0) {
+    for (;;) {
+        switch (p0) {
+            case 0:
+                if (!body(Step<0>{})) return 0;
+                [[fallthrough]];
+            case 1:
+                if (!body(Step<1>{})) return 1;
+                [[fallthrough]];
+            case 2:
+                if (!body(Step<2>{})) return 2;
+                [[fallthrough]];
+            case 3:
+                if (!body(Step<3>{})) return 3;
+                [[fallthrough]];
+            case 4:
+                if (!body(Step<4>{})) return 4;
+                [[fallthrough]];
+            default:
+                if (!body(Step<5>{})) return 5;
+        }
+        p0 = 0;
+    }
 }
 
 // y drift of the thread's 8 rows from 13 consecutive rows of a buffer
@@ -958,12 +996,15 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             }
             if (P == DEPTH - 1) parity ^= 1u;
             ++L;
-            cons.next(a);
-            if (__builtin_expect(cons.q == 0, 0) && cons.valid()) tables();
-            return cons.valid();
+            return cons.step_on();
         };
-        while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
-               body(Step<5>{})) {
+        for (int p0 = 0;;) {
+            const int pe = run_steps(body, p0);
+            if (failed) break;
+            cons.next_seg(a);
+            if (!cons.valid()) break;
+            tables();
+            p0 = (pe + 1) % DEPTH;
         }
         // a wait on a last, even row has had no barrier vote yet
         if (!failed && __syncthreads_or(!okacc)) failed = true;
@@ -1009,11 +1050,14 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             }
             if (P == DEPTH - 1) parity ^= 1u;
             ++L;
-            cons.next(a);
-            return cons.valid();
+            return cons.step_on();
         };
-        while (body(Step<0>{}) && body(Step<1>{}) && body(Step<2>{}) && body(Step<3>{}) && body(Step<4>{}) &&
-               body(Step<5>{})) {
+        for (int p0 = 0;;) {
+            const int pe = run_steps(body, p0);
+            if (failed) break;
+            cons.next_seg(a);
+            if (!cons.valid()) break;
+            p0 = (pe + 1) % DEPTH;
         }
         // the drift warps' last vote (the same barrier, reached from their branch)
         if (!failed && __syncthreads_or(0)) failed = true;
@@ -1106,35 +1150,6 @@ struct PSeq {
         if (!step_on()) next_pack(runs, start, n_runs);
     }
 };
-
-// body(Step<P>) for P = p0, p0 + 1, ... around the ring until it returns
-// false; the step it stopped at. One copy of each unrolled step: a pack's
-// end leaves the loop instead of being handled inside every step.
-template <typename Body>
-__device__ __forceinline__ int run_steps(Body& body, int p0) {
-    for (;;) {
-        switch (p0) {
-            case 0:
-                if (!body(Step<0>{})) return 0;
-                [[fallthrough]];
-            case 1:
-                if (!body(Step<1>{})) return 1;
-                [[fallthrough]];
-            case 2:
-                if (!body(Step<2>{})) return 2;
-                [[fallthrough]];
-            case 3:
-                if (!body(Step<3>{})) return 3;
-                [[fallthrough]];
-            case 4:
-                if (!body(Step<4>{})) return 4;
-                [[fallthrough]];
-            default:
-                if (!body(Step<5>{})) return 5;
-        }
-        p0 = 0;
-    }
-}
 
 struct XBProducer {
     PSeq seq;
