@@ -186,7 +186,12 @@ int vp_rho(const void* f, int dtype, int64_t n_points, int64_t n_v, double dvx, 
  * DC and Nyquist bins of the last axis ignored, as torch.fft does).
  * kx: double[nx]; ky: double[ny/2+1]; inv_ksq: double[nx][ny/2+1].
  * Outputs (any may be NULL except ex, ey): ex, ey, drho, phi: double[nx][ny].
- * energy (optional): double[2] = { 1/2 sum(ex^2+ey^2) dx dy, sum(rho) dx dy }. */
+ * energy (optional): double[2] = { 1/2 sum(ex^2+ey^2) dx dy, sum(rho) dx dy }.
+ * Sizes: 1 <= nx, ny <= 4096, and the transforms' shared memory (about
+ * 128 nx bytes for the columns, 64 ny for the inverse rows) within the
+ * 227 KB a block may hold, i.e. nx up to about 1800 and ny up to about
+ * 3600; larger sizes return VP_ERR_UNSUPPORTED (so do vp_step2d and
+ * vp_batch2d_plan in physics mode). */
 int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
                  const double* inv_ksq, double dx, double dy, double* ex, double* ey,
                  double* drho, double* phi, double* energy, void* workspace,

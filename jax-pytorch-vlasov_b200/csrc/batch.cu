@@ -185,6 +185,9 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
                 return set_error(VP_ERR_ARG, "vp_batch2d_plan: run segments must be 0, 1, 2 or 4");
         if (d.nx > 4096 || d.ny > 1024)
             return set_error(VP_ERR_ARG, "vp_batch2d_plan: nx must be <= 4096 and ny <= 1024");
+        if (phys && !poisson2d_fits(d.nx, d.ny))
+            return set_error(VP_ERR_UNSUPPORTED, "vp_batch2d_plan: a run's field solve needs nx below about 1800 "
+                                                 "and ny below about 3600 (shared memory)");
         const size_t need = step2d_layout(d.nx, d.ny, d.nvx, d.nvy, nullptr, nullptr);
         if (!d.workspace || d.workspace_bytes < need)
             return set_error(VP_ERR_WORKSPACE, "vp_batch2d_plan: run workspace too small");

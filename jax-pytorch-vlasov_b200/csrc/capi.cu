@@ -302,6 +302,9 @@ int vp_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, co
                  double* energy, void* workspace, size_t workspace_bytes, void* stream) {
     VP_CHECK(rho && kx && ky && inv_ksq && ex && ey, "vp_poisson2d: null pointer");
     VP_CHECK(nx > 0 && ny > 0 && nx <= 4096 && ny <= 4096, "vp_poisson2d: sizes must be in [1, 4096]");
+    if (!poisson2d_fits(nx, ny))
+        return set_error(VP_ERR_UNSUPPORTED, "vp_poisson2d: the transforms need more shared memory than a block "
+                                             "has (nx above about 1800 or ny above about 3600)");
     if (!workspace || workspace_bytes < poisson2d_ws_bytes(nx, ny))
         return set_error(VP_ERR_WORKSPACE, "vp_poisson2d: workspace too small");
     Pois2dWsView v{};
@@ -370,6 +373,9 @@ int vp_step2d(const vp_step2d_desc* d, void* stream) {
     VP_CHECK(!d->physics_mode || (d->kx && d->ky && d->inv_ksq), "vp_step2d: null spectral arrays");
     VP_CHECK(!d->diagnostics || !d->diag || (d->vx && d->vy), "vp_step2d: diagnostics need vx and vy");
     VP_CHECK(d->dvx != 0.0 && d->dvy != 0.0, "vp_step2d: zero velocity spacing");
+    if (d->physics_mode && !poisson2d_fits(d->nx, d->ny))
+        return set_error(VP_ERR_UNSUPPORTED, "vp_step2d: the field solve's transforms need nx below about 1800 "
+                                             "and ny below about 3600 (shared memory)");
     const size_t need = step2d_layout(d->nx, d->ny, d->nvx, d->nvy, nullptr, nullptr);
     if (!d->workspace || d->workspace_bytes < need) return set_error(VP_ERR_WORKSPACE, "vp_step2d: workspace too small");
     Step2dWs w;

@@ -211,6 +211,8 @@ int run_mlp_sweep(bool train, bool kick, const MlpSweepArgs& args, cudaStream_t 
 
 // poisson.cu
 size_t poisson2d_ws_bytes(int64_t nx, int64_t ny);
+// the 2D solve's transform kernels fit the per-block shared memory
+bool poisson2d_fits(int64_t nx, int64_t ny);
 int run_poisson2d(const double* rho, int64_t nx, int64_t ny, const double* kx, const double* ky,
                   const double* inv_ksq, double* ex, double* ey, double* drho, double* phi, void* ws,
                   Pois2dWsView* view, cudaStream_t st);

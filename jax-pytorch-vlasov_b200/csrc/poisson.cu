@@ -90,6 +90,16 @@ __host__ __device__ constexpr size_t p2_inv_smem(int ny) {
            3 * p2_parts(ny, kPBlock) * sizeof(double);
 }
 
+// the three transform kernels' shared memory against the sm_100 opt-in limit
+// of 227 KB per block (the column transform's grows as 128 nx bytes, the
+// inverse rows' as 64 ny: nx up to about 1800, ny up to about 3600)
+constexpr size_t kSmemOptin = 232448;
+bool poisson2d_fits(int64_t nx, int64_t ny) {
+    if (nx <= 0 || ny <= 0 || nx > 4096 || ny > 4096) return false;
+    return p2_fwd_smem((int)ny) <= kSmemOptin && p2_cols_smem((int)nx) <= kSmemOptin &&
+           p2_inv_smem((int)ny) <= kSmemOptin;
+}
+
 // ---- 2D: rows, forward ------------------------------------------------------
 __device__ __forceinline__ void p2_rows_fwd(const double* __restrict__ rho, int nx, int ny, double* __restrict__ drho,
                                             double2* __restrict__ R, double* __restrict__ mass_part, const int ix,

@@ -88,6 +88,17 @@ def test_argument_errors_without_gpu(lib, vp):
     d.f_out = 0x1000
     assert lib.vp_step2d(ctypes.byref(d), None) == 1  # aliasing buffers
     assert lib.vp_step2d_workspace_bytes(128, 128, 128, 128) > 128 * 128 * 8
+    # a field solve whose column transform would not fit a block's shared memory
+    d.f_out = 0x2000
+    d.nx = 2048
+    assert lib.vp_step2d(ctypes.byref(d), None) == 5 and b"shared memory" in lib.vp_last_error()
+    q = ctypes.c_void_p(0x6000)
+    rc = lib.vp_poisson2d(q, 2048, 16, q, q, q, 0.1, 0.1, q, q, None, None, None, q, 1 << 30, None)
+    assert rc == 5 and b"shared memory" in lib.vp_last_error()
+    rc = lib.vp_poisson2d(q, 16, 4096, q, q, q, 0.1, 0.1, q, q, None, None, None, q, 1 << 30, None)
+    assert rc == 5  # the inverse rows' shared memory: ny above about 3600
+    rc = lib.vp_poisson2d(q, 1024, 2048, q, q, q, 0.1, 0.1, q, q, None, None, None, q, 16, None)
+    assert rc == 3  # within the limits: the (too small) workspace is what fails
 
 
 def _fake_run(L, lib, k, nx=16, ny=16, nvx=32, nvy=32):
