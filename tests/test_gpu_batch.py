@@ -199,3 +199,25 @@ def test_autotune_small_batch(vp, tmp_path):
     torch.cuda.synchronize()
     for r in range(len(RUNS)):
         assert (t.f[r] - a.f[r]).abs().max().item() <= 1e-13 * a.f[r].abs().max().item()
+
+
+def test_batch_beyond_64_runs(vp):
+    """66 runs, fused ones on both sides of the 64-run boundary of the plane
+    passes' parameter chunks: each equals the run stepped alone."""
+    small = dict(Nx=8, Ny=8, Nvx=16, Nvy=16, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=6.0, dt=0.1)
+    big = dict(Nx=32, Ny=32, Nvx=16, Nvy=32, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=5.0, dt=0.1)
+    runs = [dict(big) if r in (1, 64, 65) else dict(small) for r in range(66)]
+    b = vp.BatchStepper2D(runs, dtype=torch.float32, window=-1, diagnostics=1)
+    assert [r for r in range(66) if b.fused[r]] == [1, 64, 65]
+    ref = {}
+    for r, p in enumerate(runs):
+        f0 = _ic(vp, p, r, torch.float32)
+        b.set_state(r, f0)
+        if r in (0, 1, 63, 64, 65):
+            ref[r] = (_single(vp, p, torch.float32, b.fused[r]), f0.clone())
+    for _ in range(2):
+        b.step(0)
+        for r, (st, f) in ref.items():
+            ref[r] = (st, st.step(f))
+            assert torch.equal(b.f[r], ref[r][1]), r
+            assert torch.equal(b.drho[r], st.drho), r
