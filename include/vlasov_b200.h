@@ -393,7 +393,8 @@ typedef struct vp_batch2d_run {
     int32_t shift_spread_y;
     int32_t segments_x;     /* CTAs per x line of this run: 1, 2, 4 (0: the batch's tile shape) */
     int32_t segments_y;     /* CTAs per y line of this run (0: the batch's tile shape) */
-    int32_t reserved;       /* 0 */
+    int32_t test_stall;     /* test hook: 1 makes the first TMA completion wait of each CTA of the fused
+                               passes on this run run out (1 s), as vp_step2d_desc.test_stall; 0 */
     void* f;                /* [nx][ny][nvx][nvy] state, advanced in place */
     void* s1;               /* scratch of the size of f */
     void* s2;               /* scratch of the size of f */
@@ -410,6 +411,9 @@ typedef struct vp_batch2d_run {
     int64_t diag_slot_stride;
     void* workspace;        /* vp_step2d_workspace_bytes(nx, ny, nvx, nvy) bytes */
     size_t workspace_bytes;
+    int32_t* status;        /* optional device int32: VP_STATUS_* bits ORed in for this run (a wait of a
+                               fused pass that ran out: the CTA's share of every run it served, this
+                               one included, is NaN; non-finite diagnostics) */
 } vp_batch2d_run;
 
 /* Tile shapes of the batched sweeps, per sweep kind (0: x drifts, 1: y

@@ -81,12 +81,12 @@ class BatchRun(ctypes.Structure):
         ("nx", I32), ("ny", I32), ("nvx", I32), ("nvy", I32),
         ("dt", D), ("dx", D), ("dy", D), ("dvx", D), ("dvy", D),
         ("window", I32), ("shift_spread_x", I32), ("shift_spread_y", I32), ("segments_x", I32),
-        ("segments_y", I32), ("reserved", I32),
+        ("segments_y", I32), ("test_stall", I32),
         ("f", P), ("s1", P), ("s2", P),
         ("shift_x", P), ("W_x", P), ("shift_y", P), ("W_y", P),
         ("kx", P), ("ky", P), ("inv_ksq", P),
         ("drho", P), ("phi", P), ("diag", P), ("diag_slot_stride", I64),
-        ("workspace", P), ("workspace_bytes", SZ),
+        ("workspace", P), ("workspace_bytes", SZ), ("status", P),
     ]
 
 

@@ -181,6 +181,7 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         if (phys && (!d.kx || !d.ky || !d.inv_ksq))
             return set_error(VP_ERR_ARG, "vp_batch2d_plan: null spectral arrays");
         if (d.dvx == 0.0 || d.dvy == 0.0) return set_error(VP_ERR_ARG, "vp_batch2d_plan: zero velocity spacing");
+        if (d.test_stall != 0 && d.test_stall != 1) return set_error(VP_ERR_ARG, "vp_batch2d_plan: test_stall must be 0 or 1");
         for (int sg : {d.segments_x, d.segments_y})
             if (sg != 0 && sg != 1 && sg != 2 && sg != 4)
                 return set_error(VP_ERR_ARG, "vp_batch2d_plan: run segments must be 0, 1, 2 or 4");
@@ -206,11 +207,11 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
             int rows1 = 0, rows2 = 0;
             int rc = plane_batch_run(static_cast<char*>(table) + L.off_p1 + r * plane_run_bytes(), true, d.f, d.s2, nx,
                                      ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, want_rho ? w.part : nullptr,
-                                     &items1, &rows1);
+                                     d.status, d.test_stall, &items1, &rows1);
             if (!rc)
                 rc = plane_batch_run(static_cast<char*>(table) + L.off_p2 + r * plane_run_bytes(), false,
                                      phys ? d.s1 : d.s2, d.f, nx, ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y,
-                                     nullptr, &items2, &rows2);
+                                     nullptr, d.status, d.test_stall, &items2, &rows2);
             if (rc) return rc;
             slab1 = std::max(slab1, rows1);
             slab2 = std::max(slab2, rows2);
@@ -273,6 +274,7 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
             a.shift_y = d.dt / d.dvy;
             a.diag = d.diag;
             a.slot_stride = d.diag_slot_stride;
+            a.status = d.status;
         }
         h.max_nx = std::max<int32_t>(h.max_nx, d.nx);
         h.max_ny = std::max<int32_t>(h.max_ny, d.ny);

@@ -173,7 +173,7 @@ bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nv
                       const void* c);
 int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx,
                     int64_t nvy, const int* shift_x, const void* W_x, const int* shift_y, const void* W_y,
-                    double* part, int64_t* items, int* slab_rows);
+                    double* part, int* status, int stall, int64_t* items, int* slab_rows);
 // runs_host / start_host: the host copies of the records and prefix sums
 // (the x-first pass takes the runs' tensor maps as a kernel parameter)
 int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs_host, const int64_t* start,

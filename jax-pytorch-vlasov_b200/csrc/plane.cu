@@ -1202,13 +1202,14 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                 pr.r0[k] = -__ldg(a.shift_x + jx) - 3;
             }
     };
-    // the loads of the producer's current step into slab d
-    auto issue = [&](int d) {
+    // the loads of the producer's current step into slab d (extra: the test
+    // hook's 16 bytes too many on the CTA's first load)
+    auto issue = [&](int d, uint32_t extra) {
         const PSeq& ps = pr.seq;
         const CUtensorMap* tin = &maps.tin[ps.r];
         const CUtensorMap* thalo = &maps.thalo[ps.r];
         const uint32_t box = (uint32_t)((ps.ny + HALO2) * CG * 4), bar = bar0 + 8 * d;
-        expect_bytes(bar, box * (uint32_t)ps.kv);
+        expect_bytes(bar, box * (uint32_t)ps.kv + extra);
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (k < ps.kv) {
@@ -1233,7 +1234,7 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
         pr.issued = 0;
         pack_rows();
         for (int n = 0; n < DEPTH && pr.seq.valid(); ++n) {
-            issue(n);
+            issue(n, n == 0 && runs[cons.r].a.stall ? 16u : 0u);
             advance();
         }
         *prod = pr;
@@ -1268,17 +1269,21 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                 }
                 const float4* rw = reinterpret_cast<const float4*>(stage + ((size_t)slot * XB_SROWS + dy) * CG);
                 const int sw = dy & 7;
-                double t[2];
-#pragma unroll
+                double t0 = 0.0, t1 = 0.0;
+#pragma unroll 1
                 for (int k = 0; k < 2; ++k) {  // two halves of 16 columns, each a fixed tree
                     const float4 u0 = rw[(4 * k) ^ sw], u1 = rw[(4 * k + 1) ^ sw], u2 = rw[(4 * k + 2) ^ sw],
                                  u3 = rw[(4 * k + 3) ^ sw];
-                    t[k] = ((((double)u0.x + (double)u0.y) + ((double)u0.z + (double)u0.w)) +
-                            (((double)u1.x + (double)u1.y) + ((double)u1.z + (double)u1.w))) +
-                           ((((double)u2.x + (double)u2.y) + ((double)u2.z + (double)u2.w)) +
-                            (((double)u3.x + (double)u3.y) + ((double)u3.z + (double)u3.w)));
+                    const double h = ((((double)u0.x + (double)u0.y) + ((double)u0.z + (double)u0.w)) +
+                                      (((double)u1.x + (double)u1.y) + ((double)u1.z + (double)u1.w))) +
+                                     ((((double)u2.x + (double)u2.y) + ((double)u2.z + (double)u2.w)) +
+                                      (((double)u3.x + (double)u3.y) + ((double)u3.z + (double)u3.w)));
+                    if (k == 0)
+                        t0 = h;
+                    else
+                        t1 = h;
                 }
-                c_part[((int64_t)m.x * c_ncg + m.cg0 + kd) * m.ny + yd] = t[0] + t[1];
+                c_part[((int64_t)m.x * c_ncg + m.cg0 + kd) * m.ny + yd] = t0 + t1;
             }
         }
     };
@@ -1412,6 +1417,8 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             while (z.valid()) {
                 const int wpg = (z.ny + YT2 - 1) / YT2;
                 const int zk = warp / wpg, zy0 = (warp - zk * wpg) * YT2;
+                if (tid == 0 && z.q == 0 && runs[z.r].a.status)  // every run this CTA served
+                    atomicOr(runs[z.r].a.status, VP_STATUS_WAIT_TIMEOUT);
                 if (z.q >= 5 && zk < z.kv) {
                     const Args& za = runs[z.r].a;
                     const int x = z.q - 5;
@@ -1439,7 +1446,7 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
 #pragma unroll
                     for (int d = P - 1; d <= P; ++d)
                         if (pr.seq.valid()) {
-                            issue(d);
+                            issue(d, 0u);
                             advance();
                         }
                 }
@@ -1508,12 +1515,14 @@ __global__ void __launch_bounds__(8 * 32, 2)
             prod->r0[k] = -__ldg(a.shift_x + jx) - 3;
         }
     };
+    uint32_t extra = 0;  // test hook: the first load of the CTA expects 16 bytes too many
     auto issue = [&](int d) {
         const PSeq& s = prod->seq;
         const CUtensorMap* tin = &maps.tin[s.r];
         const CUtensorMap* thalo = &maps.thalo[s.r];
         const uint32_t box = (uint32_t)((s.ny + HALO) * CG * 4), bar = bar0 + 8 * d;
-        expect_bytes(bar, box * (uint32_t)s.kv);
+        expect_bytes(bar, box * (uint32_t)s.kv + extra);
+        extra = 0;
         for (int k = 0; k < s.kv; ++k) {
             int v = (prod->r0[k] + s.q) % s.nx;
             if (v < 0) v += s.nx;
@@ -1530,6 +1539,7 @@ __global__ void __launch_bounds__(8 * 32, 2)
         for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         prod->seq = cons;
+        extra = runs[cons.r].a.stall ? 16u : 0u;
         pack_rows();
         long long n = 0;
         for (; n < DEPTH && prod->seq.valid(); ++n) {
@@ -1651,6 +1661,8 @@ __global__ void __launch_bounds__(8 * 32, 2)
         while (z.valid()) {
             const int wpg = (z.ny + YT - 1) / YT;
             const int zk = warp / wpg, zy0 = (warp - zk * wpg) * YT;
+            if (tid == 0 && z.q == 0 && runs[z.r].a.status)  // every run this CTA served
+                atomicOr(runs[z.r].a.status, VP_STATUS_WAIT_TIMEOUT);
             if (z.q >= 5 && zk < z.kv) {
                 const Args& za = runs[z.r].a;
                 const int x = z.q - 5;
@@ -1848,7 +1860,7 @@ bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nv
 
 int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx,
                     int64_t nvy, const int* shift_x, const void* W_x, const int* shift_y, const void* W_y,
-                    double* part, int64_t* items, int* slab_rows) {
+                    double* part, int* status, int stall, int64_t* items, int* slab_rows) {
     using namespace plane;
     // encoded in an aligned local record, then copied into the (host) table
     PlaneRun rec;
@@ -1869,6 +1881,8 @@ int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_
     a.shift_y = shift_y;
     a.W_y = static_cast<const float*>(W_y);
     a.part = part;
+    a.status = status;
+    a.stall = stall;
     // x first: packs of xb_pack(ny) groups, boxes of ny + 20 rows; y first:
     // packs of yb_pack(ny) groups, boxes of ny + 16 rows
     const int halo = xfirst ? HALO2 : HALO;

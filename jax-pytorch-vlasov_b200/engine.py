@@ -366,6 +366,8 @@ class BatchStepper2D:
         self._s2 = [view(self._arenas[2], o, s) for o, s in zip(offs, self.shapes)]
         self.slots = max(1, int(graph_slots))
         self.stage = torch.zeros((self.slots, n, L.DIAG_COUNT), dtype=torch.float64, device=self.device)
+        # per-run device status words the steps OR VP_STATUS_* bits into (read by check())
+        self.status = torch.zeros(n, dtype=torch.int32, device=self.device)
         self.drho, self.phi, self.tables = [], [], []
         runs_c = (L.BatchRun * n)()
         for r, (p, shape) in enumerate(zip(self.params, self.shapes)):
@@ -397,6 +399,7 @@ class BatchStepper2D:
             c.diag_slot_stride = n * L.DIAG_COUNT
             c.workspace = self._ws.data_ptr() + wsoffs[r]
             c.workspace_bytes = L.query("vp_step2d_workspace_bytes", *shape)
+            c.status = self.status[r].data_ptr()
         self.dx = [c.dx for c in runs_c]
         self.dy = [c.dy for c in runs_c]
         self.dvx = [c.dvx for c in runs_c]
@@ -437,6 +440,30 @@ class BatchStepper2D:
         self._table_dev = host.to(self.device)
         self.tiles = tiles
         self._graphs = {}
+
+    def check(self) -> None:
+        """Synchronise with the steps issued so far and raise VlasovError if
+        a run reported a device wait that ran out (a fused pass's CTA filled
+        its share of f with NaN, on every run it served) or non-finite
+        diagnostics; the status words are cleared either way."""
+        bits = self.status.cpu()
+        if bool(bits.any()):
+            self.status.zero_()
+            wait = [r for r in range(self.n_runs) if int(bits[r]) & L.STATUS_WAIT_TIMEOUT]
+            bad = [r for r in range(self.n_runs) if int(bits[r]) & L.STATUS_NONFINITE]
+            what = []
+            if wait:
+                what.append(f"a device wait ran out on runs {wait} (the affected parts of f are NaN)")
+            if bad:
+                what.append(f"non-finite field energy or mass on runs {bad}")
+            raise L.VlasovError("BatchStepper2D: " + "; ".join(what))
+
+    def set_test_stall(self, r: int, on: bool = True) -> None:
+        """Test hook: make the first TMA wait of each CTA of the fused passes
+        that starts on run r run out (1 s bound) in the following steps; re-plans
+        the batch."""
+        self._runs_c[r].test_stall = 1 if on else 0
+        self.retile(self.tiles)
 
     def phase_ms(self, steps: int = 3):
         """Mean per-substep device times (ms) of `steps` eager steps, keyed by

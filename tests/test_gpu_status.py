@@ -54,3 +54,36 @@ def test_nonfinite_diagnostics_are_reported(vp, kind, shape):
     assert int(st.status.item()) & vp._lib.STATUS_NONFINITE
     with pytest.raises(vp._lib.VlasovError, match="non-finite"):
         st.check()
+
+
+def test_batch_wait_timeout_is_reported_per_run(vp):
+    """The batched fused passes: the test hook on run 0 makes the first wait
+    of the CTAs that start on it run out; run 0 reports it and reads NaN, the
+    other runs step normally, and after the hook is cleared the batch steps
+    as a fresh one."""
+    base = dict(Nx=8, Ny=32, Nvx=2, Nvy=32, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=6.0, dt=0.1)
+    runs = [dict(base), dict(base), dict(base, Ny=16)]
+    b = vp.BatchStepper2D(runs, dtype=torch.float32, window=-1, diagnostics=1)
+    assert b.fused == [True, True, False]
+    f0 = [seeded((p["Nx"], p["Ny"], p["Nvx"], p["Nvy"]), 7 + r) for r, p in enumerate(runs)]
+    for r in range(3):
+        b.set_state(r, f0[r])
+    b.set_test_stall(0)
+    b.step(0)
+    torch.cuda.synchronize()
+    bits = b.status.cpu().tolist()
+    assert bits[0] & vp._lib.STATUS_WAIT_TIMEOUT and not bits[1] & vp._lib.STATUS_WAIT_TIMEOUT and bits[2] == 0
+    assert torch.isnan(b.f[0]).any() and torch.isfinite(b.f[1]).all() and torch.isfinite(b.f[2]).all()
+    with pytest.raises(vp._lib.VlasovError, match=r"device wait ran out on runs \[0\]"):
+        b.check()
+    assert int(b.status.abs().sum()) == 0
+    b.set_test_stall(0, False)
+    fresh = vp.BatchStepper2D(runs, dtype=torch.float32, window=-1, diagnostics=1)
+    for r in range(3):
+        b.set_state(r, f0[r])
+        fresh.set_state(r, f0[r])
+    b.step(0)
+    fresh.step(0)
+    b.check()
+    for r in range(3):
+        assert torch.equal(b.f[r], fresh.f[r]), r
