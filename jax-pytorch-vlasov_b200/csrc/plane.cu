@@ -1269,21 +1269,17 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                 }
                 const float4* rw = reinterpret_cast<const float4*>(stage + ((size_t)slot * XB_SROWS + dy) * CG);
                 const int sw = dy & 7;
-                double t0 = 0.0, t1 = 0.0;
-#pragma unroll 1
+                double t[2];
+#pragma unroll
                 for (int k = 0; k < 2; ++k) {  // two halves of 16 columns, each a fixed tree
                     const float4 u0 = rw[(4 * k) ^ sw], u1 = rw[(4 * k + 1) ^ sw], u2 = rw[(4 * k + 2) ^ sw],
                                  u3 = rw[(4 * k + 3) ^ sw];
-                    const double h = ((((double)u0.x + (double)u0.y) + ((double)u0.z + (double)u0.w)) +
-                                      (((double)u1.x + (double)u1.y) + ((double)u1.z + (double)u1.w))) +
-                                     ((((double)u2.x + (double)u2.y) + ((double)u2.z + (double)u2.w)) +
-                                      (((double)u3.x + (double)u3.y) + ((double)u3.z + (double)u3.w)));
-                    if (k == 0)
-                        t0 = h;
-                    else
-                        t1 = h;
+                    t[k] = ((((double)u0.x + (double)u0.y) + ((double)u0.z + (double)u0.w)) +
+                            (((double)u1.x + (double)u1.y) + ((double)u1.z + (double)u1.w))) +
+                           ((((double)u2.x + (double)u2.y) + ((double)u2.z + (double)u2.w)) +
+                            (((double)u3.x + (double)u3.y) + ((double)u3.z + (double)u3.w)));
                 }
-                c_part[((int64_t)m.x * c_ncg + m.cg0 + kd) * m.ny + yd] = t0 + t1;
+                c_part[((int64_t)m.x * c_ncg + m.cg0 + kd) * m.ny + yd] = t[0] + t[1];
             }
         }
     };
