@@ -50,7 +50,8 @@ struct BatchHeader {
     int64_t off_rfin;  // RhoFinRun[n]
     int64_t off_diag;  // DiagArgs[n]
     int64_t off_p1, off_p2;    // plane-pass records (x then y, y then x), 64-byte aligned
-    int64_t off_sp1, off_sp2;  // int64[n+1]: prefix sums of the two passes' plane items
+    int32_t n_plane, pad0;     // fused runs: records 0 .. n_plane - 1, longest lines first
+    int64_t off_sp1, off_sp2;  // int64[n+1]: prefix sums of the two passes' plane items over the records
     int64_t plane_items1, plane_items2;  // all runs' plane items (0: no fused runs)
     int32_t p1_slab_rows, p2_slab_rows;  // the largest ring slab of the fused runs
     int64_t sweep_items;     // all runs' x-drift items (0: every run fused)
@@ -202,22 +203,6 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         // the fused drift pairs: f -> s2 (x then y, the rho partials), then
         // s1 -> f (after the kick) or s2 -> f (without it)
         fused[r] = !sweeps_only && plane_batch_fits(dtype, nx, ny, nvx, nvy, d.f, d.s1, d.s2);
-        int64_t items1 = 0, items2 = 0;
-        if (fused[r]) {
-            int rows1 = 0, rows2 = 0;
-            int rc = plane_batch_run(static_cast<char*>(table) + L.off_p1 + r * plane_run_bytes(), true, d.f, d.s2, nx,
-                                     ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y, want_rho ? w.part : nullptr,
-                                     d.status, d.test_stall, &items1, &rows1);
-            if (!rc)
-                rc = plane_batch_run(static_cast<char*>(table) + L.off_p2 + r * plane_run_bytes(), false,
-                                     phys ? d.s1 : d.s2, d.f, nx, ny, nvx, nvy, d.shift_x, d.W_x, d.shift_y, d.W_y,
-                                     nullptr, d.status, d.test_stall, &items2, &rows2);
-            if (rc) return rc;
-            slab1 = std::max(slab1, rows1);
-            slab2 = std::max(slab2, rows2);
-        }
-        sp1[r + 1] = sp1[r] + items1;
-        sp2[r + 1] = sp2[r] + items2;
         int v, nt;
         // x drifts: f -> s1 and s2 -> f (with the kicks) or s1 -> f (without)
         strided_batch_args(dtype, d.f, d.s1, 1, nx, ny * nvx * nvy, nvy, nvx, d.shift_spread_x, d.shift_x, d.W_x,
@@ -335,13 +320,42 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
             sk[r + 1] = sk[r];
         }
     }
+    // the fused runs' plane records, longest lines first: a CTA takes the
+    // packs b, b + G, ... of the launch in record order, so that each round
+    // deals packs of about one length (C4: the longest CTA share 387 row
+    // steps against 435 in run order, 346 the even share)
+    std::vector<int> order;
+    for (int r = 0; r < n_runs; ++r)
+        if (fused[r]) order.push_back(r);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return runs[a].nx > runs[b].nx; });
+    for (size_t i = 0; i < order.size(); ++i) {
+        const int r = order[i];
+        const vp_batch2d_run& d = runs[r];
+        Step2dWs w;
+        step2d_layout(d.nx, d.ny, d.nvx, d.nvy, static_cast<char*>(d.workspace), &w);
+        int64_t items1 = 0, items2 = 0;
+        int rows1 = 0, rows2 = 0;
+        int rc = plane_batch_run(static_cast<char*>(table) + L.off_p1 + i * plane_run_bytes(), true, d.f, d.s2, d.nx,
+                                 d.ny, d.nvx, d.nvy, d.shift_x, d.W_x, d.shift_y, d.W_y,
+                                 (phys || diagnostics) ? w.part : nullptr, d.status, d.test_stall, &items1, &rows1);
+        if (!rc)
+            rc = plane_batch_run(static_cast<char*>(table) + L.off_p2 + i * plane_run_bytes(), false,
+                                 phys ? d.s1 : d.s2, d.f, d.nx, d.ny, d.nvx, d.nvy, d.shift_x, d.W_x, d.shift_y,
+                                 d.W_y, nullptr, d.status, d.test_stall, &items2, &rows2);
+        if (rc) return rc;
+        slab1 = std::max(slab1, rows1);
+        slab2 = std::max(slab2, rows2);
+        sp1[i + 1] = sp1[i] + items1;
+        sp2[i + 1] = sp2[i] + items2;
+    }
+    h.n_plane = (int32_t)order.size();
     for (int k = 0; k < VP_BATCH_KINDS; ++k) h.block[k] = block[k];
     h.grid[0] = grid_for(per_sm[0], sx[n_runs]);
     h.grid[1] = grid_for(per_sm[1], std::max(sy1[n_runs], sy2[n_runs]));
     h.grid[2] = grid_for(per_sm[2], std::max<int64_t>(sk[n_runs], 1));
     h.kick_smem = kick_smem;
-    h.plane_items1 = sp1[n_runs];
-    h.plane_items2 = sp2[n_runs];
+    h.plane_items1 = sp1[h.n_plane];
+    h.plane_items2 = sp2[h.n_plane];
     h.p1_slab_rows = slab1;
     h.p2_slab_rows = slab2;
     h.sweep_items = sx[n_runs];
@@ -393,7 +407,7 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     // the others: x drift (dt/2), f -> s1
     if ((rc = mark(2 * VP_PHASE_DRIFT_X1))) return rc;
     rc = launch_plane_batch(true, want_rho, at<char>(table_dev, h.off_p1), at<char>(table, h.off_p1), sp1,
-                            at<int64_t>(table, h.off_sp1), n, h.plane_items1, h.p1_slab_rows, st);
+                            at<int64_t>(table, h.off_sp1), h.n_plane, h.plane_items1, h.p1_slab_rows, st);
     if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x1), sx,
@@ -432,7 +446,7 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     if ((rc = mark(2 * VP_PHASE_DRIFT_Y2 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_X2))) return rc;
     // the fused runs: y then x back into f; the others: x drift back into f
     rc = launch_plane_batch(false, false, at<char>(table_dev, h.off_p2), at<char>(table, h.off_p2), sp2,
-                            at<int64_t>(table, h.off_sp2), n, h.plane_items2, h.p2_slab_rows, st);
+                            at<int64_t>(table, h.off_sp2), h.n_plane, h.plane_items2, h.p2_slab_rows, st);
     if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x2), sx,
