@@ -1190,8 +1190,12 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
     if (!cons.valid()) return;
     const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
     const uint32_t slab_bytes = (uint32_t)slab_floats * 4u;
-    // producer (thread PTID): its sequence and its pack's x-row offsets live in
-    // its registers; across the role split they pass through shared memory
+    // producers: thread PTID issues the first DEPTH steps; then the first lane
+    // of density warp k issues group k's loads of every step (a step's 2K TMA
+    // operations on one thread had put that thread's warp on the path to each
+    // barrier). Each keeps its copy of the sequence and of its groups' x-row
+    // offsets in registers; across the role split they pass through shared
+    // memory.
     XBProducer pr{};
     auto pack_rows = [&]() {
         const Args& a = runs[pr.seq.r].a;
@@ -1202,8 +1206,11 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                 pr.r0[k] = -__ldg(a.shift_x + jx) - 3;
             }
     };
-    // the loads of the producer's current step into slab d (extra: the test
-    // hook's 16 bytes too many on the CTA's first load)
+    // the loads of groups k0 .. k1 - 1 of the sequence's current step into
+    // slab d; group 0's issuer arms the barrier with the step's bytes (extra:
+    // the test hook's 16 bytes too many on the CTA's first load). Loads that
+    // complete before the arming leave the barrier's byte count negative for
+    // a while; the phase cannot complete before its one arrival.
     auto issue = [&](int d, uint32_t extra) {
         const PSeq& ps = pr.seq;
         const CUtensorMap* tin = &maps.tin[ps.r];
@@ -1429,7 +1436,35 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
         }
     } else {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 72;" ::: "memory");
-        if (tid == PTID) pr = *prod;
+        const bool issuer = (dy & 31) == 0;  // first lane of density warp kq issues group kq
+        const int kq = dy >> 5;
+        PSeq qs{};     // the issuer's copy of the sequence
+        int q_r0 = 0;  // its group's -(x shift) - 3
+        long long q_issued = 0;
+        if (issuer) {
+            qs = prod->seq;
+            q_r0 = kq < 4 ? prod->r0[kq] : 0;
+            q_issued = prod->issued;
+        }
+        auto issue_q = [&](int d) {
+            const uint32_t box = (uint32_t)((qs.ny + HALO2) * CG * 4), bar = bar0 + 8 * d;
+            if (kq == 0) expect_bytes(bar, box * (uint32_t)qs.kv);
+            if (kq < qs.kv) {
+                int v = (q_r0 + qs.q) % qs.nx;
+                if (v < 0) v += qs.nx;
+                const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)kq * box;
+                tma_load(&maps.tin[qs.r], dst, bar, (qs.cg0 + kq) * CG, v * qs.ny);
+                tma_load(&maps.thalo[qs.r], dst + (uint32_t)(qs.ny * CG * 4), bar, (qs.cg0 + kq) * CG, v * qs.ny);
+            }
+            q_issued += 1;
+            if (!qs.step_on()) {
+                qs.next_pack(runs, start, n_runs);
+                if (qs.valid() && kq < qs.kv) {
+                    const Args& a = runs[qs.r].a;
+                    q_r0 = -__ldg(a.shift_x + ((qs.cg0 + kq) * CG / a.nvy) % a.nvx) - 3;
+                }
+            }
+        };
         // the density warpgroup: the same steps and barriers, no waits
         auto body = [&](auto step) -> bool {
             constexpr int P = decltype(step)::value;
@@ -1438,13 +1473,10 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                     failed = true;
                     return false;
                 }
-                if (tid == PTID) {  // slabs P-1 and P are free
+                if (issuer) {  // slabs P-1 and P are free
 #pragma unroll
                     for (int d = P - 1; d <= P; ++d)
-                        if (pr.seq.valid()) {
-                            issue(d, 0u);
-                            advance();
-                        }
+                        if (qs.valid()) issue_q(d);
                 }
                 if constexpr (RHO) density(pp);
                 pp ^= 1;
@@ -1468,7 +1500,7 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             __syncthreads();  // pairs with the drift warps' barrier before their NaN fill
             if (tid == PTID) {
                 // the loads in flight land before the block leaves
-                for (long long k = L; k < pr.issued; ++k)
+                for (long long k = L; k < q_issued; ++k)
                     wait_phase(bar0 + 8 * (int)(k % DEPTH), (uint32_t)((k / DEPTH) & 1));
             }
         }
