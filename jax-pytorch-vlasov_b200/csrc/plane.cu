@@ -1519,7 +1519,7 @@ constexpr int YB_MAX_SLAB_ROWS = 2 * (32 + HALO);
 constexpr int yb_pack(int ny) { return 8 / ((ny + YT - 1) / YT); }
 
 __host__ __device__ constexpr size_t yx_batch_smem_bytes(int slab_rows) {
-    return (size_t)DEPTH * slab_rows * CG * 4 + DEPTH * 8 + sizeof(XBProducer);
+    return (size_t)DEPTH * slab_rows * CG * 4 + DEPTH * 8 + 2 * sizeof(XBProducer);
 }
 
 __global__ void __launch_bounds__(8 * 32, 2)
@@ -1528,7 +1528,7 @@ __global__ void __launch_bounds__(8 * 32, 2)
     extern __shared__ __align__(1024) unsigned char smem[];
     float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][slab_floats]
     uint64_t* bars = reinterpret_cast<uint64_t*>(slabs + DEPTH * slab_floats);
-    XBProducer* prod = reinterpret_cast<XBProducer*>(bars + DEPTH);
+    XBProducer* prod = reinterpret_cast<XBProducer*>(bars + DEPTH);  // [2]: one per issuer
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     PSeq cons;
     cons.init(runs, start, n_runs, (int)blockIdx.x, (int)gridDim.x);
@@ -1563,6 +1563,31 @@ __global__ void __launch_bounds__(8 * 32, 2)
         prod->seq.next(runs, start, n_runs);
         if (prod->seq.valid() && prod->seq.q == 0) pack_rows();
     };
+    // after the first DEPTH steps: the first lane of warp 7 - k issues group
+    // k's loads (k < 2), warp 7's arming the barrier with the step's bytes;
+    // each issuer steps its own copy of the sequence (in shared memory). One
+    // thread issuing a step's four loads had put its warp on the path to
+    // every second row's barrier.
+    auto issue_q = [&](XBProducer& q, int kq, int d) {
+        const PSeq& qs = q.seq;
+        const uint32_t box = (uint32_t)((qs.ny + HALO) * CG * 4), bar = bar0 + 8 * d;
+        if (kq == 0) expect_bytes(bar, box * (uint32_t)qs.kv);
+        if (kq < qs.kv) {
+            int v = (q.r0[kq] + qs.q) % qs.nx;
+            if (v < 0) v += qs.nx;
+            const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)kq * box;
+            tma_load(&maps.tin[qs.r], dst, bar, (qs.cg0 + kq) * CG, v * qs.ny);
+            tma_load(&maps.thalo[qs.r], dst + (uint32_t)(qs.ny * CG * 4), bar, (qs.cg0 + kq) * CG, v * qs.ny);
+        }
+        q.issued += 1;
+        if (!q.seq.step_on()) {
+            q.seq.next_pack(runs, start, n_runs);
+            if (q.seq.valid() && kq < q.seq.kv) {
+                const Args& a = runs[q.seq.r].a;
+                q.r0[kq] = -__ldg(a.shift_x + ((q.seq.cg0 + kq) * CG / a.nvy) % a.nvx) - 3;
+            }
+        }
+    };
     if (tid == 0) {
         for (int d = 0; d < DEPTH; ++d) bar_init(bar0 + 8 * d);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1575,6 +1600,7 @@ __global__ void __launch_bounds__(8 * 32, 2)
             advance();
         }
         prod->issued = n;
+        prod[1] = prod[0];
     }
     __syncthreads();
 
@@ -1656,14 +1682,12 @@ __global__ void __launch_bounds__(8 * 32, 2)
                 failed = true;
                 return false;
             }
-            if (tid == 0) {
+            if (lane == 0 && warp >= 6) {
+                const int kq = 7 - warp;
+                XBProducer& q = prod[kq];
 #pragma unroll
                 for (int d = P - 1; d <= P; ++d)
-                    if (prod->seq.valid()) {
-                        issue(d);
-                        advance();
-                        prod->issued += 1;
-                    }
+                    if (q.seq.valid()) issue_q(q, kq, d);
             }
         }
         if (P == DEPTH - 1) parity ^= 1u;
