@@ -50,7 +50,8 @@ struct BatchHeader {
     int64_t off_rfin;  // RhoFinRun[n]
     int64_t off_diag;  // DiagArgs[n]
     int64_t off_p1, off_p2;    // plane-pass records (x then y, y then x), 64-byte aligned
-    int32_t n_plane, pad0;     // fused runs: records 0 .. n_plane - 1, longest lines first
+    int32_t n_plane, n_plane_full;  // fused runs: records 0 .. n_plane - 1, whole-box ones first,
+                                    // longest lines first in each class
     int64_t off_sp1, off_sp2;  // int64[n+1]: prefix sums of the two passes' plane items over the records
     int64_t plane_items1, plane_items2;  // all runs' plane items (0: no fused runs)
     int32_t p1_slab_rows, p2_slab_rows;  // the largest ring slab of the fused runs
@@ -327,7 +328,13 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
     std::vector<int> order;
     for (int r = 0; r < n_runs; ++r)
         if (fused[r]) order.push_back(r);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return runs[a].nx > runs[b].nx; });
+    // runs with nvy % 32 == 0 first (whole-box launch), then the others (half boxes)
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const bool ha = runs[a].nvy % 32 != 0, hb = runs[b].nvy % 32 != 0;
+        return ha != hb ? !ha : runs[a].nx > runs[b].nx;
+    });
+    int n_full = 0;
+    for (int r : order) n_full += runs[r].nvy % 32 == 0 ? 1 : 0;
     for (size_t i = 0; i < order.size(); ++i) {
         const int r = order[i];
         const vp_batch2d_run& d = runs[r];
@@ -349,6 +356,7 @@ int vp_batch2d_plan(int32_t dtype, int32_t physics_mode, int32_t diagnostics, co
         sp2[i + 1] = sp2[i] + items2;
     }
     h.n_plane = (int32_t)order.size();
+    h.n_plane_full = n_full;
     for (int k = 0; k < VP_BATCH_KINDS; ++k) h.block[k] = block[k];
     h.grid[0] = grid_for(per_sm[0], sx[n_runs]);
     h.grid[1] = grid_for(per_sm[1], std::max(sy1[n_runs], sy2[n_runs]));
@@ -407,7 +415,8 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     // the others: x drift (dt/2), f -> s1
     if ((rc = mark(2 * VP_PHASE_DRIFT_X1))) return rc;
     rc = launch_plane_batch(true, want_rho, at<char>(table_dev, h.off_p1), at<char>(table, h.off_p1), sp1,
-                            at<int64_t>(table, h.off_sp1), h.n_plane, h.plane_items1, h.p1_slab_rows, st);
+                            at<int64_t>(table, h.off_sp1), h.n_plane_full, h.n_plane, h.plane_items1, h.p1_slab_rows,
+                            st);
     if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x1), sx,
@@ -446,7 +455,8 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     if ((rc = mark(2 * VP_PHASE_DRIFT_Y2 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_X2))) return rc;
     // the fused runs: y then x back into f; the others: x drift back into f
     rc = launch_plane_batch(false, false, at<char>(table_dev, h.off_p2), at<char>(table, h.off_p2), sp2,
-                            at<int64_t>(table, h.off_sp2), h.n_plane, h.plane_items2, h.p2_slab_rows, st);
+                            at<int64_t>(table, h.off_sp2), h.n_plane_full, h.n_plane, h.plane_items2, h.p2_slab_rows,
+                            st);
     if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x2), sx,

@@ -176,8 +176,11 @@ int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_
                     double* part, int* status, int stall, int64_t* items, int* slab_rows);
 // runs_host / start_host: the host copies of the records and prefix sums
 // (the x-first pass takes the runs' tensor maps as a kernel parameter)
+// records 0 .. n_full - 1 hold runs with nvy % 32 == 0 (whole 32-column TMA
+// boxes), the rest runs whose groups come in half boxes of 16 (one launch each)
 int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs_host, const int64_t* start,
-                       const int64_t* start_host, int n_runs, int64_t items, int slab_rows, cudaStream_t st);
+                       const int64_t* start_host, int n_full, int n_runs, int64_t items, int slab_rows,
+                       cudaStream_t st);
 int run_kick_contig(int dtype, const void* in, void* out, int64_t n_rows, int64_t n, const void* E, int e_f64,
                     int64_t e_div, double dt, double dv, int window, const EqSplit* eq, cudaStream_t st);
 int run_gather(int dtype, const void* in, void* out, int64_t n_outer, int64_t n, int64_t n_inner, const void* vel,

@@ -265,11 +265,11 @@ __device__ __forceinline__ int run_steps(Body& body, int p0) {
 
 // y drift of the thread's 8 rows from 13 consecutive rows of a buffer
 // (g: row y0 - s - 3 of the lane's column, halo included)
-template <bool EQ>
+template <bool EQ, int RS = CG>
 __device__ __forceinline__ void y_drift(const float* g, const float2 (&wy)[6], float by, float2 (&o)[YT / 2]) {
     float r[YT + 5];
 #pragma unroll
-    for (int k = 0; k < YT + 5; ++k) r[k] = g[k * CG];
+    for (int k = 0; k < YT + 5; ++k) r[k] = g[k * RS];
 #pragma unroll
     for (int p = 0; p < YT / 2; ++p) {
         const int i = 2 * p;
@@ -1095,9 +1095,10 @@ struct alignas(64) PlaneRun {
 };
 
 // ---- many runs, x then y, register window ---------------------------------
-// The batched x-first pass in the form of k_plane_xrd: 8 drift warps of 16 y
-// rows with the 21-row x window in registers, and a warpgroup of 4 density
-// warps (the FP64 row sums of the staged output, one thread a row, in
+// The batched x-first pass in the form of k_plane_xrd (setmaxnreg 216 / 72,
+// 208 / 88 with half boxes: the issuers' second x row): 8 drift
+// warps of 16 y rows with the 21-row x window in registers, and a warpgroup
+// of 4 density warps (the FP64 row sums of the staged output, one thread a row, in
 // k_plane_xrd's order; its first thread issues the TMA loads). A CTA steps a
 // pack of K column groups of one run through x together, K = 8 / ceil(ny /
 // 16) (two groups of up to 64 rows, four of up to 32): warp w works on group
@@ -1109,6 +1110,11 @@ struct alignas(64) PlaneRun {
 // element takes k_plane_xrd's FMA chains and every density partial its sum
 // order, so f and rho are bit-identical to the run stepped alone.
 constexpr int XB_SROWS = 128;  // staged rows per slot
+// columns per TMA box of the packed x-first pass: a group of 32 columns comes
+// in as two boxes of 16 (each at the x row of its own vx, so that groups
+// which span two vx of a run with nvy % 32 != 0 work too); in shared memory a
+// group is [half][ny + 20][16]
+constexpr int HB = 16;
 // packs per ny: up to 32 rows four groups of ny + 20 rows, up to 64 two
 constexpr int xb_pack(int ny) { return XRD_CW / ((ny + YT2 - 1) / YT2); }
 constexpr int XB_MAX_SLAB_ROWS = 4 * (32 + HALO2);
@@ -1153,7 +1159,7 @@ struct PSeq {
 
 struct XBProducer {
     PSeq seq;
-    int r0[4];  // the current pack's groups: -(x shift) - 3
+    int r0[8];  // the current pack's group halves (x first) or groups: -(x shift) - 3
     long long issued;  // loads issued (steps)
 };
 
@@ -1171,7 +1177,7 @@ __host__ __device__ constexpr size_t xrd_batch_smem_bytes(int slab_rows) {
            sizeof(XBProducer);
 }
 
-template <bool RHO>
+template <bool RHO, bool HALF>
 __global__ void __launch_bounds__(XRD_THREADS, 1)
     k_plane_xrd_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
                       const int64_t* __restrict__ start, int n_runs, int slab_floats) {
@@ -1190,6 +1196,7 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
     if (!cons.valid()) return;
     const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
     const uint32_t slab_bytes = (uint32_t)slab_floats * 4u;
+    constexpr int BW = HALF ? HB : CG, NB = CG / BW;  // box columns, boxes per group
     // producers: thread PTID issues the first DEPTH steps; then the first lane
     // of density warp k issues group k's loads of every step (a step's 2K TMA
     // operations on one thread had put that thread's warp on the path to each
@@ -1202,8 +1209,9 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (k < pr.seq.kv) {
-                const int jx = ((pr.seq.cg0 + k) * CG / a.nvy) % a.nvx;
-                pr.r0[k] = -__ldg(a.shift_x + jx) - 3;
+#pragma unroll
+                for (int h = 0; h < NB; ++h)
+                    pr.r0[2 * k + h] = -__ldg(a.shift_x + (((pr.seq.cg0 + k) * CG + h * BW) / a.nvy) % a.nvx) - 3;
             }
     };
     // the loads of groups k0 .. k1 - 1 of the sequence's current step into
@@ -1220,11 +1228,15 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (k < ps.kv) {
-                int v = (pr.r0[k] + ps.q) % ps.nx;
-                if (v < 0) v += ps.nx;
-                const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)k * box;
-                tma_load(tin, dst, bar, (ps.cg0 + k) * CG, v * ps.ny);
-                tma_load(thalo, dst + (uint32_t)(ps.ny * CG * 4), bar, (ps.cg0 + k) * CG, v * ps.ny);
+#pragma unroll
+                for (int h = 0; h < NB; ++h) {
+                    int v = (pr.r0[2 * k + h] + ps.q) % ps.nx;
+                    if (v < 0) v += ps.nx;
+                    const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)k * box + (uint32_t)h * box / NB;
+                    const int c0 = (ps.cg0 + k) * CG + h * BW;
+                    tma_load(tin, dst, bar, c0, v * ps.ny);
+                    tma_load(thalo, dst + (uint32_t)(ps.ny * BW * 4), bar, c0, v * ps.ny);
+                }
             }
         pr.issued += 1;
     };
@@ -1293,7 +1305,11 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
 
     // the register budget of each role holds inside its own branch
     if (drift) {
-        asm volatile("setmaxnreg.inc.sync.aligned.u32 216;" ::: "memory");
+        // the half-box issuers' second x row needs the larger density budget
+        if constexpr (HALF)
+            asm volatile("setmaxnreg.inc.sync.aligned.u32 208;" ::: "memory");
+        else
+            asm volatile("setmaxnreg.inc.sync.aligned.u32 216;" ::: "memory");
         float2 win[WR / 2][6];  // rows 0..19 of the window, in pairs
         float wl[6];            // row 20
 #pragma unroll
@@ -1318,8 +1334,8 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             m = a.m;
             if (act) {
                 const int cg = cons.cg0 + kg;
-                const int jx = (cg * CG / a.nvy) % a.nvx;
-                const int jy = (cg * CG) % a.nvy + lane;
+                const int jx = ((cg * CG + lane) / a.nvy) % a.nvx;  // per lane: a group may span two vx
+                const int jy = (cg * CG + lane) % a.nvy;
 #pragma unroll
                 for (int j = 0; j < 6; ++j) {
                     const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
@@ -1328,7 +1344,8 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                 }
                 int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
                 if (r < 0) r += ny;
-                yoff = kg * (ny + HALO2) * CG + r * CG + lane;
+                // the lane's box (BW columns, rows BW floats apart)
+                yoff = kg * (ny + HALO2) * CG + (lane / BW) * (ny + HALO2) * BW + r * BW + (lane % BW);
             }
         };
         tables();
@@ -1343,8 +1360,8 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
                 ok = wait_phase(bar0 + 8 * P, parity);
                 const float* sl = slabs + P * slab_floats + yoff;
 #pragma unroll
-                for (int p = 0; p < WR / 2; ++p) win[p][P] = make_float2(sl[(2 * p) * CG], sl[(2 * p + 1) * CG]);
-                wl[P] = sl[(WR - 1) * CG];
+                for (int p = 0; p < WR / 2; ++p) win[p][P] = make_float2(sl[(2 * p) * BW], sl[(2 * p + 1) * BW]);
+                wl[P] = sl[(WR - 1) * BW];
                 if (emit) {
                     float xd[WR];
 #pragma unroll
@@ -1435,33 +1452,43 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
             }
         }
     } else {
-        asm volatile("setmaxnreg.dec.sync.aligned.u32 72;" ::: "memory");
+        if constexpr (HALF)
+            asm volatile("setmaxnreg.dec.sync.aligned.u32 88;" ::: "memory");
+        else
+            asm volatile("setmaxnreg.dec.sync.aligned.u32 72;" ::: "memory");
         const bool issuer = (dy & 31) == 0;  // first lane of density warp kq issues group kq
         const int kq = dy >> 5;
-        PSeq qs{};     // the issuer's copy of the sequence
-        int q_r0 = 0;  // its group's -(x shift) - 3
+        PSeq qs{};                  // the issuer's copy of the sequence
+        int q_r0 = 0, q_r1 = 0;     // its group's halves: -(x shift) - 3
         long long q_issued = 0;
         if (issuer) {
             qs = prod->seq;
-            q_r0 = kq < 4 ? prod->r0[kq] : 0;
+            q_r0 = kq < 4 ? prod->r0[2 * kq] : 0;
+            q_r1 = kq < 4 ? prod->r0[2 * kq + 1] : 0;
             q_issued = prod->issued;
         }
         auto issue_q = [&](int d) {
             const uint32_t box = (uint32_t)((qs.ny + HALO2) * CG * 4), bar = bar0 + 8 * d;
             if (kq == 0) expect_bytes(bar, box * (uint32_t)qs.kv);
             if (kq < qs.kv) {
-                int v = (q_r0 + qs.q) % qs.nx;
-                if (v < 0) v += qs.nx;
-                const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)kq * box;
-                tma_load(&maps.tin[qs.r], dst, bar, (qs.cg0 + kq) * CG, v * qs.ny);
-                tma_load(&maps.thalo[qs.r], dst + (uint32_t)(qs.ny * CG * 4), bar, (qs.cg0 + kq) * CG, v * qs.ny);
+#pragma unroll
+                for (int h = 0; h < NB; ++h) {
+                    int v = ((h ? q_r1 : q_r0) + qs.q) % qs.nx;
+                    if (v < 0) v += qs.nx;
+                    const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)kq * box + (uint32_t)h * box / NB;
+                    const int c0 = (qs.cg0 + kq) * CG + h * BW;
+                    tma_load(&maps.tin[qs.r], dst, bar, c0, v * qs.ny);
+                    tma_load(&maps.thalo[qs.r], dst + (uint32_t)(qs.ny * BW * 4), bar, c0, v * qs.ny);
+                }
             }
             q_issued += 1;
             if (!qs.step_on()) {
                 qs.next_pack(runs, start, n_runs);
                 if (qs.valid() && kq < qs.kv) {
                     const Args& a = runs[qs.r].a;
-                    q_r0 = -__ldg(a.shift_x + ((qs.cg0 + kq) * CG / a.nvy) % a.nvx) - 3;
+                    const int c0 = (qs.cg0 + kq) * CG;
+                    q_r0 = -__ldg(a.shift_x + (c0 / a.nvy) % a.nvx) - 3;
+                    if (HALF) q_r1 = -__ldg(a.shift_x + ((c0 + HB) / a.nvy) % a.nvx) - 3;
                 }
             }
         };
@@ -1522,6 +1549,7 @@ __host__ __device__ constexpr size_t yx_batch_smem_bytes(int slab_rows) {
     return (size_t)DEPTH * slab_rows * CG * 4 + DEPTH * 8 + 2 * sizeof(XBProducer);
 }
 
+template <bool HALF>
 __global__ void __launch_bounds__(8 * 32, 2)
     k_plane_yx_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
                      const int64_t* __restrict__ start, int n_runs, int slab_floats) {
@@ -1535,13 +1563,13 @@ __global__ void __launch_bounds__(8 * 32, 2)
     if (!cons.valid()) return;
     const uint32_t slab0 = smem_u32(slabs), bar0 = smem_u32(bars);
     const uint32_t slab_bytes = (uint32_t)slab_floats * 4u;
+    constexpr int BW = HALF ? HB : CG, NB = CG / BW;  // box columns, boxes per group
     auto pack_rows = [&]() {
         const PSeq& s = prod->seq;
         const Args& a = runs[s.r].a;
-        for (int k = 0; k < s.kv; ++k) {
-            const int jx = ((s.cg0 + k) * CG / a.nvy) % a.nvx;
-            prod->r0[k] = -__ldg(a.shift_x + jx) - 3;
-        }
+        for (int k = 0; k < s.kv; ++k)
+            for (int h = 0; h < NB; ++h)
+                prod->r0[2 * k + h] = -__ldg(a.shift_x + (((s.cg0 + k) * CG + h * BW) / a.nvy) % a.nvx) - 3;
     };
     uint32_t extra = 0;  // test hook: the first load of the CTA expects 16 bytes too many
     auto issue = [&](int d) {
@@ -1551,13 +1579,15 @@ __global__ void __launch_bounds__(8 * 32, 2)
         const uint32_t box = (uint32_t)((s.ny + HALO) * CG * 4), bar = bar0 + 8 * d;
         expect_bytes(bar, box * (uint32_t)s.kv + extra);
         extra = 0;
-        for (int k = 0; k < s.kv; ++k) {
-            int v = (prod->r0[k] + s.q) % s.nx;
-            if (v < 0) v += s.nx;
-            const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)k * box;
-            tma_load(tin, dst, bar, (s.cg0 + k) * CG, v * s.ny);
-            tma_load(thalo, dst + (uint32_t)(s.ny * CG * 4), bar, (s.cg0 + k) * CG, v * s.ny);
-        }
+        for (int k = 0; k < s.kv; ++k)
+            for (int h = 0; h < NB; ++h) {
+                int v = (prod->r0[2 * k + h] + s.q) % s.nx;
+                if (v < 0) v += s.nx;
+                const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)k * box + (uint32_t)h * box / NB;
+                const int c0 = (s.cg0 + k) * CG + h * BW;
+                tma_load(tin, dst, bar, c0, v * s.ny);
+                tma_load(thalo, dst + (uint32_t)(s.ny * BW * 4), bar, c0, v * s.ny);
+            }
     };
     auto advance = [&]() {
         prod->seq.next(runs, start, n_runs);
@@ -1572,19 +1602,22 @@ __global__ void __launch_bounds__(8 * 32, 2)
         const PSeq& qs = q.seq;
         const uint32_t box = (uint32_t)((qs.ny + HALO) * CG * 4), bar = bar0 + 8 * d;
         if (kq == 0) expect_bytes(bar, box * (uint32_t)qs.kv);
-        if (kq < qs.kv) {
-            int v = (q.r0[kq] + qs.q) % qs.nx;
-            if (v < 0) v += qs.nx;
-            const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)kq * box;
-            tma_load(&maps.tin[qs.r], dst, bar, (qs.cg0 + kq) * CG, v * qs.ny);
-            tma_load(&maps.thalo[qs.r], dst + (uint32_t)(qs.ny * CG * 4), bar, (qs.cg0 + kq) * CG, v * qs.ny);
-        }
+        if (kq < qs.kv)
+            for (int h = 0; h < NB; ++h) {
+                int v = (q.r0[2 * kq + h] + qs.q) % qs.nx;
+                if (v < 0) v += qs.nx;
+                const uint32_t dst = slab0 + (uint32_t)d * slab_bytes + (uint32_t)kq * box + (uint32_t)h * box / NB;
+                const int c0 = (qs.cg0 + kq) * CG + h * BW;
+                tma_load(&maps.tin[qs.r], dst, bar, c0, v * qs.ny);
+                tma_load(&maps.thalo[qs.r], dst + (uint32_t)(qs.ny * BW * 4), bar, c0, v * qs.ny);
+            }
         q.issued += 1;
         if (!q.seq.step_on()) {
             q.seq.next_pack(runs, start, n_runs);
             if (q.seq.valid() && kq < q.seq.kv) {
                 const Args& a = runs[q.seq.r].a;
-                q.r0[kq] = -__ldg(a.shift_x + ((q.seq.cg0 + kq) * CG / a.nvy) % a.nvx) - 3;
+                for (int h = 0; h < NB; ++h)
+                    q.r0[2 * kq + h] = -__ldg(a.shift_x + (((q.seq.cg0 + kq) * CG + h * BW) / a.nvy) % a.nvx) - 3;
             }
         }
     };
@@ -1628,8 +1661,8 @@ __global__ void __launch_bounds__(8 * 32, 2)
         m = a.m;
         if (act) {
             const int cg = cons.cg0 + kg;
-            const int jx = (cg * CG / a.nvy) % a.nvx;
-            const int jy = (cg * CG) % a.nvy + lane;
+            const int jx = ((cg * CG + lane) / a.nvy) % a.nvx;  // per lane: a group may span two vx
+            const int jy = (cg * CG + lane) % a.nvy;
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
                 const float u = __ldg(a.W_x + (5 - j) * a.nvx + jx), v = __ldg(a.W_y + (5 - j) * a.nvy + jy);
@@ -1638,7 +1671,8 @@ __global__ void __launch_bounds__(8 * 32, 2)
             }
             int r = (y0 - __ldg(a.shift_y + jy) - 3) % ny;
             if (r < 0) r += ny;
-            yoff = kg * (ny + HALO) * CG + r * CG + lane;
+            // the lane's box (BW columns, rows BW floats apart)
+            yoff = kg * (ny + HALO) * CG + (lane / BW) * (ny + HALO) * BW + r * BW + (lane % BW);
         }
     };
     tables();
@@ -1649,7 +1683,7 @@ __global__ void __launch_bounds__(8 * 32, 2)
         if (act) {
             ok = wait_phase(bar0 + 8 * P, parity);
             float2 nv[YT / 2];
-            y_drift<false>(slabs + P * slab_floats + yoff, wy, 0.f, nv);
+            y_drift<false, BW>(slabs + P * slab_floats + yoff, wy, 0.f, nv);
             if (cons.q >= 5) {
                 float* dst = outp + ((int64_t)(cons.q - 5) * ny + y0) * m + (int64_t)(cons.cg0 + kg) * CG + lane;
                 float2 o[YT / 2];
@@ -1748,10 +1782,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 }
 
 // [nx*ny][m] FP32 view of f with a {CG, rows} box
-static bool make_map(CUtensorMap* tm, const void* base, int64_t m, int64_t rows_total, int box_rows) {
+static bool make_map(CUtensorMap* tm, const void* base, int64_t m, int64_t rows_total, int box_rows,
+                     int box_cols = CG) {
     const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)rows_total};
     const cuuint64_t strides[1] = {(cuuint64_t)(m * sizeof(float))};
-    const cuuint32_t box[2] = {(cuuint32_t)CG, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return encoder()(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1854,9 +1889,10 @@ static int launch_runs(Kern kern, int block, size_t smem, const PlaneRun* runs, 
     return VP_OK;
 }
 
+template <bool HALF>
 static int launch_yx_batch(const PlaneRun* runs, const PlaneRun* runs_host, const int64_t* start,
                            const int64_t* start_host, int n_runs, int slab_rows, cudaStream_t st) {
-    auto kern = k_plane_yx_batch;
+    auto kern = k_plane_yx_batch<HALF>;
     const size_t smem = yx_batch_smem_bytes(slab_rows);
     static int raised[64] = {0};
     int dev = 0;
@@ -1875,10 +1911,10 @@ static int launch_yx_batch(const PlaneRun* runs, const PlaneRun* runs_host, cons
                        "k_plane_yx_batch");
 }
 
-template <bool RHO>
+template <bool RHO, bool HALF>
 static int launch_xrd_batch_t(const PlaneRun* runs, const PlaneRun* runs_host, const int64_t* start,
                               const int64_t* start_host, int n_runs, int slab_rows, cudaStream_t st) {
-    auto kern = k_plane_xrd_batch<RHO>;
+    auto kern = k_plane_xrd_batch<RHO, HALF>;
     const size_t smem = xrd_batch_smem_bytes(slab_rows);
     static int raised[64] = {0};
     int dev = 0;
@@ -1906,8 +1942,14 @@ size_t plane_run_bytes() { return sizeof(plane::PlaneRun); }
 // x window's 5 warm-up rows of every line adding a fifth to the loads.
 bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* a, const void* b,
                       const void* c) {
-    return plane_fits(dtype, nx, ny, nvx, nvy, a) && plane_fits(dtype, nx, ny, nvx, nvy, b) &&
-           plane_fits(dtype, nx, ny, nvx, nvy, c) && ny >= 32 && ny <= plane::YMAX / 2 && ny % 8 == 0;
+    using namespace plane;
+    if (dtype != VP_F32 || ny < 32 || ny > YMAX / 2 || ny % 8 != 0 || nx < 1 || nvx < 1) return false;
+    // groups of 32 columns in half boxes of 16, each inside one vx
+    if (nvy % HB != 0 || (nvx * nvy) % CG != 0) return false;
+    if ((int64_t)nx * ny >= (1ll << 31) || nvx * nvy >= (1ll << 31) || nvx * nvy / CG * nx >= (1ll << 31)) return false;
+    for (const void* p : {a, b, c})
+        if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+    return encoder() != nullptr;
 }
 
 int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_t nx, int64_t ny, int64_t nvx,
@@ -1942,7 +1984,10 @@ int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_
     pr->slab_rows = pr->k_pack * ((int)ny + halo);
     if (ny < HALO2 || ny % 8 != 0 || pr->slab_rows > (xfirst ? XB_MAX_SLAB_ROWS : YB_MAX_SLAB_ROWS))
         return set_error(VP_ERR_UNSUPPORTED, "plane batch: rows outside the packed layouts");
-    if (!make_map(&pr->tin, in, a.m, nx * ny, (int)ny) || !make_map(&pr->thalo, in, a.m, nx * ny, halo))
+    // runs whose 32-column groups may span two vx (nvy % 32 != 0) take their
+    // groups in two half boxes, each at its own x row
+    const int bc = nvy % CG ? HB : CG;
+    if (!make_map(&pr->tin, in, a.m, nx * ny, (int)ny, bc) || !make_map(&pr->thalo, in, a.m, nx * ny, halo, bc))
         return set_error(VP_ERR_CUDA, "plane batch: cuTensorMapEncodeTiled failed");
     std::memcpy(record, &rec, sizeof(PlaneRun));
     *items = (a.n_cg + pr->k_pack - 1) / pr->k_pack;
@@ -1951,14 +1996,31 @@ int plane_batch_run(void* record, bool xfirst, const void* in, void* out, int64_
 }
 
 int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs_host, const int64_t* start,
-                       const int64_t* start_host, int n_runs, int64_t items, int slab_rows, cudaStream_t st) {
+                       const int64_t* start_host, int n_full, int n_runs, int64_t items, int slab_rows,
+                       cudaStream_t st) {
     using namespace plane;
     if (items <= 0) return VP_OK;
     const PlaneRun* pr = static_cast<const PlaneRun*>(runs);
     const PlaneRun* ph = static_cast<const PlaneRun*>(runs_host);
-    if (!xfirst) return launch_yx_batch(pr, ph, start, start_host, n_runs, slab_rows, st);
-    return rho ? launch_xrd_batch_t<true>(pr, ph, start, start_host, n_runs, slab_rows, st)
-               : launch_xrd_batch_t<false>(pr, ph, start, start_host, n_runs, slab_rows, st);
+    // records 0 .. n_full - 1 in whole 32-column boxes, the rest in half boxes
+    for (int half = 0; half < 2; ++half) {
+        const int r0 = half ? n_full : 0, nr = half ? n_runs - n_full : n_full;
+        if (nr <= 0 || start_host[r0 + nr] == start_host[r0]) continue;
+        const PlaneRun *q = pr + r0, *qh = ph + r0;
+        const int64_t *sq = start + r0, *sqh = start_host + r0;
+        int rc;
+        if (!xfirst)
+            rc = half ? launch_yx_batch<true>(q, qh, sq, sqh, nr, slab_rows, st)
+                      : launch_yx_batch<false>(q, qh, sq, sqh, nr, slab_rows, st);
+        else if (rho)
+            rc = half ? launch_xrd_batch_t<true, true>(q, qh, sq, sqh, nr, slab_rows, st)
+                      : launch_xrd_batch_t<true, false>(q, qh, sq, sqh, nr, slab_rows, st);
+        else
+            rc = half ? launch_xrd_batch_t<false, true>(q, qh, sq, sqh, nr, slab_rows, st)
+                      : launch_xrd_batch_t<false, false>(q, qh, sq, sqh, nr, slab_rows, st);
+        if (rc) return rc;
+    }
+    return VP_OK;
 }
 
 bool plane_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* f) {

@@ -347,7 +347,7 @@ class BatchStepper2D:
             self.shapes.append(shape)
         # the rule of vp_batch2d_plan (the arenas keep every buffer 256-byte aligned)
         self.fused = [self.fuse_drifts and dtype == torch.float32 and 32 <= s[1] <= 64 and s[1] % 8 == 0
-                      and s[3] % 32 == 0 for s in self.shapes]
+                      and s[3] % 16 == 0 and (s[2] * s[3]) % 32 == 0 for s in self.shapes]
         for p, shape in zip(self.params, self.shapes):
             offs.append(fbytes)
             fbytes += al(esz * shape[0] * shape[1] * shape[2] * shape[3])
