@@ -383,7 +383,8 @@ size_t vp_step1d_workspace_bytes(int64_t nx, int64_t nv);
  * descriptors go to the kernels as parameters), which must stay as planned.
  * Each run's state is advanced in place: f -> s2 -> s1 -> f for the runs
  * whose drift pairs are fused (FP32, 32 <= ny <= 64 with ny % 8 == 0,
- * nvy % 32 == 0, 16-byte aligned buffers, unless vp_batch_tiles.sweeps_only),
+ * nvy % 16 == 0 and nvx * nvy % 32 == 0, 16-byte aligned buffers, unless
+ * vp_batch_tiles.sweeps_only),
  * else f -> s1 -> s2 -> s1 -> s2 -> f. */
 typedef struct vp_batch2d_run {
     int32_t nx, ny, nvx, nvy;
@@ -425,7 +426,7 @@ typedef struct vp_batch_tiles {
     int32_t segments[VP_BATCH_KINDS];    /* CTAs per line of the drifts: 1, 2 or 4 (ignored for the kick) */
     int32_t sweeps_only;                 /* 1: one sweep per axis for every run, even those the fused
                                             drift pairs take (FP32, 32 <= ny <= 64, ny % 8 == 0,
-                                            nvy % 32 == 0) */
+                                            nvy % 16 == 0, nvx * nvy % 32 == 0) */
 } vp_batch_tiles;
 
 size_t vp_batch2d_table_bytes(int32_t n_runs);

@@ -8,7 +8,7 @@
 // device copy (the fused runs' tensor maps are copied from the host table
 // into the plane kernels' parameters), so a sequence of steps is capturable
 // in a CUDA graph. The runs whose layout the fused drift pairs take (FP32,
-// 32 <= ny <= 64 a multiple of 8, nvy a multiple of 32; several column
+// 32 <= ny <= 64 a multiple of 8, nvy a multiple of 16; several column
 // groups of a run per CTA) make three passes over f: x then y with the rho partials
 // (f -> s2), the fused kick (s2 -> s1), y then x (s1 -> f); the others one
 // sweep per axis: x (f -> s1), y + rho partials (s1 -> s2), kick (s2 -> s1),

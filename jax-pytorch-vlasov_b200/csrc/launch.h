@@ -161,7 +161,7 @@ int run_plane(int dtype, bool xfirst, const void* in, void* out, int64_t nx, int
               int64_t x_begin, int64_t x_count, const int* shift_x, const void* W_x, const int* shift_y,
               const void* W_y, double* part, int* tiles, const EqSplit* eq, int* status, int stall, cudaStream_t st);
 // Batched drift pairs (runs of up to 64 rows, a multiple of 8, FP32,
-// nvy % 32 == 0, aligned): one record of plane_run_bytes() per fused run and
+// nvy % 16 == 0, aligned): one record of plane_run_bytes() per fused run and
 // pass in the device table (64-byte aligned, in any order), filled on the host by
 // plane_batch_run (in -> out; part: the density partials
 // [nx][nvx*nvy/32][ny] of the x-first pass, or NULL); items = the run's

@@ -1937,9 +1937,10 @@ static int launch_xrd_batch_t(const PlaneRun* runs, const PlaneRun* runs_host, c
 size_t plane_run_bytes() { return sizeof(plane::PlaneRun); }
 
 // Runs of 32..64 rows, a multiple of 8 (the packs of the x-first pass stage
-// whole 8-row swizzle blocks). The packed passes take 20..64 rows; below 32
-// they lose to the sweeps (24^4 batches: 1.565 against 1.135 ms a step), the
-// x window's 5 warm-up rows of every line adding a fifth to the loads.
+// whole 8-row swizzle blocks), nvy a multiple of 16. The packed passes take
+// 20..64 rows; below 32 they lose to the sweeps (24^4 batches: 1.565 against
+// 1.135 ms a step), the x window's 5 warm-up rows of every line adding a
+// fifth to the loads.
 bool plane_batch_fits(int dtype, int64_t nx, int64_t ny, int64_t nvx, int64_t nvy, const void* a, const void* b,
                       const void* c) {
     using namespace plane;

@@ -309,7 +309,7 @@ class BatchStepper2D:
     (at most 12 launches per step for up to 64 runs) and the state of run
     r is advanced in place in self.f[r]. Each run's step is vp_step2d's: the
     runs in `fused` (FP32, 32 <= Ny <= 64 a multiple of 8, Nvy a multiple of
-    32) take their drift pairs as fused passes, bit-identical to a Stepper2D
+    16, Nvx * Nvy of 32) take their drift pairs as fused passes, bit-identical to a Stepper2D
     with the fused passes; the others one sweep per axis (fuse_drifts=False:
     all of them).
 
