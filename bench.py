@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--diagnostics", type=int, default=1, help="0 none, 1 field energy + mass, 2 + L2/kinetic")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-history-check", action="store_true",
+                    help="skip the 20-step comparison with the reference's FP64 run (128^4 Landau only)")
     ap.add_argument("--sweeps-only", action="store_true",
                     help="2D2V and the batch: one sweep per axis even where the fused (x, y) plane passes apply")
     ap.add_argument("--split", action="store_true",
@@ -335,6 +337,50 @@ def _initial_f(a, dev, dtype, rank, torch):
     return importlib.import_module("jax-pytorch-vlasov_b200.ops").init_product(sp, fv, dtype)
 
 
+def reference_history(a, vp, dev, dtype, torch):
+    """Errors of the first 20 steps against the reference solver's own FP64
+    run of the 128^4 Landau configuration (tests/golden/history_c3.npz, made
+    by tests/golden/make_golden.py): field energy and mass after every step,
+    relative to their largest magnitude, and the mid-step density fluctuation
+    at steps 10 and 20, for the storage type (and split) this bench timed.
+    None for other workloads."""
+    path = os.path.join(ROOT, "tests", "golden", "history_c3.npz")
+    if (a.kind != "2d" or tuple(a.grid) != (128, 128, 128, 128) or a.ic != "landau" or
+            tuple(a.icp[:2]) != (0.05, 0.5) or a.dt != 0.1 or a.vmax != 6.0 or abs(a.L - 4 * math.pi) > 1e-12 or
+            not os.path.exists(path)):
+        return None
+    H = np.load(path)
+    n = a.grid[0]
+    st = vp.Stepper2D(n, n, n, n, a.L, a.L, a.vmax, a.vmax, a.dt, dtype=dtype, device=dev, window=1,
+                      fuse_drifts=not a.sweeps_only, equilibrium="maxwellian" if a.split else None,
+                      precise_tables=a.split)
+    # the golden run's initial condition: the FP64 product of the spatial
+    # profile and the 2D Maxwellian on the reference's grids, rounded once
+    g = vp.vlasov2d2v.Grid.create(n, n, n, n, a.L, a.L, a.vmax, a.vmax, device="cpu", dtype=torch.float64)
+    sp = 1.0 + 0.05 * (torch.cos(0.5 * g.x)[:, None] + torch.cos(0.5 * g.y)[None, :])
+    fv = torch.exp(-0.5 * (g.vx[:, None] ** 2 + g.vy[None, :] ** 2)) / (2.0 * math.pi)
+    if a.split:
+        f64 = vp.ops.init_product(sp.to(dev), fv.to(dev), torch.float64)
+        x = st.split(f64)
+        del f64
+    else:
+        x = vp.ops.init_product(sp.to(dev), fv.to(dev), dtype)
+    h = torch.zeros((20, vp._lib.DIAG_COUNT), dtype=torch.float64, device=dev)
+    x = st.run(x, 10, history=h[:10], graph=True)
+    d10 = st.drho.clone()
+    x = st.run(x, 10, history=h[10:], graph=True)
+    torch.cuda.synchronize(dev)
+    st.check()
+    h, d10, d20 = h.cpu().numpy(), d10.cpu().numpy(), st.drho.cpu().numpy()
+    rel = lambda got, ref: float(np.abs(got - ref).max() / np.abs(ref).max())  # noqa: E731
+    out = {"steps": 20, "W_E": rel(h[:, 0], H["W_E"]), "mass": rel(h[:, 1], H["mass"]),
+           "drho_10": rel(d10, H["drho_10"]), "drho_20": rel(d20, H["drho_20"]),
+           "reference": "tests/golden/history_c3.npz: the reference solver in FP64 on the CPU"}
+    del st, x
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(a):
     import torch
 
@@ -481,6 +527,7 @@ def run_ours(a):
     e2e = None
     if a.e2e_steps > 0:
         e2e = run_e2e(a, x, dev, dtype, world, dist, torch, vp, stepper=st if a.split else None)
+    ref_hist = reference_history(a, vp, dev, dtype, torch) if rank == 0 and not a.no_history_check else None
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -515,6 +562,8 @@ def run_ours(a):
             "diagnostics": {"field_energy_first": float(h[0, 0]), "field_energy_last": float(h[-1, 0]),
                             "mass_drift_rel": float((h[-1, 1] - h[0, 1]) / h[0, 1]), "finite": finite},
         }
+        if ref_hist is not None:
+            line["diagnostics"]["vs_reference_history"] = ref_hist
         if ph is not None:
             line["phases_ms"] = ph
             line["phases_gbs"] = phase_gbs
