@@ -418,16 +418,19 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
                             at<int64_t>(table, h.off_sp1), h.n_plane_full, h.n_plane, h.plane_items1, h.p1_slab_rows,
                             st);
     if (rc) return rc;
+    // the other runs' x sweep starts its CTAs as the plane pass's leave
+    const bool after_planes = h.n_plane > 0;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x1), sx,
-                                  n, h.block[0], h.grid[0], 0, st);
+                                  n, h.block[0], h.grid[0], 0, after_planes, st);
         if (rc) return rc;
     }
     if ((rc = mark(2 * VP_PHASE_DRIFT_X1 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_Y1))) return rc;
     // y drift (dt/2) fused with the rho partials: s1 -> s2
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_y, h.nt_y, want_rho, h.wrap_y && !want_rho,
-                                  at<StridedArgs>(table_dev, h.off_y1), sy1, n, h.block[1], h.grid[1], h.max_ny, st);
+                                  at<StridedArgs>(table_dev, h.off_y1), sy1, n, h.block[1], h.grid[1], h.max_ny, false,
+                                  st);
         if (rc) return rc;
     }
     if (h.phys) {
@@ -449,7 +452,7 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     // y drift (dt/2)
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_y, h.nt_y, false, h.wrap_y, at<StridedArgs>(table_dev, h.off_y2), sy2,
-                                  n, h.block[1], h.grid[1], 0, st);
+                                  n, h.block[1], h.grid[1], 0, false, st);
         if (rc) return rc;
     }
     if ((rc = mark(2 * VP_PHASE_DRIFT_Y2 + 1)) || (rc = mark(2 * VP_PHASE_DRIFT_X2))) return rc;
@@ -460,7 +463,7 @@ int vp_batch2d_step(const void* table, const void* table_dev, int32_t slot, void
     if (rc) return rc;
     if (sweeps) {
         rc = launch_strided_batch(h.dtype, h.vec_x, h.nt_x, false, h.wrap_x, at<StridedArgs>(table_dev, h.off_x2), sx,
-                                  n, h.block[0], h.grid[0], 0, st);
+                                  n, h.block[0], h.grid[0], 0, after_planes, st);
         if (rc) return rc;
     }
     if ((rc = mark(2 * VP_PHASE_DRIFT_X2 + 1)) || (rc = mark(2 * VP_PHASE_DIAG))) return rc;

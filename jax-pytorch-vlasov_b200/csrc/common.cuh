@@ -239,6 +239,17 @@ __device__ __forceinline__ int wrap_up(int r, int n) {
 // ---------------------------------------------------------------------------
 // shared-memory addresses, the global timer, mbarrier waits with a limit
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch. pdl_release (at a kernel's start) lets the
+// next launch on the stream, made with the programmatic-serialization
+// attribute, start its CTAs while this grid still runs; pdl_hold (before a
+// kernel exits) waits until the launch before it has completed and its
+// writes are visible, and returns at once for a launch made without the
+// attribute. A dependent launch must not touch what its predecessor touches;
+// holding before exit makes its completion imply the predecessor's, so the
+// ordinary launches after it see both.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_hold() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

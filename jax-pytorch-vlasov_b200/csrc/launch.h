@@ -195,8 +195,12 @@ int strided_batch_args(int dtype, const void* in, void* out, int64_t n_outer, in
                        double* part, int block, StridedArgs* a, int* vec, int* nt);
 void strided_batch_finish(StridedArgs* a, int vec, int block);
 int strided_batch_pref_vec(int dtype);
+// pdl: launch as a programmatic dependent of the kernel before it on st (a
+// plane pass over the batch's other runs, which must not share a buffer with
+// these sweeps)
 int launch_strided_batch(int dtype, int vec, int nt, bool rho, bool wrap, const StridedArgs* runs,
-                         const int64_t* start, int n_runs, int block, int grid_cap, int max_line, cudaStream_t st);
+                         const int64_t* start, int n_runs, int block, int grid_cap, int max_line, bool pdl,
+                         cudaStream_t st);
 int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int max_outer, int max_line, cudaStream_t st);
 int kick2d_batch_args(int dtype, const void* in, void* out, int64_t n_planes, int64_t nvx, int64_t nvy,
                       const double* Ex, const double* Ey, double dt, double dvx, double dvy, int window,

@@ -1177,10 +1177,13 @@ __host__ __device__ constexpr size_t xrd_batch_smem_bytes(int slab_rows) {
            sizeof(XBProducer);
 }
 
+// The launches of one plane pass (the whole-box and half-box classes, more
+// than 64 runs, then the x sweep of the batch's other runs) follow each other
+// as programmatic dependents (pdl_release / pdl_hold): they work on different
+// runs, so each starts its CTAs on the SMs the launch before it leaves.
 template <bool RHO, bool HALF>
-__global__ void __launch_bounds__(XRD_THREADS, 1)
-    k_plane_xrd_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
-                      const int64_t* __restrict__ start, int n_runs, int slab_floats) {
+__device__ __forceinline__ void xrd_batch_body(const XBMaps& maps, const PlaneRun* __restrict__ runs,
+                                               const int64_t* __restrict__ start, int n_runs, int slab_floats) {
     extern __shared__ __align__(1024) unsigned char smem[];
     float* slabs = reinterpret_cast<float*>(smem);                 // [DEPTH][slab_floats]
     float* stage = slabs + DEPTH * slab_floats;                     // [DSLOTS][XB_SROWS][CG], swizzled
@@ -1534,6 +1537,15 @@ __global__ void __launch_bounds__(XRD_THREADS, 1)
     }
 }
 
+template <bool RHO, bool HALF>
+__global__ void __launch_bounds__(XRD_THREADS, 1)
+    k_plane_xrd_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
+                      const int64_t* __restrict__ start, int n_runs, int slab_floats) {
+    pdl_release();
+    xrd_batch_body<RHO, HALF>(maps, runs, start, n_runs, slab_floats);
+    pdl_hold();
+}
+
 // ---- many runs, y then x ---------------------------------------------------
 // The batched y-first pass in the form of k_plane<0>: 8 warps of 8 y rows, each
 // thread's y drift from 13 rows of the slab, then the 6-row x window of
@@ -1550,9 +1562,8 @@ __host__ __device__ constexpr size_t yx_batch_smem_bytes(int slab_rows) {
 }
 
 template <bool HALF>
-__global__ void __launch_bounds__(8 * 32, 2)
-    k_plane_yx_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
-                     const int64_t* __restrict__ start, int n_runs, int slab_floats) {
+__device__ __forceinline__ void yx_batch_body(const XBMaps& maps, const PlaneRun* __restrict__ runs,
+                                              const int64_t* __restrict__ start, int n_runs, int slab_floats) {
     extern __shared__ __align__(1024) unsigned char smem[];
     float* slabs = reinterpret_cast<float*>(smem);  // [DEPTH][slab_floats]
     uint64_t* bars = reinterpret_cast<uint64_t*>(slabs + DEPTH * slab_floats);
@@ -1763,6 +1774,15 @@ __global__ void __launch_bounds__(8 * 32, 2)
     }
 }
 
+template <bool HALF>
+__global__ void __launch_bounds__(8 * 32, 2)
+    k_plane_yx_batch(const __grid_constant__ XBMaps maps, const PlaneRun* __restrict__ runs,
+                     const int64_t* __restrict__ start, int n_runs, int slab_floats) {
+    pdl_release();
+    yx_batch_body<HALF>(maps, runs, start, n_runs, slab_floats);
+    pdl_hold();
+}
+
 // cuTensorMapEncodeTiled from the driver, looked up once
 static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -1868,7 +1888,7 @@ static int launch_xr(const CUtensorMap& tin, const CUtensorMap& thalo, const Arg
 template <typename Kern>
 static int launch_runs(Kern kern, int block, size_t smem, const PlaneRun* runs, const PlaneRun* runs_host,
                        const int64_t* start, const int64_t* start_host, int n_runs, int per_sm, int slab_rows,
-                       cudaStream_t st, const char* name) {
+                       bool* first, cudaStream_t st, const char* name) {
     XBMaps maps;  // host staging of the parameter (the launch copies it)
     std::memset(static_cast<void*>(&maps), 0, sizeof(maps));
     const char* hb = reinterpret_cast<const char*>(runs_host);  // the host table need not be 64-byte aligned
@@ -1882,8 +1902,22 @@ static int launch_runs(Kern kern, int block, size_t smem, const PlaneRun* runs, 
             std::memcpy(static_cast<void*>(&maps.thalo[i]), rec + offsetof(PlaneRun, thalo), sizeof(CUtensorMap));
         }
         const int64_t grid = std::min<int64_t>(items, (int64_t)sm_count() * per_sm);
-        kern<<<(unsigned)grid, block, smem, st>>>(maps, runs + r0, start + r0, nr, slab_rows * CG);
+        // every launch of the pass after its first one as a programmatic
+        // dependent of the launch before it
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3((unsigned)block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = *first ? 0 : 1;
+        *first = false;
+        const cudaError_t le = cudaLaunchKernelEx(&cfg, kern, maps, runs + r0, start + r0, nr, slab_rows * CG);
         int rc = check_launch(name);
+        if (!rc && le != cudaSuccess) rc = set_error(VP_ERR_CUDA, "plane batch: cudaLaunchKernelEx failed");
         if (rc) return rc;
     }
     return VP_OK;
@@ -1891,7 +1925,7 @@ static int launch_runs(Kern kern, int block, size_t smem, const PlaneRun* runs, 
 
 template <bool HALF>
 static int launch_yx_batch(const PlaneRun* runs, const PlaneRun* runs_host, const int64_t* start,
-                           const int64_t* start_host, int n_runs, int slab_rows, cudaStream_t st) {
+                           const int64_t* start_host, int n_runs, int slab_rows, bool* first, cudaStream_t st) {
     auto kern = k_plane_yx_batch<HALF>;
     const size_t smem = yx_batch_smem_bytes(slab_rows);
     static int raised[64] = {0};
@@ -1907,13 +1941,13 @@ static int launch_yx_batch(const PlaneRun* runs, const PlaneRun* runs_host, cons
     if (slab_rows < 1 || slab_rows > YB_MAX_SLAB_ROWS) return set_error(VP_ERR_ARG, "plane batch: bad slab rows");
     const int occ = occupancy(kern, 8 * 32, smem);
     if (occ < 1) return set_error(VP_ERR_UNSUPPORTED, "plane batch: the kernel does not fit an SM");
-    return launch_runs(kern, 8 * 32, smem, runs, runs_host, start, start_host, n_runs, occ, slab_rows, st,
+    return launch_runs(kern, 8 * 32, smem, runs, runs_host, start, start_host, n_runs, occ, slab_rows, first, st,
                        "k_plane_yx_batch");
 }
 
 template <bool RHO, bool HALF>
 static int launch_xrd_batch_t(const PlaneRun* runs, const PlaneRun* runs_host, const int64_t* start,
-                              const int64_t* start_host, int n_runs, int slab_rows, cudaStream_t st) {
+                              const int64_t* start_host, int n_runs, int slab_rows, bool* first, cudaStream_t st) {
     auto kern = k_plane_xrd_batch<RHO, HALF>;
     const size_t smem = xrd_batch_smem_bytes(slab_rows);
     static int raised[64] = {0};
@@ -1928,8 +1962,8 @@ static int launch_xrd_batch_t(const PlaneRun* runs, const PlaneRun* runs_host, c
         raised[dev] = 1;
     }
     if (slab_rows < 1 || slab_rows > XB_MAX_SLAB_ROWS) return set_error(VP_ERR_ARG, "plane batch: bad slab rows");
-    return launch_runs(kern, XRD_THREADS, smem, runs, runs_host, start, start_host, n_runs, 1, slab_rows, st,
-                       "k_plane_xrd_batch");
+    return launch_runs(kern, XRD_THREADS, smem, runs, runs_host, start, start_host, n_runs, 1, slab_rows, first,
+                       st, "k_plane_xrd_batch");
 }
 
 }  // namespace plane
@@ -2003,7 +2037,9 @@ int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs
     if (items <= 0) return VP_OK;
     const PlaneRun* pr = static_cast<const PlaneRun*>(runs);
     const PlaneRun* ph = static_cast<const PlaneRun*>(runs_host);
-    // records 0 .. n_full - 1 in whole 32-column boxes, the rest in half boxes
+    // records 0 .. n_full - 1 in whole 32-column boxes, the rest in half boxes;
+    // the launches after the first start as its CTAs leave the SMs
+    bool first = true;
     for (int half = 0; half < 2; ++half) {
         const int r0 = half ? n_full : 0, nr = half ? n_runs - n_full : n_full;
         if (nr <= 0 || start_host[r0 + nr] == start_host[r0]) continue;
@@ -2011,14 +2047,14 @@ int launch_plane_batch(bool xfirst, bool rho, const void* runs, const void* runs
         const int64_t *sq = start + r0, *sqh = start_host + r0;
         int rc;
         if (!xfirst)
-            rc = half ? launch_yx_batch<true>(q, qh, sq, sqh, nr, slab_rows, st)
-                      : launch_yx_batch<false>(q, qh, sq, sqh, nr, slab_rows, st);
+            rc = half ? launch_yx_batch<true>(q, qh, sq, sqh, nr, slab_rows, &first, st)
+                      : launch_yx_batch<false>(q, qh, sq, sqh, nr, slab_rows, &first, st);
         else if (rho)
-            rc = half ? launch_xrd_batch_t<true, true>(q, qh, sq, sqh, nr, slab_rows, st)
-                      : launch_xrd_batch_t<true, false>(q, qh, sq, sqh, nr, slab_rows, st);
+            rc = half ? launch_xrd_batch_t<true, true>(q, qh, sq, sqh, nr, slab_rows, &first, st)
+                      : launch_xrd_batch_t<true, false>(q, qh, sq, sqh, nr, slab_rows, &first, st);
         else
-            rc = half ? launch_xrd_batch_t<false, true>(q, qh, sq, sqh, nr, slab_rows, st)
-                      : launch_xrd_batch_t<false, false>(q, qh, sq, sqh, nr, slab_rows, st);
+            rc = half ? launch_xrd_batch_t<false, true>(q, qh, sq, sqh, nr, slab_rows, &first, st)
+                      : launch_xrd_batch_t<false, false>(q, qh, sq, sqh, nr, slab_rows, &first, st);
         if (rc) return rc;
     }
     return VP_OK;

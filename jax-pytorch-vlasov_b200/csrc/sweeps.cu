@@ -308,7 +308,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_strided(const __grid_constant__ S
 
 // The same sweep over the items of many runs: run r owns the global items
 // [start[r], start[r+1]); a block's items only increase, so its run index
-// only moves forward.
+// only moves forward. Launched as a programmatic dependent of a plane pass
+// over the batch's other runs, it holds its completion until the pass's.
 template <typename TS, int VEC, int NT, bool RHO, bool WRAPREUSE>
 __global__ void __launch_bounds__(kBlock, 2)
     k_strided_batch(const StridedArgs* __restrict__ runs, const int64_t* __restrict__ start, int n_runs) {
@@ -320,6 +321,7 @@ __global__ void __launch_bounds__(kBlock, 2)
         const StridedArgs a = runs[r];
         strided_item<TS, VEC, NT, false, RHO, WRAPREUSE, false, chunk_rows<TS, NT, RHO>()>(a, g - start[r], smem_raw);
     }
+    pdl_hold();
 }
 
 // rho[o*n + l] = scale * sum_t part[o][t][l]
@@ -1113,47 +1115,64 @@ int strided_batch_pref_vec(int dtype) { return dtype == VP_F64 ? 2 : 4; }
 
 template <typename TS, int VEC, int NT, bool RHO, bool WRAP>
 static int launch_sb_t(const StridedArgs* runs, const int64_t* start, int n_runs, int block, int grid_cap,
-                       size_t smem, cudaStream_t st) {
+                       size_t smem, bool pdl, cudaStream_t st) {
     auto kern = k_strided_batch<TS, VEC, NT, RHO, WRAP>;
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return set_cuda_error("cudaFuncSetAttribute(k_strided_batch)");
     const int occ = occupancy(kern, block, smem);
     const int grid = std::max(1, std::min(grid_cap, sm_count() * occ));
-    kern<<<grid, block, smem, st>>>(runs, start, n_runs);
-    return check_launch("k_strided_batch");
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    const cudaError_t le = cudaLaunchKernelEx(&cfg, kern, runs, start, n_runs);
+    int rc = check_launch("k_strided_batch");
+    if (!rc && le != cudaSuccess) rc = set_error(VP_ERR_CUDA, "k_strided_batch: cudaLaunchKernelEx failed");
+    return rc;
 }
 
 template <typename TS, bool RHO, bool WRAP>
 static int launch_sb_v(int vec, int nt, const StridedArgs* runs, const int64_t* start, int n_runs, int block,
-                       int grid_cap, size_t smem, cudaStream_t st) {
+                       int grid_cap, size_t smem, bool pdl, cudaStream_t st) {
     constexpr int V = sizeof(TS) == 8 ? 2 : 4;
-    if (vec == V && nt == 7) return launch_sb_t<TS, V, 7, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, st);
-    if (vec == V) return launch_sb_t<TS, V, 6, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, st);
-    return launch_sb_t<TS, 1, 6, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, st);
+    if (vec == V && nt == 7)
+        return launch_sb_t<TS, V, 7, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, pdl, st);
+    if (vec == V) return launch_sb_t<TS, V, 6, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, pdl, st);
+    return launch_sb_t<TS, 1, 6, RHO, WRAP>(runs, start, n_runs, block, grid_cap, smem, pdl, st);
 }
 
 template <bool RHO, bool WRAP>
 static int launch_sb_d(int dtype, int vec, int nt, const StridedArgs* runs, const int64_t* start, int n_runs,
-                       int block, int grid_cap, size_t smem, cudaStream_t st) {
+                       int block, int grid_cap, size_t smem, bool pdl, cudaStream_t st) {
     switch (dtype) {
-        case VP_F32: return launch_sb_v<float, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
-        case VP_F64: return launch_sb_v<double, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+        case VP_F32:
+            return launch_sb_v<float, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, pdl, st);
+        case VP_F64:
+            return launch_sb_v<double, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, pdl, st);
         case VP_BF16:
-            return launch_sb_v<__nv_bfloat16, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+            return launch_sb_v<__nv_bfloat16, RHO, WRAP>(vec, nt, runs, start, n_runs, block, grid_cap, smem, pdl,
+                                                          st);
     }
     return set_error(VP_ERR_DTYPE, "unknown dtype");
 }
 
 int launch_strided_batch(int dtype, int vec, int nt, bool rho, bool wrap, const StridedArgs* runs,
-                         const int64_t* start, int n_runs, int block, int grid_cap, int max_line, cudaStream_t st) {
+                         const int64_t* start, int n_runs, int block, int grid_cap, int max_line, bool pdl,
+                         cudaStream_t st) {
     if (block != 128 && block != 256) return set_error(VP_ERR_ARG, "batched sweep: block must be 128 or 256");
     if (rho) {
         const size_t smem = (size_t)(block / 32) * max_line * sizeof(double);
-        return launch_sb_d<true, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, smem, st);
+        return launch_sb_d<true, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, smem, pdl, st);
     }
-    if (wrap) return launch_sb_d<false, true>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, st);
-    return launch_sb_d<false, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, st);
+    if (wrap) return launch_sb_d<false, true>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, pdl, st);
+    return launch_sb_d<false, false>(dtype, vec, nt, runs, start, n_runs, block, grid_cap, 0, pdl, st);
 }
 
 int launch_rho_finalize_batch(const RhoFinRun* runs, int n_runs, int max_outer, int max_line, cudaStream_t st) {
