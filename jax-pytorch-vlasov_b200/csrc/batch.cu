@@ -14,8 +14,9 @@
 // sweep per axis: x (f -> s1), y + rho partials (s1 -> s2), kick (s2 -> s1),
 // y (s1 -> s2), x (s2 -> f). Each kind of pass is one launch for all runs
 // that take it, plus the rho finalize, 3 Poisson kernels and the
-// diagnostics: at most 12 launches per step for up to 64 runs (the fused
-// passes launch once per 64 runs: their tensor maps are launch parameters).
+// diagnostics: at most 14 launches per step for up to 64 runs (the fused
+// passes launch once per box class and per 64 runs: their tensor maps are
+// launch parameters; the launches of a pass chain as programmatic dependents).
 // Every run's arithmetic is that of vp_step2d (same item bodies, same
 // weights, same reduction order for the default tile shapes).
 #include <algorithm>

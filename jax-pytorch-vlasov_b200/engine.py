@@ -306,7 +306,7 @@ class Stepper1D(_Stepper):
 class BatchStepper2D:
     """Independent 2D2V runs of uneven sizes and parameters advanced in
     lockstep: vp_batch2d_step launches one kernel per substep for all runs
-    (at most 12 launches per step for up to 64 runs) and the state of run
+    (at most 14 launches per step for up to 64 runs) and the state of run
     r is advanced in place in self.f[r]. Each run's step is vp_step2d's: the
     runs in `fused` (FP32, 32 <= Ny <= 64 a multiple of 8, Nvy a multiple of
     16, Nvx * Nvy of 32) take their drift pairs as fused passes, bit-identical to a Stepper2D
