@@ -202,8 +202,10 @@ def test_autotune_small_batch(vp, tmp_path):
 
 
 def test_batch_beyond_64_runs(vp):
-    """66 runs, fused ones on both sides of the 64-run boundary of the plane
-    passes' parameter chunks: each equals the run stepped alone."""
+    """66 runs, fused ones at run indices on both sides of 64 (the plane
+    records, fused runs only, map back to their runs): each equals the run
+    stepped alone. More than 64 fused runs per launch class:
+    test_batch_chained_plane_launches."""
     small = dict(Nx=8, Ny=8, Nvx=16, Nvy=16, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=6.0, dt=0.1)
     big = dict(Nx=32, Ny=32, Nvx=16, Nvy=32, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=5.0, dt=0.1)
     runs = [dict(big) if r in (1, 64, 65) else dict(small) for r in range(66)]
@@ -221,6 +223,44 @@ def test_batch_beyond_64_runs(vp):
             ref[r] = (st, st.step(f))
             assert torch.equal(b.f[r], ref[r][1]), r
             assert torch.equal(b.drho[r], st.drho), r
+
+
+@pytest.mark.parametrize("physics", [True, False])
+def test_batch_chained_plane_launches(vp, physics):
+    """More than 64 fused runs in each box class (two launches per class and
+    pass, the 64-run parameter chunks) and runs on sweeps: the plane passes'
+    four launches and the sweep after them follow each other as programmatic
+    dependents. Every run against the same batch on one sweep per axis:
+    bit-identical drifts, and with the field the density to 1e-9 (its
+    summation order differs)."""
+    base = dict(Nx=32, Ny=32, Lx=4 * math.pi, Ly=4 * math.pi, Vx_max=6.0, Vy_max=6.0, dt=0.1)
+    whole = dict(base, Nvx=16, Nvy=32)
+    half = dict(base, Nvx=16, Nvy=48)
+    swept = dict(base, Nx=16, Ny=16, Nvx=16, Nvy=32)
+    runs = [dict(whole) for _ in range(66)] + [dict(half) for _ in range(66)] + [dict(swept) for _ in range(3)]
+    # interleave the classes, so that the plan's ordering is exercised too
+    order = [r for trio in zip(range(0, 66), range(66, 132)) for r in trio] + [132, 133, 134]
+    runs = [runs[r] for r in order]
+    dtype = torch.float32
+    a = vp.BatchStepper2D(runs, dtype=dtype, physics_mode=physics, diagnostics=1 if physics else 0)
+    b = vp.BatchStepper2D(runs, dtype=dtype, physics_mode=physics, diagnostics=1 if physics else 0,
+                          fuse_drifts=False)
+    assert sum(a.fused) == 132 and not any(b.fused)
+    for r, p in enumerate(runs):
+        f0 = _ic(vp, p, r, dtype)
+        a.set_state(r, f0)
+        b.set_state(r, f0)
+    for _ in range(2):
+        a.step(0)
+        b.step(0)
+    torch.cuda.synchronize()
+    a.check()
+    for r in range(len(runs)):
+        if physics:
+            np.testing.assert_allclose(a.drho[r].cpu().numpy(), b.drho[r].cpu().numpy(), rtol=0, atol=1e-9)
+            assert (a.f[r] - b.f[r]).abs().max().item() <= 1e-5 * b.f[r].abs().max().item(), r
+        else:
+            assert torch.equal(a.f[r], b.f[r]), r
 
 
 @pytest.mark.parametrize("physics", [True, False])
